@@ -1,0 +1,153 @@
+/*
+ * b200knn -- exact brute-force Euclidean neighbour search on NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libb200knn.so.  Plain pointers and sizes only.  Every entry point
+ * returns an int status (B2K_OK on success); b2k_last_error() gives a message
+ * for the calling thread's last failure.
+ *
+ * Results contract (the one mlxlearn.neighbors defines):
+ *  - kNN rows are ordered by the exact real squared distance of the float32
+ *    coordinates, ties broken by the smaller training index;
+ *  - a radius neighbour is a training row with exact squared distance
+ *    <= fl64(radius * radius);
+ *  - distances are float64 sqrt of the canonical squared distance (a strictly
+ *    sequential float64 sum over features of (q_k - x_k)^2, no FMA); radius
+ *    distances are sqrt(min(canonical, R2));
+ *  - indices are int64.
+ *
+ * Each declaration cites the reference interface it replaces, by file:line in
+ * the mlxlearn source tree.
+ */
+#ifndef B200KNN_H
+#define B200KNN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define B2K_API __attribute__((visibility("default")))
+#else
+#define B2K_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define B2K_OK 0
+#define B2K_EINVAL 1      /* shape, k, offset, overlap or pointer errors      */
+#define B2K_ENONFINITE 2  /* NaN / Inf coordinates                            */
+#define B2K_ENOMEM 3      /* device or host allocation failed                 */
+#define B2K_ECUDA 4       /* a CUDA runtime call failed                       */
+#define B2K_ETIMEOUT 5    /* a bounded device wait gave up (kernel error)     */
+#define B2K_EUNSUPPORTED 6 /* e.g. no sm_100 device, or a documented limit    */
+#define B2K_EINJECTED 7   /* fault injected through B2K_FAULT (tests only)    */
+
+/* ----------------------------------------------------------- search modes */
+#define B2K_MODE_AUTO 0        /* bf16 screen where certified, else fp32      */
+#define B2K_MODE_FP32 1        /* plain form: fp32 CUDA-core Gram screen      */
+#define B2K_MODE_BF16 2        /* bf16 tcgen05 screen + certified re-rank     */
+#define B2K_MODE_EXACT 3       /* float64 exhaustive scan + exact ties (slow) */
+
+typedef struct b2k_index b2k_index;
+
+/* Per-call counters (optional: pass NULL). */
+typedef struct b2k_stats {
+  int32_t mode_used;        /* B2K_MODE_* actually run                         */
+  int32_t splits;           /* reference splits of the screen                  */
+  int64_t candidates;       /* candidates re-ranked in float64                 */
+  int64_t list_entries;     /* screen list appends                             */
+  int64_t fallback_rows;    /* queries resolved by the exhaustive exact scan   */
+  int64_t exact_compares;   /* near-tie pairs resolved with exact integer keys */
+  double screen_ms;         /* device time of the screen kernel (if timed)     */
+  double total_ms;          /* device time of the whole call (if timed)        */
+} b2k_stats;
+
+/* Library version (major*10000 + minor*100 + patch). */
+B2K_API int b2k_version(void);
+
+/* Message for the calling thread's last failed call ("" if none). */
+B2K_API const char *b2k_last_error(void);
+
+/* ------------------------------------------------------------------ index */
+
+/* Build a device-resident index from host float32 X[n, d] (C order).  The
+ * index owns a copy; later changes to X do not affect it.
+ * Replaces build_index / DeviceNeighborIndex construction
+ * (src/mlxlearn/_kernels/distance.py:366-392,
+ *  src/mlxlearn_device/_neighbors.py:447-466). */
+B2K_API int b2k_index_create(const float *X, int64_t n, int32_t d, int32_t device, b2k_index **out);
+
+/* Same from a device pointer (copied on `stream`, a cudaStream_t or NULL). */
+B2K_API int b2k_index_create_device(const float *dX, int64_t n, int32_t d, void *stream,
+                            b2k_index **out);
+
+/* Release every device buffer of the index. */
+B2K_API int b2k_index_destroy(b2k_index *index);
+
+/* n, d of the index. Replaces NeighborIndex.n_samples / n_features
+ * (src/mlxlearn/_kernels/distance.py:167-173). */
+B2K_API int b2k_index_shape(const b2k_index *index, int64_t *n, int32_t *d);
+
+/* Copy the owned float32 training rows back to host X[n, d]. Replaces
+ * NeighborIndex.training_data / .X (src/mlxlearn/_kernels/distance.py:98-103,148-156). */
+B2K_API int b2k_index_download(const b2k_index *index, float *X);
+
+/* Device pointer of the owned float32 rows [n, d] (valid until destroy). */
+B2K_API const float *b2k_index_device_data(const b2k_index *index);
+
+/* -------------------------------------------------------------------- kNN */
+
+/* k nearest training rows of each of m host queries Q[m, d].
+ * Outputs (host): idx int64[m, k]; dist float64[m, k] or NULL.
+ * exclude_self: query row i is training row q_offset + i and is skipped.
+ * Replaces NeighborIndex.query (src/mlxlearn/_kernels/distance.py:242-270) and
+ * the native CPU scan _neighbors_cpu_native.query
+ * (src/mlxlearn/_kernels/_neighbors_cpu_native.cpp:362-418). */
+B2K_API int b2k_knn(b2k_index *index, const float *Q, int64_t m, int32_t k, int32_t exclude_self,
+            int64_t q_offset, int32_t mode, double *dist, int64_t *idx, b2k_stats *stats);
+
+/* Same with device pointers, enqueued on `stream` (cudaStream_t; NULL = legacy
+ * default stream).  The call synchronises `stream` before it returns, so
+ * device-side errors (bounded-wait timeouts) are reported by its status.
+ * dQ may be b2k_index_device_data(index) + q_offset*d for self-queries.
+ * Replaces NeighborIndex.query_device / DeviceNeighborIndex.query
+ * (src/mlxlearn/_kernels/distance.py:211-240,
+ *  src/mlxlearn_device/_neighbors.py:271-443). */
+B2K_API int b2k_knn_device(b2k_index *index, const float *dQ, int64_t m, int32_t k,
+                   int32_t exclude_self, int64_t q_offset, int32_t mode, double *d_dist,
+                   int64_t *d_idx, void *stream, b2k_stats *stats);
+
+/* ----------------------------------------------------------------- radius */
+
+typedef struct b2k_radius_result b2k_radius_result;
+
+/* Every training row within `radius` (inclusive, exact) of each host query.
+ * The result is held by the library; read its size with
+ * b2k_radius_result_nnz, copy it out with b2k_radius_result_fetch, then
+ * release it.  Rows ascend by training index, or by (distance, index) when
+ * sort_results is set.
+ * Replaces NeighborIndex.query_radius_csr / RadiusSearch.query_with_plan and
+ * the Metal screen (src/mlxlearn/_kernels/distance.py:285-342,
+ * src/mlxlearn/_kernels/radius.py:380-453,
+ * src/mlxlearn/_kernels/radius_metal_v1.py:552-611). */
+B2K_API int b2k_radius(b2k_index *index, const float *Q, int64_t m, double radius,
+               int32_t exclude_self, int64_t q_offset, int32_t need_distance,
+               int32_t sort_results, b2k_radius_result **out);
+
+/* Number of (query, neighbour) pairs of a radius result. */
+B2K_API int b2k_radius_result_nnz(const b2k_radius_result *res, int64_t *nnz);
+
+/* Copy a radius result into host CSR buffers: indptr int64[m+1],
+ * indices int64[nnz], dist float64[nnz] or NULL (RadiusCSR,
+ * src/mlxlearn/_kernels/radius_result.py:33-55). */
+B2K_API int b2k_radius_result_fetch(const b2k_radius_result *res, int64_t *indptr, int64_t *indices,
+                            double *dist);
+
+B2K_API int b2k_radius_result_release(b2k_radius_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200KNN_H */

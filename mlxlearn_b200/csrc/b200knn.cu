@@ -1,0 +1,601 @@
+// C ABI of libb200knn.so: index lifetime and the kNN entry points.
+//
+// Call flow of one kNN batch (all on one stream):
+//   prep_queries  -> per-query screen bound E (and the -2*bf16(q) operand)
+//   screen        -> tcgen05 bf16 (screen_tc.cu) or fp32 CUDA-core (screen_simt.cu)
+//   certify       -> float64 re-rank + exact near-tie resolution (certify.cu)
+//   exact         -> exhaustive exact scan of the rare rows certify could not
+//                    finish (list overflow), no-op otherwise
+// Scratch buffers come from the stream-ordered allocator (cudaMallocAsync).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+struct b2k_index {
+  b2k::Index ix;
+};
+
+namespace b2k {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define B2K_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(e_ == cudaErrorMemoryAllocation ? B2K_ENOMEM : B2K_ECUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+  } while (0)
+
+// Host-side fault injection for failure-path tests (B2K_FAULT=alloc|launch|timeout).
+static int fault_mode() {
+  const char* f = getenv("B2K_FAULT");
+  if (!f || !*f) return 0;
+  if (!strcmp(f, "alloc")) return 1;
+  if (!strcmp(f, "launch")) return 2;
+  if (!strcmp(f, "timeout")) return 3;
+  return 0;
+}
+
+int num_sms(int device) {
+  static int cached[64] = {0};
+  if (device < 0 || device >= 64) return 148;
+  if (!cached[device]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[device] = v;
+  }
+  return cached[device];
+}
+
+// --------------------------------------------------------------- TMA maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                        uint32_t box_inner, uint32_t box_outer) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * 2};
+  cuuint32_t box[2] = {box_inner, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// ------------------------------------------------------------------ helpers
+static int check_device(int device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0)
+    return fail(B2K_EUNSUPPORTED, "no CUDA device is available");
+  if (device < 0 || device >= count) return fail(B2K_EINVAL, "invalid device %d", device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+    return fail(B2K_ECUDA, "cudaGetDeviceProperties failed");
+  if (prop.major != 10)
+    return fail(B2K_EUNSUPPORTED, "libb200knn needs an sm_100 (B200) device, found sm_%d%d",
+                prop.major, prop.minor);
+  return B2K_OK;
+}
+
+template <typename T>
+static int dalloc(T** p, size_t count, cudaStream_t st) {
+  if (fault_mode() == 1) return fail(B2K_ENOMEM, "injected allocation failure (B2K_FAULT=alloc)");
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), count * sizeof(T), st);
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? B2K_ENOMEM : B2K_ECUDA,
+                "device allocation of %zu bytes failed: %s", count * sizeof(T),
+                cudaGetErrorString(e));
+  return B2K_OK;
+}
+
+static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+static bool overlaps(const void* a, size_t an, const void* b, size_t bn) {
+  if (!a || !b || !an || !bn) return false;
+  auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + bn && y < x + an;
+}
+
+// Free a list of stream-ordered allocations (ignores nulls).
+struct StreamFree {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  ~StreamFree() {
+    for (void* p : ptrs)
+      if (p) cudaFreeAsync(p, st);
+  }
+  template <typename T>
+  T* keep(T* p) {
+    ptrs.push_back(p);
+    return p;
+  }
+};
+
+static int finish_index(Index& ix, cudaStream_t st) {
+  float init[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  B2K_CUDA(cudaMemcpyAsync(ix.stats_dev, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  launch_prep_index(&ix, st);
+  B2K_CUDA(cudaGetLastError());
+  float stats[8];
+  B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  ix.xn_max = stats[0];
+  ix.nx_max = stats[1];
+  ix.ex32_max = stats[5];
+  int bad;
+  memcpy(&bad, &stats[2], 4);
+  ix.range_ok = bad == 0;
+  return B2K_OK;
+}
+
+static int ensure_bf16(Index& ix) {
+  std::lock_guard<std::mutex> lock(ix.mu);
+  if (ix.bf16_ready) return B2K_OK;
+  cudaStream_t st = ix.stream;
+  ix.dp = (int32_t)round_up(ix.d, kTcBK);
+  ix.n_pad_tc = round_up(ix.n, kTcBN);
+  B2K_CUDA(cudaMalloc(&ix.Xh, (size_t)ix.n_pad_tc * ix.dp * sizeof(uint16_t)));
+  B2K_CUDA(cudaMalloc(&ix.nxh, (size_t)ix.n_pad_tc * sizeof(float)));
+  launch_prep_index_bf16(&ix, st);
+  B2K_CUDA(cudaGetLastError());
+  float stats[8];
+  B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  ix.xh_max = stats[3];
+  ix.ex_max = stats[4];
+  if (!tensor_map_2d_bf16(&ix.tmap_b, ix.Xh, (uint64_t)ix.dp, (uint64_t)ix.n_pad_tc, kTcBK, kTcBN))
+    return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the reference rows");
+  ix.bf16_ready = true;
+  return B2K_OK;
+}
+
+// Reference splits: fill the GPU with (query tile, split) work units while
+// keeping the number of candidate lists per query small.
+static int choose_splits(int64_t m_tiles, int64_t n_tiles, int64_t slots) {
+  if (m_tiles <= 0 || n_tiles <= 0) return 1;
+  int best = 1;
+  double best_cost = 1e300;
+  for (int S = 1; S <= 16 && S <= n_tiles; ++S) {
+    const double units = (double)m_tiles * S;
+    const double waves = std::ceil(units / (double)slots);
+    // time ~ waves * (n_tiles / S); small penalty per extra split (more list traffic)
+    const double cost = waves * std::ceil((double)n_tiles / S) * (1.0 + 0.01 * (S - 1));
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = S;
+    }
+  }
+  return best;
+}
+
+static int run_exact(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
+                     int64_t q_offset, double* d_dist, int64_t* d_idx, const int* rows,
+                     const int* row_count, unsigned long long* counters, int* status,
+                     cudaStream_t st, StreamFree& fr, bool use_scratch) {
+  ExactArgs ea{};
+  ea.X = ix.X;
+  ea.Q = dQ;
+  ea.n = ix.n;
+  ea.m = m;
+  ea.d = ix.d;
+  ea.k = k;
+  ea.exclude_self = exclude_self;
+  ea.q_offset = q_offset;
+  ea.rows = rows;
+  ea.row_count = row_count;
+  ea.dist = d_dist;
+  ea.idx = d_idx;
+  ea.counters = counters;
+  ea.status = status;
+  const int sms = num_sms(ix.device);
+  ea.grid = (int)std::min<int64_t>(rows ? sms : m, (int64_t)2 * sms);
+  if (ea.grid <= 0) return B2K_OK;
+  ea.scratch = nullptr;
+  if (use_scratch) {
+    int rc = dalloc(&ea.scratch, (size_t)ea.grid * ix.n, st);
+    if (rc) return rc;
+    fr.keep(ea.scratch);
+  }
+  launch_exact(ea, st);
+  B2K_CUDA(cudaGetLastError());
+  return B2K_OK;
+}
+
+static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
+                           int64_t q_offset, int mode, double* d_dist, int64_t* d_idx,
+                           cudaStream_t st, b2k_stats* stats) {
+  const int fm = fault_mode();
+  if (fm == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
+  if (mode == B2K_MODE_AUTO)
+    mode = (!ix.range_ok || k > kMaxK) ? B2K_MODE_EXACT
+           : (ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16
+                                         : B2K_MODE_FP32;
+  if ((mode == B2K_MODE_BF16 || mode == B2K_MODE_FP32) && (!ix.range_ok || k > kMaxK))
+    mode = B2K_MODE_EXACT;
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->mode_used = mode;
+  }
+  if (m == 0) return B2K_OK;
+  cudaSetDevice(ix.device);
+  StreamFree fr{st, {}};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (stats)
+    for (auto& e : ev) cudaEventCreate(&e);
+  if (stats) cudaEventRecord(ev[0], st);
+
+  int* status = nullptr;
+  unsigned long long* counters = nullptr;
+  int rc;
+  if ((rc = dalloc(&status, 8, st))) return rc;
+  fr.keep(status);
+  if ((rc = dalloc(&counters, 4, st))) return rc;
+  fr.keep(counters);
+  B2K_CUDA(cudaMemsetAsync(status, 0, 8 * sizeof(int), st));
+  B2K_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+
+  int S = 1;
+  if (mode == B2K_MODE_EXACT) {
+    rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, nullptr, nullptr,
+                   counters, status, st, fr, true);
+    if (rc) return rc;
+  } else {
+    if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
+    const bool tc = mode == B2K_MODE_BF16;
+    const int64_t bm = tc ? kTcBM : kSimtBM;
+    const int64_t m_pad = round_up(m, bm);
+    const int64_t n_tiles = tc ? ix.n_pad_tc / kTcBN : (ix.n + kSimtBN - 1) / kSimtBN;
+    const int sms = num_sms(ix.device);
+    S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
+    QueryPrep qp{};
+    if ((rc = dalloc(&qp.E, (size_t)m_pad, st))) return rc;
+    fr.keep(qp.E);
+    qp.flags = status + 4;  // shares the zeroed status block
+    if (tc) {
+      if ((rc = dalloc(&qp.Ah, (size_t)m_pad * ix.dp, st))) return rc;
+      fr.keep(qp.Ah);
+    }
+    launch_prep_queries(&ix, dQ, m, m_pad, mode, qp, st);
+    B2K_CUDA(cudaGetLastError());
+    ScreenOut so{};
+    so.cap = kListCap;
+    so.m_pad = (int)m_pad;
+    if ((rc = dalloc(&so.lists, (size_t)S * m_pad * kListCap, st))) return rc;
+    fr.keep(so.lists);
+    if ((rc = dalloc(&so.counts, (size_t)S * m_pad, st))) return rc;
+    fr.keep(so.counts);
+    if ((rc = dalloc(&so.kth, (size_t)S * m_pad * k, st))) return rc;
+    fr.keep(so.kth);
+    if (stats) cudaEventRecord(ev[1], st);
+    if (tc) {
+      CUtensorMap tmap_a;
+      if (!tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
+        return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
+      int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, k, exclude_self, q_offset, S, qp.E, so,
+                                status, st);
+      if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
+                          cudaGetErrorString((cudaError_t)lr));
+    } else {
+      launch_screen_simt(&ix, dQ, m, m_pad, k, exclude_self, q_offset, S, qp.E, so, st);
+      B2K_CUDA(cudaGetLastError());
+    }
+    if (stats) cudaEventRecord(ev[2], st);
+    int* fb_list = nullptr;
+    if ((rc = dalloc(&fb_list, (size_t)m, st))) return rc;
+    fr.keep(fb_list);
+    CertifyArgs ca{};
+    ca.X = ix.X;
+    ca.Q = dQ;
+    ca.n = ix.n;
+    ca.m = m;
+    ca.d = ix.d;
+    ca.k = k;
+    ca.S = S;
+    ca.scr = so;
+    ca.E = qp.E;
+    ca.dist = d_dist;
+    ca.idx = d_idx;
+    ca.fallback_list = fb_list;
+    ca.fallback_count = status + 2;
+    ca.counters = counters;
+    launch_certify(ca, st);
+    B2K_CUDA(cudaGetLastError());
+    // Rows the screen could not certify (list overflow, or query coordinates
+    // outside the screen's safe range: see the flag check below).
+    rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
+                   counters, status, st, fr, false);
+    if (rc) return rc;
+  }
+  if (stats) cudaEventRecord(ev[3], st);
+  int hstatus[8];
+  unsigned long long hcnt[4];
+  B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaMemcpyAsync(hcnt, counters, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  if (fm == 3) hstatus[0] = DEV_TIMEOUT_FULL;
+  if (hstatus[0] == DEV_TOO_MANY_TIES)
+    return fail(B2K_EUNSUPPORTED,
+                "more than %d training rows tie (within float64 error) with a query's k-th "
+                "neighbour",
+                kExactCap);
+  if (hstatus[0] != DEV_OK)
+    return fail(B2K_ETIMEOUT, "a bounded device wait gave up (code %d)", hstatus[0]);
+  if (hstatus[4] & 1) {
+    // Some query coordinate is outside the screens' safe range: redo exactly.
+    return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, B2K_MODE_EXACT, d_dist, d_idx,
+                           st, stats);
+  }
+  if (stats) {
+    stats->splits = S;
+    stats->candidates = (int64_t)hcnt[0];
+    stats->list_entries = (int64_t)hcnt[1];
+    stats->exact_compares = (int64_t)hcnt[2];
+    stats->fallback_rows = (int64_t)hcnt[3];
+    float ms = 0;
+    if (mode != B2K_MODE_EXACT && cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess)
+      stats->screen_ms = ms;
+    if (cudaEventElapsedTime(&ms, ev[0], ev[3]) == cudaSuccess) stats->total_ms = ms;
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  return B2K_OK;
+}
+
+static int validate_knn(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
+                        int64_t q_offset, int32_t mode) {
+  if (m < 0) return fail(B2K_EINVAL, "negative query count");
+  if (k <= 0) return fail(B2K_EINVAL, "Expected n_neighbors > 0. Got %d", k);
+  const int64_t limit = ix.n - (exclude_self ? 1 : 0);
+  if (k > limit) return fail(B2K_EINVAL, "n_neighbors must be <= %lld, got %d.", (long long)limit, k);
+  if (m >= (int64_t)1 << 31) return fail(B2K_EINVAL, "query count must fit int32");
+  if (exclude_self && (q_offset < 0 || q_offset + m > ix.n))
+    return fail(B2K_EINVAL,
+                "exclude_self requires the query matrix to be the training matrix: got %lld "
+                "query rows at offset %lld and %lld training rows.",
+                (long long)m, (long long)q_offset, (long long)ix.n);
+  if (mode < B2K_MODE_AUTO || mode > B2K_MODE_EXACT) return fail(B2K_EINVAL, "unknown mode %d", mode);
+  return B2K_OK;
+}
+
+static bool host_finite(const float* v, size_t count) {
+  for (size_t i = 0; i < count; ++i) {
+    uint32_t b;
+    memcpy(&b, v + i, 4);
+    if ((b & 0x7f800000u) == 0x7f800000u) return false;
+  }
+  return true;
+}
+
+}  // namespace b2k
+
+using namespace b2k;
+
+// ===================================================================== C ABI
+extern "C" {
+
+int b2k_version(void) { return 100; }
+
+const char* b2k_last_error(void) { return g_last_error.c_str(); }
+
+static int create_common(int device, int64_t n, int32_t d, b2k_index** out) {
+  if (!out) return fail(B2K_EINVAL, "out must not be NULL");
+  *out = nullptr;
+  if (n <= 0 || d <= 0) return fail(B2K_EINVAL, "X must be a nonempty two-dimensional matrix");
+  if (n >= ((int64_t)1 << 31)) return fail(B2K_EINVAL, "training row count must fit int32 indices");
+  if (fault_mode() == 1) return fail(B2K_ENOMEM, "injected allocation failure (B2K_FAULT=alloc)");
+  return check_device(device);
+}
+
+// Keep the stream-ordered pool's memory mapped between calls (the default
+// release threshold of 0 unmaps it at every synchronisation, so each query
+// batch would re-map its scratch).
+static void keep_pool(int device) {
+  static bool done[64] = {false};
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  done[device] = true;
+}
+
+static int build_from_device(b2k_index* h, const float* src, cudaMemcpyKind kind,
+                             cudaStream_t user_st) {
+  Index& ix = h->ix;
+  B2K_CUDA(cudaSetDevice(ix.device));
+  keep_pool(ix.device);
+  B2K_CUDA(cudaStreamCreateWithFlags(&ix.stream, cudaStreamNonBlocking));
+  const size_t bytes = (size_t)ix.n * ix.d * sizeof(float);
+  B2K_CUDA(cudaMalloc(&ix.X, bytes));
+  B2K_CUDA(cudaMalloc(&ix.nx32, (size_t)ix.n * sizeof(float)));
+  B2K_CUDA(cudaMalloc(&ix.center, (size_t)ix.d * sizeof(float)));
+  B2K_CUDA(cudaMalloc(&ix.colsum, (size_t)ix.d * sizeof(double)));
+  B2K_CUDA(cudaMalloc(&ix.nx64, (size_t)ix.n * sizeof(double)));
+  B2K_CUDA(cudaMalloc(&ix.stats_dev, 8 * sizeof(float)));
+  if (kind == cudaMemcpyDeviceToDevice && user_st) {
+    B2K_CUDA(cudaMemcpyAsync(ix.X, src, bytes, kind, user_st));
+    B2K_CUDA(cudaStreamSynchronize(user_st));
+  } else {
+    B2K_CUDA(cudaMemcpyAsync(ix.X, src, bytes, kind, ix.stream));
+  }
+  return finish_index(ix, ix.stream);
+}
+
+int b2k_index_create(const float* X, int64_t n, int32_t d, int32_t device, b2k_index** out) {
+  int rc = create_common(device, n, d, out);
+  if (rc) return rc;
+  if (!X) return fail(B2K_EINVAL, "X must not be NULL");
+  if (!host_finite(X, (size_t)n * d))
+    return fail(B2K_ENONFINITE, "training coordinates must be finite");
+  auto* h = new b2k_index();
+  h->ix.device = device;
+  h->ix.n = n;
+  h->ix.d = d;
+  rc = build_from_device(h, X, cudaMemcpyHostToDevice, nullptr);
+  if (rc) {
+    b2k_index_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return B2K_OK;
+}
+
+int b2k_index_create_device(const float* dX, int64_t n, int32_t d, void* stream,
+                            b2k_index** out) {
+  int device = 0;
+  cudaPointerAttributes attr;
+  if (dX && cudaPointerGetAttributes(&attr, dX) == cudaSuccess && attr.type == cudaMemoryTypeDevice)
+    device = attr.device;
+  int rc = create_common(device, n, d, out);
+  if (rc) return rc;
+  if (!dX) return fail(B2K_EINVAL, "X must not be NULL");
+  auto* h = new b2k_index();
+  h->ix.device = device;
+  h->ix.n = n;
+  h->ix.d = d;
+  rc = build_from_device(h, dX, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  if (rc) {
+    b2k_index_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return B2K_OK;
+}
+
+int b2k_index_destroy(b2k_index* h) {
+  if (!h) return B2K_OK;
+  Index& ix = h->ix;
+  cudaSetDevice(ix.device);
+  if (ix.stream) cudaStreamSynchronize(ix.stream);
+  cudaFree(ix.X);
+  cudaFree(ix.nx32);
+  cudaFree(ix.center);
+  cudaFree(ix.colsum);
+  cudaFree(ix.nx64);
+  cudaFree(ix.stats_dev);
+  cudaFree(ix.Xh);
+  cudaFree(ix.nxh);
+  if (ix.stream) cudaStreamDestroy(ix.stream);
+  delete h;
+  return B2K_OK;
+}
+
+int b2k_index_shape(const b2k_index* h, int64_t* n, int32_t* d) {
+  if (!h) return fail(B2K_EINVAL, "index must not be NULL");
+  if (n) *n = h->ix.n;
+  if (d) *d = h->ix.d;
+  return B2K_OK;
+}
+
+int b2k_index_download(const b2k_index* h, float* X) {
+  if (!h || !X) return fail(B2K_EINVAL, "index and X must not be NULL");
+  cudaSetDevice(h->ix.device);
+  B2K_CUDA(cudaMemcpy(X, h->ix.X, (size_t)h->ix.n * h->ix.d * sizeof(float),
+                      cudaMemcpyDeviceToHost));
+  return B2K_OK;
+}
+
+const float* b2k_index_device_data(const b2k_index* h) { return h ? h->ix.X : nullptr; }
+
+int b2k_knn_device(b2k_index* h, const float* dQ, int64_t m, int32_t k, int32_t exclude_self,
+                   int64_t q_offset, int32_t mode, double* d_dist, int64_t* d_idx, void* stream,
+                   b2k_stats* stats) {
+  if (!h) return fail(B2K_EINVAL, "index must not be NULL");
+  Index& ix = h->ix;
+  int rc = validate_knn(ix, m, k, exclude_self, q_offset, mode);
+  if (rc) return rc;
+  if (m > 0 && (!dQ || !d_idx)) return fail(B2K_EINVAL, "queries and indices must not be NULL");
+  if (overlaps(d_idx, (size_t)m * k * 8, dQ, (size_t)m * ix.d * 4) ||
+      overlaps(d_dist, (size_t)m * k * 8, dQ, (size_t)m * ix.d * 4) ||
+      overlaps(d_idx, (size_t)m * k * 8, d_dist, (size_t)m * k * 8))
+    return fail(B2K_EINVAL, "output buffers must not overlap inputs or each other");
+  return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, mode, d_dist, d_idx,
+                         (cudaStream_t)stream, stats);
+}
+
+int b2k_knn(b2k_index* h, const float* Q, int64_t m, int32_t k, int32_t exclude_self,
+            int64_t q_offset, int32_t mode, double* dist, int64_t* idx, b2k_stats* stats) {
+  if (!h) return fail(B2K_EINVAL, "index must not be NULL");
+  Index& ix = h->ix;
+  int rc = validate_knn(ix, m, k, exclude_self, q_offset, mode);
+  if (rc) return rc;
+  if (m == 0) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    return B2K_OK;
+  }
+  if (!Q || !idx) return fail(B2K_EINVAL, "queries and indices must not be NULL");
+  if (!host_finite(Q, (size_t)m * ix.d))
+    return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
+  cudaSetDevice(ix.device);
+  cudaStream_t st = ix.stream;
+  float* dQ = nullptr;
+  double* dd = nullptr;
+  int64_t* di = nullptr;
+  StreamFree fr{st, {}};
+  if ((rc = dalloc(&dQ, (size_t)m * ix.d, st))) return rc;
+  fr.keep(dQ);
+  if ((rc = dalloc(&di, (size_t)m * k, st))) return rc;
+  fr.keep(di);
+  if (dist) {
+    if ((rc = dalloc(&dd, (size_t)m * k, st))) return rc;
+    fr.keep(dd);
+  }
+  B2K_CUDA(cudaMemcpyAsync(dQ, Q, (size_t)m * ix.d * sizeof(float), cudaMemcpyHostToDevice, st));
+  rc = knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, mode, dd, di, st, stats);
+  if (rc) return rc;
+  B2K_CUDA(cudaMemcpyAsync(idx, di, (size_t)m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  if (dist)
+    B2K_CUDA(cudaMemcpyAsync(dist, dd, (size_t)m * k * sizeof(double), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  return B2K_OK;
+}
+
+}  // extern "C"

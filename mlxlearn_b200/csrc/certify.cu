@@ -1,0 +1,321 @@
+// Certification, float64 re-rank and exact tie resolution.
+//
+// certify_kernel (one warp per query) turns the screen's candidate lists into
+// the final answer:
+//   1. V_k = k-th smallest screen value over all splits (bisection over the
+//      splits' k smallest values); threshold Tf = V_k + 2E (rounded up).
+//   2. Candidates = list entries with v <= Tf (tracker.cuh proves that no other
+//      row can be in the answer).
+//   3. Canonical float64 squared distance of each candidate (strictly
+//      sequential, no FMA: bit-identical to the host canonical value).
+//   4. Sort by (value, index); within every run of neighbours whose float64
+//      error intervals overlap (and which reaches into the first k), order by
+//      the exact integer key (exact.cuh), ties by index.
+// Queries whose lists overflowed go to exact_kernel.
+//
+// Replaces the reference's refine / certify / exact-order passes
+// (src/mlxlearn_device/_neighbors_fused.py:545-834,
+//  _neighbors_shortlist.py:16-170, _neighbors_precision.py:9-259) and its
+// partitioned exact fallback (_neighbors_fallback.py:62-298).
+#include <cfloat>
+
+#include "common.cuh"
+#include "exact.cuh"
+#include "internal.cuh"
+
+namespace b2k {
+
+namespace {
+
+constexpr int kCertWarps = 4;
+
+// |canonical - S| <= g S with g = (d+2)u/(1-(d+2)u), u = 2^-53, for a
+// sequential sum of d non-negative rounded terms (reference
+// src/mlxlearn/_kernels/radius_contract.py:16-25); intervals use 2g.
+__device__ __forceinline__ double interval_g2(int d) {
+  const double u = 0x1p-53;
+  return 2.0 * (double)(d + 2) * u / (1.0 - (double)(d + 2) * u);
+}
+
+__device__ __forceinline__ uint32_t float_key(float f) {
+  uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Ascending (s, id) bitonic sort of P (power of two) entries by one warp.
+__device__ void warp_bitonic(double* s, int* id, int P, int lane) {
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = lane; t < P / 2; t += 32) {
+        const int i = 2 * t - (t & (stride - 1));
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const double a = s[i], b = s[j];
+        const int ia = id[i], ib = id[j];
+        const bool gt = (a > b) || (a == b && ia > ib);
+        if (gt == up) {
+          s[i] = b;
+          s[j] = a;
+          id[i] = ib;
+          id[j] = ia;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Sort C candidates (padded to a power of two P) and fix the order of every
+// near-tie run that starts inside the first k.  Runs only lane 0 for the
+// exact part.  Returns the number of exact comparisons made.
+__device__ unsigned warp_sort_resolve(double* s, int* id, int C, int k, const float* q,
+                                      const float* X, int d, int lane) {
+  int P = 2;
+  while (P < C) P <<= 1;
+  for (int i = C + lane; i < P; i += 32) {
+    s[i] = DBL_MAX;
+    id[i] = INT_MAX;
+  }
+  __syncwarp();
+  warp_bitonic(s, id, P, lane);
+  unsigned compares = 0;
+  if (lane == 0) {
+    const double g2 = interval_g2(d);
+    const double lo_f = 1.0 - g2, hi_f = 1.0 + g2;
+    int i = 0;
+    while (i < k && i < C) {
+      int j = i + 1;
+      while (j < C && __dmul_rd(s[j], lo_f) <= __dmul_ru(s[j - 1], hi_f)) ++j;
+      if (j - i > 1 && s[j - 1] != 0.0) {
+        // exact insertion sort of the run [i, j)
+        for (int a = i + 1; a < j; ++a) {
+          const double sa = s[a];
+          const int ia = id[a];
+          int b = a;
+          while (b > i) {
+            const int ib = id[b - 1];
+            int c = exact_compare(q, X + (size_t)ia * d, X + (size_t)ib * d, d);
+            ++compares;
+            if (c > 0 || (c == 0 && ia > ib)) break;
+            s[b] = s[b - 1];
+            id[b] = ib;
+            --b;
+          }
+          s[b] = sa;
+          id[b] = ia;
+        }
+      }
+      i = j;
+    }
+  }
+  __syncwarp();
+  return compares;
+}
+
+__global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyArgs a) {
+  extern __shared__ uint8_t smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kCertWarps + w;
+  if (row >= a.m) return;
+  double* cs = reinterpret_cast<double*>(smem) + (size_t)w * kCertifyCap;
+  int* ci = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + kCertWarps * kCertifyCap) +
+            (size_t)w * kCertifyCap;
+  const ScreenOut& so = a.scr;
+  const int k = a.k, S = a.S;
+
+  // 1. overflow check
+  bool overflow = false;
+  unsigned entries = 0;
+  for (int s = lane; s < S; s += 32) {
+    int c = so.counts[(size_t)s * so.m_pad + row];
+    overflow |= c > so.cap;
+    entries += c;
+  }
+  overflow = __any_sync(0xffffffffu, overflow);
+  if (overflow) {
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    return;
+  }
+  entries = __reduce_add_sync(0xffffffffu, entries);
+
+  // 2. V_k by bisection over the splits' k smallest values
+  const int total = S * k;
+  uint32_t lo = 0, hi = 0xffffffffu;
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    unsigned cnt = 0;
+    for (int i = lane; i < total; i += 32) {
+      const int s = i / k, t = i % k;
+      cnt += float_key(so.kth[((size_t)s * so.m_pad + row) * k + t]) <= mid;
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if (cnt >= (unsigned)k) hi = mid;
+    else lo = mid + 1;
+  }
+  const float Vk = key_float(lo);
+  const float Tf = __fadd_ru(Vk, __fmul_ru(2.0f, a.E[row]));
+
+  // 3. gather candidates v <= Tf
+  int C = 0;
+  bool too_many = false;
+  for (int s = 0; s < S && !too_many; ++s) {
+    const size_t slot = (size_t)s * so.m_pad + row;
+    const int cnt = so.counts[slot];
+    const int2* lst = so.lists + slot * so.cap;
+    for (int base = 0; base < cnt; base += 32) {
+      const int i = base + lane;
+      bool pass = false;
+      int col = 0;
+      if (i < cnt) {
+        const int2 e = lst[i];
+        pass = __int_as_float(e.x) <= Tf;
+        col = e.y;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, pass);
+      const int pos = C + __popc(bal & ((1u << lane) - 1));
+      if (pass && pos < kCertifyCap) ci[pos] = col;
+      C += __popc(bal);
+      if (C > kCertifyCap) {
+        too_many = true;
+        break;
+      }
+    }
+  }
+  if (too_many || C < k) {
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    return;
+  }
+  __syncwarp();
+  // 4. canonical float64 values
+  const float* q = a.Q + (size_t)row * a.d;
+  for (int c = lane; c < C; c += 32) cs[c] = canonical_d2(q, a.X + (size_t)ci[c] * a.d, a.d);
+  __syncwarp();
+  const unsigned cmp = warp_sort_resolve(cs, ci, C, k, q, a.X, a.d, lane);
+  for (int t = lane; t < k; t += 32) {
+    a.idx[row * k + t] = ci[t];
+    if (a.dist) a.dist[row * k + t] = sqrt(cs[t]);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.counters[0], (unsigned long long)C);
+    atomicAdd(&a.counters[1], (unsigned long long)entries);
+    if (cmp) atomicAdd(&a.counters[2], (unsigned long long)cmp);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exhaustive exact scan: one CTA per query.  Canonical float64 values of all
+// rows, an exact radix select of the k-th smallest value, every row whose
+// error interval reaches it, then the same sort + exact resolution.
+// ---------------------------------------------------------------------------
+constexpr int kExactThreads = 256;
+
+__device__ __forceinline__ double exact_value(const ExactArgs& a, const float* q, int64_t row,
+                                              int64_t j, const double* sc) {
+  if (sc) return sc[j];
+  if (a.exclude_self && j == a.q_offset + row) return INFINITY;
+  return canonical_d2(q, a.X + (size_t)j * a.d, a.d);
+}
+
+__global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a) {
+  extern __shared__ uint8_t smem[];
+  double* cs = reinterpret_cast<double*>(smem);            // [kExactCap]
+  int* ci = reinterpret_cast<int*>(cs + kExactCap);         // [kExactCap]
+  __shared__ unsigned hist[256];
+  __shared__ unsigned long long s_prefix;
+  __shared__ int s_rank, s_count;
+  const int tid = threadIdx.x;
+  const int count = a.rows ? *a.row_count : (int)a.m;
+  double* sc = a.scratch ? a.scratch + (size_t)blockIdx.x * a.n : nullptr;
+  for (int it = blockIdx.x; it < count; it += gridDim.x) {
+    const int64_t row = a.rows ? a.rows[it] : it;
+    const float* q = a.Q + (size_t)row * a.d;
+    if (sc) {
+      for (int64_t j = tid; j < a.n; j += kExactThreads) {
+        sc[j] = (a.exclude_self && j == a.q_offset + row)
+                    ? INFINITY
+                    : canonical_d2(q, a.X + (size_t)j * a.d, a.d);
+      }
+      __syncthreads();
+    }
+    // radix select over the bit patterns of non-negative doubles (monotone)
+    unsigned long long prefix = 0, mask = 0;
+    if (tid == 0) s_rank = a.k;
+    __syncthreads();
+    for (int shift = 56; shift >= 0; shift -= 8) {
+      hist[tid] = 0;
+      __syncthreads();
+      for (int64_t j = tid; j < a.n; j += kExactThreads) {
+        const unsigned long long b = __double_as_longlong(exact_value(a, q, row, j, sc));
+        if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        int r = s_rank;
+        unsigned acc = 0;
+        int dgt = 0;
+        for (; dgt < 256; ++dgt) {
+          if (acc + hist[dgt] >= (unsigned)r) break;
+          acc += hist[dgt];
+        }
+        s_rank = r - (int)acc;
+        s_prefix = prefix | ((unsigned long long)dgt << shift);
+      }
+      __syncthreads();
+      prefix = s_prefix;
+      mask |= 255ull << shift;
+    }
+    const double Vk = __longlong_as_double((long long)prefix);
+    const double g2 = interval_g2(a.d);
+    const double reach = __dmul_ru(Vk, 1.0 + g2);
+    if (tid == 0) s_count = 0;
+    __syncthreads();
+    for (int64_t j = tid; j < a.n; j += kExactThreads) {
+      const double v = exact_value(a, q, row, j, sc);
+      if (v != INFINITY && __dmul_rd(v, 1.0 - g2) <= reach) {
+        const int pos = atomicAdd(&s_count, 1);
+        if (pos < kExactCap) {
+          cs[pos] = v;
+          ci[pos] = (int)j;
+        }
+      }
+    }
+    __syncthreads();
+    const int C = s_count;
+    if (C > kExactCap) {
+      if (tid == 0) atomicCAS(a.status, DEV_OK, DEV_TOO_MANY_TIES);
+    } else if (tid < 32) {
+      const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
+      for (int t = tid; t < a.k; t += 32) {
+        a.idx[row * a.k + t] = ci[t];
+        if (a.dist) a.dist[row * a.k + t] = sqrt(cs[t]);
+      }
+      if (tid == 0) {
+        atomicAdd(&a.counters[3], 1ull);
+        if (cmp) atomicAdd(&a.counters[2], (unsigned long long)cmp);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+void launch_certify(const CertifyArgs& a, cudaStream_t st) {
+  if (a.m <= 0) return;
+  const size_t smem = (size_t)kCertWarps * kCertifyCap * (sizeof(double) + sizeof(int));
+  cudaFuncSetAttribute(certify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned grid = (unsigned)((a.m + kCertWarps - 1) / kCertWarps);
+  certify_kernel<<<grid, kCertWarps * 32, smem, st>>>(a);
+}
+
+void launch_exact(const ExactArgs& a, cudaStream_t st) {
+  if (a.grid <= 0) return;
+  const size_t smem = (size_t)kExactCap * (sizeof(double) + sizeof(int));
+  cudaFuncSetAttribute(exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  exact_kernel<<<a.grid, kExactThreads, smem, st>>>(a);
+}
+
+}  // namespace b2k

@@ -1,0 +1,120 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "../../include/b200knn.h"
+
+namespace b2k {
+
+constexpr int kTcBM = 128;   // query rows per tcgen05 tile (TMEM lanes)
+constexpr int kTcBN = 256;   // reference rows per tcgen05 tile (TMEM columns)
+constexpr int kTcBK = 64;    // 16-bit elements per 128-byte swizzle row
+constexpr int kSimtBM = 128; // query rows per CUDA-core tile
+constexpr int kSimtBN = 128; // reference rows per CUDA-core tile
+constexpr int kListCap = 512;      // screen list entries per (split, query)
+constexpr int kCertifyCap = 1024;  // re-rank candidates per query held in shared memory
+constexpr int kExactCap = 4096;    // exhaustive-scan candidates per query
+constexpr int kMaxK = 64;          // largest k the screens track in registers
+
+// Outputs of a screen kernel: per (split, query) a list of (v, column)
+// candidates, the list length (may exceed cap = overflow), and the k smallest
+// v values the split saw.
+struct ScreenOut {
+  int2* lists;     // [S][m_pad][cap]
+  int* counts;     // [S][m_pad]
+  float* kth;      // [S][m_pad][k]
+  int cap;
+  int m_pad;
+};
+
+// Device-resident index (one per fitted estimator).
+struct Index {
+  int device = 0;
+  int64_t n = 0;
+  int32_t d = 0;
+  float* X = nullptr;        // [n, d] owned float32 copy
+  float* center = nullptr;   // [d] fl32 of the column means (screens work on x - center)
+  double* colsum = nullptr;  // [d] column sums (float64)
+  float* nx32 = nullptr;     // [n] fl32(||x - center||^2)
+  double* nx64 = nullptr;    // [n] ||x - center||^2 in float64
+  // screen statistics (device scalars, then cached on host)
+  float* stats_dev = nullptr;  // [8]: see prep kernels
+  float xn_max = 0, nx_max = 0;  // max ||fp32 operand||, max ||x - center||^2
+  float ex32_max = 0;            // max ||(x - center) - fp32 operand||
+  bool range_ok = false;         // all |x| in {0} U [2^-60, 2^50]
+  // bf16 copy for the tcgen05 screen (lazy)
+  bool bf16_ready = false;
+  int64_t n_pad_tc = 0;          // multiple of kTcBN
+  int32_t dp = 0;                // d padded to a multiple of kTcBK
+  uint16_t* Xh = nullptr;        // [n_pad_tc, dp]
+  float* nxh = nullptr;          // [n_pad_tc] fl32(||x||^2), NaN on padding rows
+  float xh_max = 0, ex_max = 0;  // max ||bf16 operand||, max ||(x - center) - bf16 operand||
+  CUtensorMap tmap_b;            // TMA map over Xh, box 64 x 256
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+};
+
+// ------------------------------------------------------------ prep kernels
+void launch_prep_index(Index* ix, cudaStream_t st);
+void launch_prep_index_bf16(Index* ix, cudaStream_t st);
+// Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
+struct QueryPrep {
+  float* E;        // [m_pad] screen error bound (fp32, rounded up)
+  uint16_t* Ah;    // [m_pad, dp] -2*bf16(q - center) (bf16 mode only)
+  int* flags;      // [1]: bit 0 = some coordinate outside the screen range
+};
+void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
+                         QueryPrep qp, cudaStream_t st);
+
+// ---------------------------------------------------------- screen kernels
+int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad, int k,
+                     int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
+                     int* status, cudaStream_t st);
+void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int k,
+                        int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
+                        cudaStream_t st);
+
+// -------------------------------------------------- certify + re-rank + exact
+struct CertifyArgs {
+  const float* X;
+  const float* Q;
+  int64_t n, m;
+  int d, k, S;
+  ScreenOut scr;
+  const float* E;
+  double* dist;        // [m, k] or null
+  int64_t* idx;        // [m, k]
+  int* fallback_list;  // [m] query ids needing the exhaustive scan
+  int* fallback_count; // [1]
+  unsigned long long* counters;  // [4]: candidates, entries, exact compares, -
+};
+void launch_certify(const CertifyArgs& a, cudaStream_t st);
+
+struct ExactArgs {
+  const float* X;
+  const float* Q;
+  int64_t n, m;
+  int d, k;
+  int exclude_self;
+  int64_t q_offset;
+  const int* rows;      // query ids to process, or null = all rows
+  const int* row_count; // device count for `rows`
+  double* scratch;      // [grid][n]
+  int grid;
+  double* dist;
+  int64_t* idx;
+  unsigned long long* counters;
+  int* status;
+};
+void launch_exact(const ExactArgs& a, cudaStream_t st);
+
+// helpers
+bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                        uint32_t box_inner, uint32_t box_outer);
+int num_sms(int device);
+
+}  // namespace b2k

@@ -1,0 +1,232 @@
+// Index and query preparation kernels.
+//
+// Both screens work on centred coordinates y = x - c (c = fl32 of the mean of
+// the training rows, as the reference centres its Gram screen,
+// src/mlxlearn_device/_neighbors.py:232-239): distances are translation
+// invariant, and centring keeps the Gram cancellation error proportional to
+// the spread of the data instead of its offset.
+//
+// A screen compares v = fl32(||y_x||^2) - 2 <q^, x^> (q^, x^ = the fp32 or
+// bf16 operands of y_q, y_x) against a per-query threshold.  Each query gets
+// a certified bound E with |S(q,x) - (||y_q||^2 + v)| <= E, where S is the
+// exact squared distance, built from norms measured here (the pattern of the
+// reference's compact screen, src/mlxlearn_device/_neighbors_compact.py:83-88,
+// and its Gram lower bound, src/mlxlearn_device/_neighbors_general.py:188-242):
+//
+//   e = y - y^ (operand rounding, measured in float64), u = 2^-24,
+//   E = 2(|q^||e_x| + |e_q||x^| + |e_q||e_x|)      operand rounding
+//     + 2 g |q^||x^|                               dot-product accumulation
+//     + 2u ||y_x||^2 + 2u |q^||x^| (1.01)          stored norm + final add
+//     + 2^-50 ||y_q||^2,  times (1 + 2^-16), plus dp 2^-120 for underflow,
+// with the x-side norms replaced by their maxima over the index and
+//   g = (d + 4) u (1.01)          fp32 FMA chains (CUDA-core screen),
+//   g = (dp + 16) 2^-20           tcgen05 fp32 accumulation (16 ulp per add).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace b2k {
+
+namespace {
+
+// Screen inputs must avoid fp32 overflow of products/norms: every coordinate
+// is 0 or has magnitude in [2^-60, 2^50] (the reference's FP32 Gram screen
+// has the same kind of guard, src/mlxlearn/_kernels/radius_contract.py:46-50).
+__device__ __forceinline__ bool coord_in_range(float v) {
+  uint32_t a = __float_as_uint(v) & 0x7fffffffu;
+  return a == 0 || (a >= (67u << 23) && a <= (177u << 23));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// positive float max via integer atomics (bit patterns of non-negative floats are ordered)
+__device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
+  atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+}
+
+// Column sums of X (float64), accumulated per block then atomically.
+__global__ void column_sum_kernel(const float* __restrict__ X, int64_t n, int d,
+                                  int64_t rows_per_block, double* __restrict__ sums) {
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+  const int64_t r1 = min(n, r0 + rows_per_block);
+  for (int c = threadIdx.x; c < d; c += blockDim.x) {
+    double s = 0.0;
+    for (int64_t r = r0; r < r1; ++r) s += (double)X[r * d + c];
+    atomicAdd(sums + c, s);
+  }
+}
+
+__global__ void center_kernel(const double* __restrict__ sums, int64_t n, int d,
+                              float* __restrict__ center) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < d) center[c] = (float)(sums[c] / (double)n);
+}
+
+// stats: [0] max |x^| fp32 operand, [1] max ||y||^2, [2] range violations (int),
+//        [3] max |x~| bf16 operand, [4] max |e| bf16, [5] max |e| fp32
+__global__ void prep_index_kernel(const float* __restrict__ X, int64_t n, int d,
+                                  const float* __restrict__ center, float* __restrict__ nx32,
+                                  double* __restrict__ nx64, float* __restrict__ stats) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float* x = X + row * d;
+  double yy = 0.0, hh = 0.0, ee = 0.0;
+  bool ok = true;
+  for (int i = lane; i < d; i += 32) {
+    const float v = x[i];
+    ok &= coord_in_range(v);
+    const double y = (double)v - (double)center[i];
+    const float h = v - center[i];  // fp32 operand of the CUDA-core screen
+    const double e = y - (double)h;
+    yy += y * y;
+    hh += (double)h * (double)h;
+    ee += e * e;
+  }
+  yy = warp_sum(yy);
+  hh = warp_sum(hh);
+  ee = warp_sum(ee);
+  ok = __all_sync(0xffffffffu, ok);
+  if (lane == 0) {
+    nx64[row] = yy;
+    nx32[row] = (float)yy;
+    atomic_max_pos(stats + 0, __double2float_ru(sqrt(hh) * (1.0 + 1e-15)));
+    atomic_max_pos(stats + 1, __double2float_ru(yy * (1.0 + 1e-15)));
+    atomic_max_pos(stats + 5, __double2float_ru(sqrt(ee) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy)));
+    if (!ok) atomicAdd(reinterpret_cast<int*>(stats + 2), 1);
+  }
+}
+
+__global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, int d,
+                                       int64_t n_pad, int dp, const float* __restrict__ center,
+                                       const float* __restrict__ nx32,
+                                       __nv_bfloat16* __restrict__ Xh, float* __restrict__ nxh,
+                                       float* __restrict__ stats) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  if (row >= n_pad) return;
+  __nv_bfloat16* xh = Xh + row * dp;
+  if (row >= n) {
+    for (int i = lane; i < dp; i += 32) xh[i] = __float2bfloat16_rn(0.0f);
+    if (lane == 0) nxh[row] = __int_as_float(0x7fc00000);  // NaN: never admitted
+    return;
+  }
+  const float* x = X + row * d;
+  double hn = 0.0, en = 0.0, yy = 0.0;
+  for (int i = lane; i < dp; i += 32) {
+    const float v = i < d ? x[i] : 0.0f;
+    const float c = i < d ? center[i] : 0.0f;
+    const double y = (double)v - (double)c;
+    const __nv_bfloat16 h = __float2bfloat16_rn(v - c);
+    xh[i] = h;
+    const double hv = (double)__bfloat162float(h);
+    const double e = y - hv;
+    hn += hv * hv;
+    en += e * e;
+    yy += y * y;
+  }
+  hn = warp_sum(hn);
+  en = warp_sum(en);
+  yy = warp_sum(yy);
+  if (lane == 0) {
+    nxh[row] = nx32[row];
+    atomic_max_pos(stats + 3, __double2float_ru(sqrt(hn) * (1.0 + 1e-15)));
+    atomic_max_pos(stats + 4, __double2float_ru(sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy)));
+  }
+}
+
+__global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int64_t m_pad,
+                                    int d, int dp, int mode, const float* __restrict__ center,
+                                    float xh_max, float nx_max, float ex_max,
+                                    float* __restrict__ E, __nv_bfloat16* __restrict__ Ah,
+                                    int* __restrict__ flags) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  if (row >= m_pad) return;
+  const double u = 0x1p-24;
+  const bool bf16 = mode == B2K_MODE_BF16;
+  if (row >= m) {
+    if (bf16)
+      for (int i = lane; i < dp; i += 32) Ah[row * dp + i] = __float2bfloat16_rn(0.0f);
+    if (lane == 0) E[row] = 0.0f;
+    return;
+  }
+  const float* q = Q + row * d;
+  double yy = 0.0, hn = 0.0, en = 0.0;
+  bool ok = true;
+  const int width = bf16 ? dp : d;
+  for (int i = lane; i < width; i += 32) {
+    const float v = i < d ? q[i] : 0.0f;
+    const float c = i < d ? center[i] : 0.0f;
+    ok &= coord_in_range(v);
+    const double y = (double)v - (double)c;
+    const float h32 = v - c;
+    double hv;
+    if (bf16) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(h32);
+      hv = (double)__bfloat162float(h);
+      Ah[row * dp + i] = __float2bfloat16_rn(-2.0f * __bfloat162float(h));  // exact
+    } else {
+      hv = (double)h32;
+    }
+    const double e = y - hv;
+    yy += y * y;
+    hn += hv * hv;
+    en += e * e;
+  }
+  yy = warp_sum(yy);
+  hn = warp_sum(hn);
+  en = warp_sum(en);
+  ok = __all_sync(0xffffffffu, ok);
+  if (lane == 0) {
+    const double qh = sqrt(hn) * (1.0 + 1e-15);
+    const double eq = sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy);
+    const double XH = xh_max, EX = ex_max, NX = nx_max;
+    const double g = bf16 ? (double)(dp + 16) * 0x1p-20 : (double)(d + 4) * u * 1.01;
+    double bound = 2.0 * (qh * EX + eq * XH + eq * EX) + 2.0 * g * qh * XH + 2.0 * u * NX +
+                   2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy;
+    bound = bound * (1.0 + 0x1p-16) + (double)width * 0x1p-120;
+    E[row] = __double2float_ru(bound);
+    if (!ok) atomicOr(flags, 1);
+  }
+}
+
+}  // namespace
+
+void launch_prep_index(Index* ix, cudaStream_t st) {
+  const int64_t rows_per_block = 2048;
+  const int64_t blocks = (ix->n + rows_per_block - 1) / rows_per_block;
+  cudaMemsetAsync(ix->colsum, 0, (size_t)ix->d * sizeof(double), st);
+  column_sum_kernel<<<(unsigned)blocks, 128, 0, st>>>(ix->X, ix->n, ix->d, rows_per_block,
+                                                      ix->colsum);
+  center_kernel<<<(ix->d + 127) / 128, 128, 0, st>>>(ix->colsum, ix->n, ix->d, ix->center);
+  const int warps = 8;
+  prep_index_kernel<<<(unsigned)((ix->n + warps - 1) / warps), warps * 32, 0, st>>>(
+      ix->X, ix->n, ix->d, ix->center, ix->nx32, ix->nx64, ix->stats_dev);
+}
+
+void launch_prep_index_bf16(Index* ix, cudaStream_t st) {
+  const int warps = 8;
+  const int64_t blocks = (ix->n_pad_tc + warps - 1) / warps;
+  prep_index_bf16_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
+      ix->X, ix->n, ix->d, ix->n_pad_tc, ix->dp, ix->center, ix->nx32,
+      reinterpret_cast<__nv_bfloat16*>(ix->Xh), ix->nxh, ix->stats_dev);
+}
+
+void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
+                         QueryPrep qp, cudaStream_t st) {
+  const int warps = 8;
+  const int64_t blocks = (m_pad + warps - 1) / warps;
+  if (blocks == 0) return;
+  const bool bf16 = mode == B2K_MODE_BF16;
+  prep_queries_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
+      Q, m, m_pad, ix->d, ix->dp, mode, ix->center, bf16 ? ix->xh_max : ix->xn_max, ix->nx_max,
+      bf16 ? ix->ex_max : ix->ex32_max, qp.E, reinterpret_cast<__nv_bfloat16*>(qp.Ah), qp.flags);
+}
+
+}  // namespace b2k

@@ -1,0 +1,350 @@
+// bf16 distance screen on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Replaces the reference's Gram screens (src/mlxlearn_device/_neighbors_general.py:188-329,
+// the fp16 compact screen _neighbors_compact.py:20-371 and the int8 MPP
+// screen _neighbors_integer.py:40-201), which materialise the distance tile in
+// memory.  Here the tile lives only in TMEM.
+//
+// One persistent CTA per SM, warp-specialised:
+//   warp 0      TMA producer: query tile A (128 rows x dp, bf16, -2*q) once
+//               per work unit; reference tiles B (256 rows x 64 cols) into an
+//               NST-deep shared-memory ring (128-byte swizzle).
+//   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16,
+//               fp32 accumulators in TMEM, double-buffered (2 x 256 columns).
+//   warps 2..5  epilogue: tcgen05.ld 32 columns at a time (two loads in
+//               flight), add ||x||^2 (staged per tile in shared memory, the
+//               next tile's norms prefetched), 3-input min over the chunk,
+//               and only when the minimum passes the row's threshold, admit
+//               columns to the candidate list (tracker.cuh).  The accumulator
+//               is handed back to the MMA warp as soon as its last chunk is in
+//               registers.  The 128 x 256 distance tile never reaches HBM.
+// A work unit is (query tile of 128 rows, split s of the reference tiles);
+// units are dealt round-robin over the persistent CTAs.
+//
+// Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
+// B = bf16(x - c)); the certified error bound of v = fl32(acc + ||x - c||^2) is
+// derived in prep.cu with g = (dp + 16) 2^-20 for the tensor-core fp32
+// accumulation.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "internal.cuh"
+#include "tracker.cuh"
+
+namespace b2k {
+
+namespace {
+
+struct TcParams {
+  int m, KB, n_tiles, S, tiles_per_split, m_tiles, k, exclude_self, stages;
+  long long q_offset;
+  const float* nx;  // [n_pad_tc], NaN on padding rows
+  const float* E;   // [m_pad]
+  ScreenOut out;
+  int* status;
+};
+
+constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;  // 16 KB per 64-column block
+constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;  // 32 KB per 64-column block
+constexpr int kThreads = 192;
+constexpr int kSpillStride = 33;
+
+__host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream) {
+  size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
+  size_t stage = a_stream ? kATileBytes + kBTileBytes : kBTileBytes;
+  size_t spill = 128 * kSpillStride * sizeof(float);
+  size_t nx = 2 * kTcBN * sizeof(float);
+  size_t bars = (2 * (size_t)stages + 6) * sizeof(uint64_t) + 16;
+  return 1024 /*alignment slack*/ + a + stage * stages + spill + nx + bars;
+}
+
+template <int KMAX, bool A_STREAM>
+__global__ void __launch_bounds__(kThreads, 1)
+    screen_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+                     const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int KB = p.KB;
+  const int nst = p.stages;
+  uint8_t* a_smem = smem;
+  uint8_t* b_smem = smem + (A_STREAM ? 0 : KB * kATileBytes);
+  const uint32_t stage_bytes = A_STREAM ? kATileBytes + kBTileBytes : kBTileBytes;
+  float* spill_all = reinterpret_cast<float*>(b_smem + (size_t)nst * stage_bytes);
+  float* nx_all = spill_all + 128 * kSpillStride;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(nx_all + 2 * kTcBN);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + nst;
+  uint64_t* a_full = bars + 2 * nst;
+  uint64_t* a_empty = a_full + 1;
+  uint64_t* acc_full = a_empty + 1;   // [2]
+  uint64_t* acc_empty = acc_full + 2; // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  volatile int* status = p.status;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nst; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(a_full, 1);
+    mbar_init(a_empty, 1);
+    mbar_init(&acc_full[0], 1);
+    mbar_init(&acc_full[1], 1);
+    mbar_init(&acc_empty[0], 128);
+    mbar_init(&acc_empty[1], 128);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int total_units = p.m_tiles * p.S;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      prefetch_tmap(&tmA);
+      prefetch_tmap(&tmB);
+      uint32_t stage = 0, phase = 0, a_phase = 0;
+      for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
+        const int t = u / p.S, s = u % p.S;
+        const int j0 = s * p.tiles_per_split;
+        const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+        if (!A_STREAM) {
+          if (!mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A)) goto prod_done;
+          a_phase ^= 1;
+          mbar_arrive_expect_tx(a_full, KB * kATileBytes);
+          for (int kb = 0; kb < KB; ++kb)
+            tma_load_2d(a_smem + kb * kATileBytes, &tmA, a_full, kb * kTcBK, t * kTcBM);
+        }
+        for (int j = j0; j < j1; ++j) {
+          for (int kb = 0; kb < KB; ++kb) {
+            if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) goto prod_done;
+            uint8_t* st = b_smem + (size_t)stage * stage_bytes;
+            if (A_STREAM) {
+              mbar_arrive_expect_tx(&full[stage], kATileBytes + kBTileBytes);
+              tma_load_2d(st, &tmA, &full[stage], kb * kTcBK, t * kTcBM);
+              tma_load_2d(st + kATileBytes, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
+            } else {
+              mbar_arrive_expect_tx(&full[stage], kBTileBytes);
+              tma_load_2d(st, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
+            }
+            if (++stage == (uint32_t)nst) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+      }
+      // Drain: wait until the consumer released every stage we filled, so no
+      // bulk copy is still in flight when the CTA exits.
+      for (int s = 0; s < nst; ++s) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) break;
+        if (++stage == (uint32_t)nst) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+    prod_done:;
+    }
+  } else if (warp == 1) {
+    // --------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
+      uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0;
+      for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
+        const int s = u % p.S;
+        const int j0 = s * p.tiles_per_split;
+        const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+        if (!A_STREAM) {
+          if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto mma_done;
+          a_phase ^= 1;
+          tc_fence_after();
+        }
+        for (int j = j0; j < j1; ++j) {
+          const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
+          if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto mma_done;
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + buf * kTcBN;
+          for (int kb = 0; kb < KB; ++kb) {
+            if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto mma_done;
+            tc_fence_after();
+            uint8_t* st = b_smem + (size_t)stage * stage_bytes;
+            const uint8_t* a_tile = A_STREAM ? st : a_smem + kb * kATileBytes;
+            const uint8_t* b_tile = A_STREAM ? st + kATileBytes : st;
+            const uint64_t adesc = smem_desc_sw128(a_tile);
+            const uint64_t bdesc = smem_desc_sw128(b_tile);
+#pragma unroll
+            for (int kk = 0; kk < kTcBK / 16; ++kk) {
+              // advance 16 bf16 = 32 bytes inside the swizzle atom: +2 in 16-byte units
+              mma_f16(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, idesc, (kb | kk) != 0);
+            }
+            mma_commit(&empty[stage]);
+            if (++stage == (uint32_t)nst) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+          mma_commit(&acc_full[buf]);
+          ++acc_it;
+        }
+        // Release the query tile for the next unit (not after the last one, so
+        // no arrival can land after the CTA has exited).
+        if (!A_STREAM && u + (int)gridDim.x < total_units) mma_commit(a_empty);
+      }
+    mma_done:;
+    }
+  } else {
+    // ----------------------------------------------------------- epilogue
+    const int g = warp & 3;                 // TMEM lane group this warp may access
+    const int row_in_tile = g * 32 + lane;
+    const int et = threadIdx.x - 64;        // 0..127
+    float* spill = spill_all + et * kSpillStride;
+    float* nx_smem = nx_all;                // [2][kTcBN] column norms of the current / next tile
+    uint32_t acc_it = 0;
+    for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
+      const int t = u / p.S, s = u % p.S;
+      const int j0 = s * p.tiles_per_split;
+      const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+      const int row = t * kTcBM + row_in_tile;
+      const bool valid = row < p.m;
+      RowTracker<KMAX> tr;
+      const size_t slot = (size_t)s * p.out.m_pad + row;
+      tr.init(p.k, valid ? p.E[row] : 0.0f,
+              p.exclude_self ? (int)(p.q_offset + row) : -1,
+              p.out.lists + slot * p.out.cap, p.out.cap);
+      // column norms of the unit's first tile
+      {
+        const float2 nn = __ldg(reinterpret_cast<const float2*>(p.nx + (size_t)j0 * kTcBN) + et);
+        reinterpret_cast<float2*>(nx_smem)[et] = nn;
+      }
+      named_bar_sync(1, 128);
+      int nb = 0;
+      for (int j = j0; j < j1; ++j) {
+        // prefetch the next tile's norms; they land in smem after this tile
+        float2 nn_next = make_float2(0.f, 0.f);
+        if (j + 1 < j1)
+          nn_next = __ldg(reinterpret_cast<const float2*>(p.nx + (size_t)(j + 1) * kTcBN) + et);
+        const float* nxs = nx_smem + nb * kTcBN;
+        const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
+        if (!mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)) goto epi_done;
+        tc_fence_after();
+        const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN;
+        auto process = [&](const uint32_t(&r)[32], int c) {
+          const float4* np = reinterpret_cast<const float4*>(nxs + c * 32);
+          float v[32];
+#pragma unroll
+          for (int q4 = 0; q4 < 8; ++q4) {
+            const float4 nn = np[q4];
+            float a0 = __uint_as_float(r[4 * q4]), a1 = __uint_as_float(r[4 * q4 + 1]);
+            float a2 = __uint_as_float(r[4 * q4 + 2]), a3 = __uint_as_float(r[4 * q4 + 3]);
+            add_f32x2(a0, a1, nn.x, nn.y);
+            add_f32x2(a2, a3, nn.z, nn.w);
+            v[4 * q4] = a0;
+            v[4 * q4 + 1] = a1;
+            v[4 * q4 + 2] = a2;
+            v[4 * q4 + 3] = a3;
+          }
+          if (valid) tr.offer32(v, j * kTcBN + c * 32, spill);
+        };
+        // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
+        uint32_t ra[32], rb[32];
+        tmem_ld_32x32b_x32(tbase, ra);
+        tmem_ld_wait_regs(ra);
+#pragma unroll 1
+        for (int c = 0; c < kTcBN / 32; c += 2) {
+          tmem_ld_32x32b_x32(tbase + (c + 1) * 32, rb);
+          process(ra, c);
+          tmem_ld_wait_regs(rb);
+          if (c + 2 < kTcBN / 32) {
+            tmem_ld_32x32b_x32(tbase + (c + 2) * 32, ra);
+            process(rb, c + 1);
+            tmem_ld_wait_regs(ra);
+          } else {
+            // every column of this accumulator is in registers: hand it back
+            tc_fence_before();
+            mbar_arrive(&acc_empty[buf]);
+            process(rb, c + 1);
+          }
+        }
+        ++acc_it;
+        reinterpret_cast<float2*>(nx_smem + (nb ^ 1) * kTcBN)[et] = nn_next;
+        named_bar_sync(1, 128);
+        nb ^= 1;
+      }
+      if (valid) {
+        p.out.counts[slot] = tr.cnt;
+        tr.write_kth(p.out.kth + slot * p.k, p.k);
+      }
+    }
+  epi_done:;
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+template <int KMAX, bool A_STREAM>
+int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcParams& p, int grid,
+                      size_t smem, cudaStream_t st) {
+  auto kern = screen_tc_kernel<KMAX, A_STREAM>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return (int)e;
+  kern<<<grid, kThreads, smem, st>>>(*ta, *tb, p);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad, int k,
+                     int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
+                     int* status, cudaStream_t st) {
+  TcParams p{};
+  p.m = (int)m;
+  p.KB = ix->dp / kTcBK;
+  p.n_tiles = (int)(ix->n_pad_tc / kTcBN);
+  p.S = S;
+  p.tiles_per_split = (p.n_tiles + S - 1) / S;
+  p.m_tiles = (int)(m_pad / kTcBM);
+  p.k = k;
+  p.exclude_self = exclude_self;
+  p.q_offset = q_offset;
+  p.nx = ix->nxh;
+  p.E = E;
+  p.out = out;
+  p.status = status;
+  const bool a_stream = p.KB > 4;
+  const size_t budget = 227 * 1024;
+  int stages = 8;
+  while (stages > 2 && tc_smem_bytes(p.KB, stages, a_stream) > budget) --stages;
+  p.stages = stages;
+  size_t smem = tc_smem_bytes(p.KB, stages, a_stream);
+  int units = p.m_tiles * S;
+  int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
+  if (grid <= 0) return 0;
+  if (k <= 16) {
+    return a_stream ? launch_tc_variant<16, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
+                    : launch_tc_variant<16, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
+  } else if (k <= 32) {
+    return a_stream ? launch_tc_variant<32, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
+                    : launch_tc_variant<32, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
+  }
+  return a_stream ? launch_tc_variant<64, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
+                  : launch_tc_variant<64, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
+}
+
+}  // namespace b2k

@@ -1,0 +1,187 @@
+"""The drop-in seam: ``NeighborIndex`` / ``build_index`` on the CUDA library.
+
+Mirrors ``mlxlearn._kernels.distance.NeighborIndex`` (reference
+src/mlxlearn/_kernels/distance.py:66-392): the estimators call only
+``build_index`` and the index methods below, and get back float64 distances
+and int64 indices in ``(distance, index)`` order.  Every query runs on the
+GPU through libb200knn.so; there is no CPU route.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["NeighborIndex", "build_index"]
+
+NUMPY_FLOAT = np.float32
+INDEX_DTYPE = np.int64
+
+
+def _as_f32_c(X) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(X, dtype=NUMPY_FLOAT))
+
+
+class NeighborIndex:
+    """Owned training rows plus a device-resident search index.
+
+    The host float32 copy serves pickling and ``training_data``; the device
+    copy (created lazily on first use, or eagerly by ``build_index``) is the
+    only thing searched.
+    """
+
+    def __init__(self, X: np.ndarray, *, device: int = 0, mode: str = "auto"):
+        if X.ndim != 2 or 0 in X.shape:
+            raise ValueError("X must be a nonempty two-dimensional matrix")
+        if X.shape[0] >= 2**31:
+            raise ValueError("training row count must fit int32 indices")
+        self._host_X = X
+        self.device = int(device)
+        self.mode = mode
+        self._handle = None
+        self._lock = threading.Lock()
+        self.last_query_backend = None
+        self.last_stats = None
+
+    # ------------------------------------------------------------ lifetime
+    def _ensure_device(self):
+        if self._handle is None:
+            with self._lock:
+                if self._handle is None:
+                    lib = _lib.load()
+                    h = ctypes.c_void_p()
+                    X = self._host_X
+                    _lib.check(lib.b2k_index_create(X.ctypes.data, X.shape[0], X.shape[1],
+                                                    self.device, ctypes.byref(h)),
+                               "b2k_index_create")
+                    self._handle = h
+        return self._handle
+
+    def close(self):
+        if self._handle is not None and _lib._lib is not None:
+            _lib._lib.b2k_index_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __getstate__(self):
+        # Host rows and parameters only; the device index is rebuilt lazily
+        # (reference distance.py:191-209).
+        return {"X": self._host_X, "device": self.device, "mode": self.mode}
+
+    def __setstate__(self, state):
+        self.__init__(state["X"], device=state.get("device", 0), mode=state.get("mode", "auto"))
+
+    # ----------------------------------------------------------- properties
+    @property
+    def training_data(self) -> np.ndarray:
+        return self._host_X
+
+    @property
+    def X(self) -> np.ndarray:
+        return self._host_X
+
+    @property
+    def n_samples(self) -> int:
+        return int(self._host_X.shape[0])
+
+    @property
+    def n_features(self) -> int:
+        return int(self._host_X.shape[1])
+
+    # -------------------------------------------------------------- queries
+    def _check_query(self, n_query: int, k: int, exclude_self: bool):
+        limit = self.n_samples - int(bool(exclude_self))
+        if k > limit:
+            raise ValueError(f"n_neighbors must be <= {limit}, got {k}.")
+        if exclude_self and n_query != self.n_samples:
+            raise ValueError(
+                "exclude_self requires the query matrix to be the training matrix: "
+                f"got {n_query} query rows and {self.n_samples} training rows.")
+
+    def query(self, Q, k, *, return_distance=True, exclude_self=False,
+              query_block_size=None, train_block_size=None, mode=None, stats=False):
+        """Float64 distances (or None) and int64 indices, each ``[n_query, k]``.
+
+        ``query_block_size`` splits the queries into independent batches;
+        results do not depend on it.  ``train_block_size`` is accepted for
+        compatibility: the engine tiles the training rows itself and its
+        merge is exact, so blocking never changes an answer.
+        """
+        Q = _as_f32_c(Q)
+        k = int(k)
+        if Q.ndim != 2 or Q.shape[1] != self.n_features:
+            raise ValueError(f"Q must have shape (n, {self.n_features})")
+        m = Q.shape[0]
+        self._check_query(m, k, exclude_self)
+        idx = np.empty((m, k), dtype=INDEX_DTYPE)
+        dist = np.empty((m, k), dtype=np.float64) if return_distance else None
+        if m:
+            h = self._ensure_device()
+            lib = _lib.load()
+            code = _lib.MODES[mode or self.mode]
+            st = _lib.Stats()
+            step = m if not query_block_size else max(1, int(query_block_size))
+            for start in range(0, m, step):
+                stop = min(m, start + step)
+                rc = lib.b2k_knn(h, Q[start:stop].ctypes.data, stop - start, k,
+                                 int(bool(exclude_self)), start, code,
+                                 None if dist is None else dist[start:stop].ctypes.data,
+                                 idx[start:stop].ctypes.data, ctypes.byref(st) if stats else None)
+                _lib.check(rc, "b2k_knn")
+            self.last_stats = st.as_dict() if stats else None
+        self.last_query_backend = "cuda"
+        return dist, idx
+
+    def query_device(self, Q, k, *, return_distance=True, exclude_self=False, q_offset=0,
+                     mode=None, stats=False, stream=None):
+        """Device-resident query: ``Q`` is a CUDA float32 tensor ``[m, d]``.
+
+        Returns torch tensors on the same device (float64 distances or None,
+        int64 indices), computed on the current torch stream.
+        """
+        import torch
+
+        if not (isinstance(Q, torch.Tensor) and Q.is_cuda):
+            raise TypeError("query_device expects a CUDA tensor")
+        Q = Q.detach().to(torch.float32).contiguous()
+        m, k = int(Q.shape[0]), int(k)
+        if exclude_self:
+            limit = self.n_samples - 1
+            if k > limit:
+                raise ValueError(f"n_neighbors must be <= {limit}, got {k}.")
+        elif k > self.n_samples:
+            raise ValueError(f"n_neighbors must be <= {self.n_samples}, got {k}.")
+        idx = torch.empty((m, k), dtype=torch.int64, device=Q.device)
+        dist = torch.empty((m, k), dtype=torch.float64, device=Q.device) if return_distance else None
+        if m:
+            h = self._ensure_device()
+            st = _lib.Stats()
+            s = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
+            rc = _lib.load().b2k_knn_device(
+                h, Q.data_ptr(), m, k, int(bool(exclude_self)), int(q_offset),
+                _lib.MODES[mode or self.mode], None if dist is None else dist.data_ptr(),
+                idx.data_ptr(), s, ctypes.byref(st) if stats else None)
+            _lib.check(rc, "b2k_knn_device")
+            self.last_stats = st.as_dict() if stats else None
+        self.last_query_backend = "cuda"
+        return dist, idx
+
+
+def build_index(X, *, backend: str = "cuda", _owned: bool = False, device: int = 0,
+                mode: str = "auto") -> NeighborIndex:
+    """Own a float32 C-order copy of ``X`` (never alias a caller's array).
+
+    ``backend`` is accepted for signature compatibility with the reference
+    (distance.py:366-392); every backend name runs on the CUDA library.
+    """
+    Xf = (np.ascontiguousarray(np.asarray(X, dtype=NUMPY_FLOAT)) if _owned
+          else np.array(X, dtype=NUMPY_FLOAT, order="C", copy=True))
+    return NeighborIndex(Xf, device=device, mode=mode)

@@ -1,0 +1,202 @@
+"""kNN parity of the CUDA library against the oracle and the reference's outputs.
+
+Indices must be bit-exact.  Distances are checked two ways: bit-exact against
+the oracle's canonical float64 value, and within atol=rtol=1e-6 of the
+reference's own outputs (the tolerance of its parity helper,
+tests/_helpers.py:73-120 of mlx-learn).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+from datasets import cfg1, mixture, pixels
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["bf16", "fp32", "exact"]
+
+
+def make_index(X, **kw):
+    from mlxlearn_b200.index import build_index
+
+    return build_index(X, **kw)
+
+
+def check(dist, idx, ref_dist, ref_idx, *, exact_dist=None):
+    np.testing.assert_array_equal(idx, ref_idx)
+    np.testing.assert_allclose(dist, ref_dist, rtol=1e-6, atol=1e-6)
+    if exact_dist is not None:
+        np.testing.assert_array_equal(dist, exact_dist)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_cfg1_matches_reference_and_oracle(mode):
+    X, Q = cfg1()
+    g = golden("knn_cfg1.npz")
+    od, oi = oracle.knn(X, Q, 5)
+    dist, idx = make_index(X).query(Q, 5, mode=mode)
+    check(dist, idx, g["dist"], g["idx"], exact_dist=od)
+    assert dist.dtype == np.float64 and idx.dtype == np.int64
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_self_query_with_duplicates(mode):
+    X, _ = cfg1()
+    Xs = X[:3000].copy()
+    Xs[100:130] = Xs[:30]
+    g = golden("knn_self_dups.npz")
+    dist, idx = make_index(Xs).query(Xs, 7, exclude_self=True, mode=mode)
+    check(dist, idx, g["dist"], g["idx"])
+    assert not np.any(idx == np.arange(len(Xs))[:, None])
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_mixture128_subset(mode):
+    C = np.random.default_rng(2).uniform(-1, 1, (1024, 128))
+    X, _ = mixture(np.random.default_rng(2), 50000, C, 0.1)
+    Q, _ = mixture(np.random.default_rng(3), 256, C, 0.1)
+    g = golden("knn_mixture128.npz")
+    index = make_index(X)
+    dist, idx = index.query(Q, 10, mode=mode, stats=True)
+    check(dist, idx, g["dist"], g["idx"])
+    st = index.last_stats
+    assert st["fallback_rows"] == 0, st
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_pixels784_subset(mode):
+    rng = np.random.default_rng(7)
+    X, y, T = pixels(rng, 8000)
+    Q, _, _ = pixels(rng, 200, templates=T)
+    g = golden("knn_pixels784.npz")
+    dist, idx = make_index(X).query(Q, 5, mode=mode)
+    check(dist, idx, g["dist"], g["idx"])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_ties_break_on_training_index(mode):
+    X = np.array([[1.0], [1.0], [1.0], [2.0]], dtype=np.float32)
+    dist, idx = make_index(X).query(np.array([[0.0]], dtype=np.float32), 3, mode=mode)
+    np.testing.assert_array_equal(idx, [[0, 1, 2]])
+    np.testing.assert_allclose(dist, [[1.0, 1.0, 1.0]])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_offset_seed251_exact_order(mode):
+    """Rows 1902 and 43153: float32 squared distances round equal, exact order differs
+    (reference tests/unit/test_neighbors_precision.py:42-92)."""
+    rng = np.random.default_rng(251)
+    train = (rng.normal(size=(50_000, 32)) + 10_000).astype(np.float32)
+    queries = (rng.normal(size=(256, 32)) + 10_000).astype(np.float32)
+    q = queries[79:80]
+    sub = train[[1902, 43153]]
+    _, i2 = make_index(sub).query(q, 2, mode=mode)
+    np.testing.assert_array_equal(i2, [[1, 0]])
+    od, oi = oracle.knn(train, np.repeat(q, 65, axis=0), 5)
+    assert oi[0, 3] == 43153 and oi[0, 4] == 1902
+    dist, idx = make_index(train).query(np.repeat(q, 65, axis=0), 5, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_equal_distances_choose_smallest_indices(mode):
+    train = np.zeros((8, 32), dtype=np.float32)
+    train[:4, :2] = [[1, 0], [-1, 0], [0, 1], [0, -1]]
+    train[4:, 0] = 2
+    query = np.zeros((1, 32), dtype=np.float32)
+    for k in (1, 3):
+        dist, idx = make_index(train).query(query, k, mode=mode)
+        np.testing.assert_array_equal(idx, np.arange(k)[None, :])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_monotone_copied_rows(mode):
+    train = np.arange(8192 * 32, dtype=np.float32).reshape(8192, 32)
+    queries = train[[0, 3, 4, 4096, 8191]].copy()
+    od, oi = oracle.knn(train, queries, 5)
+    dist, idx = make_index(train).query(queries, 5, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(idx[:, 0], [0, 3, 4, 4096, 8191])
+    np.testing.assert_array_equal(dist[:, 0], 0)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n,d,m,k", [(512, 16, 31, 7), (5000, 24, 96, 9), (300, 12, 16, 64),
+                                     (40, 3, 40, 1), (3000, 130, 257, 33), (1000, 700, 19, 5)])
+def test_random_shapes_match_oracle(mode, n, d, m, k, rng):
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    Q = rng.normal(size=(m, d)).astype(np.float32)
+    od, oi = oracle.knn(X, Q, k)
+    dist, idx = make_index(X).query(Q, k, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_lattice_ties_and_duplicates(mode, rng):
+    """Integer lattice points: many exactly equal distances with different coordinates."""
+    X = rng.integers(-3, 4, size=(6000, 8)).astype(np.float32)
+    Q = rng.integers(-3, 4, size=(300, 8)).astype(np.float32) + 0.5
+    od, oi = oracle.knn(X, Q, 20)
+    dist, idx = make_index(X).query(Q, 20, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+
+
+def test_empty_query_and_k_limits(rng):
+    X = rng.normal(size=(20, 3)).astype(np.float32)
+    index = make_index(X)
+    dist, idx = index.query(np.empty((0, 3), np.float32), 4)
+    assert idx.shape == (0, 4) and dist.shape == (0, 4)
+    X6 = rng.normal(size=(6, 3)).astype(np.float32)
+    i6 = make_index(X6)
+    with pytest.raises(ValueError, match="n_neighbors must be <= 6"):
+        i6.query(X6, 7)
+    with pytest.raises(ValueError, match="n_neighbors must be <= 5"):
+        i6.query(X6, 6, exclude_self=True)
+
+
+def test_blocking_is_invariant(rng):
+    X = rng.normal(size=(300, 5)).astype(np.float32)
+    Q = rng.normal(size=(37, 5)).astype(np.float32)
+    index = make_index(X)
+    ref = index.query(Q, 4)
+    for qb in (1, 2, 7, 8, 37):
+        d, i = index.query(Q, 4, query_block_size=qb)
+        np.testing.assert_array_equal(i, ref[1])
+        np.testing.assert_array_equal(d, ref[0])
+
+
+def test_repeat_calls_bitwise_identical(rng):
+    X = rng.normal(size=(20000, 48)).astype(np.float32)
+    Q = rng.normal(size=(500, 48)).astype(np.float32)
+    index = make_index(X)
+    a = index.query(Q, 10)
+    b = index.query(Q, 10)
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[0], b[0])
+
+
+def test_index_owns_its_copy(rng):
+    X = rng.normal(size=(500, 8)).astype(np.float32)
+    Q = rng.normal(size=(20, 8)).astype(np.float32)
+    index = make_index(X)
+    before = index.query(Q, 3)
+    X[:] = 0
+    after = index.query(Q, 3)
+    np.testing.assert_array_equal(before[1], after[1])
+
+
+def test_device_query_matches_host(rng):
+    import torch
+
+    X = rng.normal(size=(4000, 64)).astype(np.float32)
+    Q = rng.normal(size=(300, 64)).astype(np.float32)
+    index = make_index(X)
+    hd, hi = index.query(Q, 8)
+    dd, di = index.query_device(torch.from_numpy(Q).cuda(), 8)
+    np.testing.assert_array_equal(di.cpu().numpy(), hi)
+    np.testing.assert_array_equal(dd.cpu().numpy(), hd)
