@@ -1,0 +1,331 @@
+"""Benchmark: exact kNN queries/s at 1M x 128 reference rows, 100k queries, k=10.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = kneighbors of the whole 100,000-query batch against the fitted
+1,000,000 x 128 float32 index (Gaussian mixture: 1,024 centres uniform in
+[-1,1]^128, sigma 0.1; reference rows seed 2, queries seed 3), k = 10.  The
+headline `value` is the bf16-screen + certified re-rank form with inputs
+resident in HBM; the plain fp32 form is measured in the same run
+(`plain_fp32`).  `e2e` goes through the public host API with pinned host
+buffers (query upload and result download inside the timed region).
+
+Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
+index and answers its own 100,000 queries (weak scaling, no collective on the
+data path); time is the max over ranks.
+
+--impl reference times the reference's own CPU implementation of this path
+(mlxlearn's exact native scan, compiled from the reference sources into
+oracle/_ref) on the host cores, on bounded query samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "tests"))
+
+METRIC = ("exact kNN queries/s at 1M×128 k=10: BF16-screen+certified vs FP32; % TC peak")
+N_REF, N_QUERY, D, K = 1_000_000, 100_000, 128, 10
+WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["bf16_tflops"], p["bf16_tflops_sustained"], p["hbm_gbs"], "measured"
+    except Exception:
+        return 1590.0, 1400.0, 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_time(X, Q, sample, threads, k=K):
+    """Time the reference's own exact CPU kNN scan (oracle/_ref) on a query sample.
+
+    Returns (queries/s, results (dist, idx), kind, cores).
+    """
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+
+    ref = oracle.ref_native()
+    Qs = np.ascontiguousarray(Q[:sample])
+    dist = np.empty((sample, k), np.float64)
+    idx = np.empty((sample, k), np.int64)
+    if ref is not None:
+        kind = "reference"
+        chunks = np.array_split(np.arange(sample), threads)
+
+        def run(rows):
+            if len(rows):
+                a, b = rows[0], rows[-1] + 1
+                # reference: src/mlxlearn/_kernels/_neighbors_cpu_native.cpp:362-418 (GIL released)
+                ref.neighbors.query(X, Qs[a:b], k, False, 0, dist[a:b], idx[a:b])
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(run, chunks))
+        el = time.perf_counter() - t0
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        dist, idx = oracle.knn(X, Qs, k, nthreads=threads)
+        el = time.perf_counter() - t0
+    return sample / el, (dist, idx), kind
+
+
+def run_reference_arm(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from datasets import cfg2a
+
+    X, Q = cfg2a(N_REF, N_QUERY, D)
+    threads = os.cpu_count() or 1
+    sample = max(threads, int(os.environ.get("B2K_REF_SAMPLE", "0")) or threads * 2)
+    vals = []
+    kind = "reference"
+    for step in range(args.warmup + args.steps):
+        qps, _, kind = cpu_reference_time(X, Q[(step * sample) % N_QUERY:], sample, threads)
+        if step >= args.warmup:
+            vals.append(qps)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * N_QUERY / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_ref": N_REF, "d": D, "n_query": N_QUERY, "k": K},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} queries per step of the {N_QUERY}-query batch; "
+                                   "ms_per_step extrapolates to the full batch"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    from datasets import cfg2a
+    from mlxlearn_b200 import _lib
+    from mlxlearn_b200.index import build_index
+
+    X, _ = cfg2a(N_REF, 1, D)
+    # each rank answers its own query shard (weak scaling)
+    from datasets import mixture
+
+    C = np.random.default_rng(2).uniform(-1, 1, (1024, D))
+    Q, _ = mixture(np.random.default_rng(3 + 1000 * rank), N_QUERY, C, 0.1)
+    index = build_index(X, device=local)
+    index._ensure_device()
+    Qd = torch.from_numpy(Q).cuda()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def timed(mode, steps, warmup):
+        stats = []
+        for _ in range(warmup):
+            index.query_device(Qd, K, mode=mode)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            index.query_device(Qd, K, mode=mode, stats=True)
+            stats.append(index.last_stats)
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1) / steps
+        if pg is not None:
+            t = torch.tensor([ms], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, stats
+
+    with ClockSampler(local) as clk:
+        ms_bf16, st_bf16 = timed("bf16", args.steps, args.warmup)
+    clocks = clk.summary()
+    ms_fp32, st_fp32 = timed("fp32", max(1, min(2, args.steps)), 1)
+
+    # e2e: public host API, pinned host buffers, copies inside the timed region
+    Qh = torch.from_numpy(Q).pin_memory().numpy()
+    out_i = torch.empty((N_QUERY, K), dtype=torch.int64).pin_memory().numpy()
+    out_d = torch.empty((N_QUERY, K), dtype=torch.float64).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        index.query(Qh, K, mode="bf16", out=(out_d, out_i))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        index.query(Qh, K, mode="bf16", out=(out_d, out_i))
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if pg is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    result = None
+    if rank == 0:
+        tf_burst, tf_sust, hbm, peak_kind = peaks()
+        flops = 2.0 * N_REF * D * N_QUERY
+        screen_ms = statistics.median(s["screen_ms"] for s in st_bf16)
+        achieved = flops / (screen_ms * 1e-3) / 1e12
+        total_timed_s = ms_bf16 * args.steps / 1000.0
+        peak = tf_sust if total_timed_s > 1.0 else tf_burst
+        fp32_screen_ms = statistics.median(s["screen_ms"] for s in st_fp32)
+        traffic = os.environ.get("B2K_SCREEN_TRAFFIC_BYTES")
+        result = {
+            "metric": METRIC,
+            "value": ws * N_QUERY / (ms_bf16 / 1000.0),
+            "unit": "queries/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_bf16,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16",
+            "data": "synthetic: Gaussian mixture (1024 centres U[-1,1]^128, sigma 0.1), "
+                    "seeds 2/3",
+            "config": {"workload": WORKLOAD, "n_ref": N_REF, "d": D, "n_query": N_QUERY, "k": K,
+                       "queries_per_gpu": N_QUERY, "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (bf16 index 256 MB, fp32 index 512 MB)"},
+            "roofline": {"kernel": "screen_tc_kernel (bf16 tcgen05 distance tile)",
+                         "bound": "tensor", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} "
+                                        f"{'sustained' if peak == tf_sust else 'burst'} bf16",
+                         "algorithmic_flops_per_launch": flops,
+                         "traffic": None if traffic is None else float(traffic)},
+            "plain_fp32": {"value": ws * N_QUERY / (ms_fp32 / 1000.0), "unit": "queries/s",
+                           "ms_per_step": ms_fp32, "screen_ms": fp32_screen_ms,
+                           "screen_tflops": flops / (fp32_screen_ms * 1e-3) / 1e12,
+                           "bf16_speedup": ms_fp32 / ms_bf16},
+            "screen_stats": {k: v for k, v in st_bf16[-1].items()},
+            "e2e": {"value": ws * N_QUERY / e2e_s, "unit": "queries/s",
+                    "h2d_bytes_per_step": int(Qh.nbytes),
+                    "d2h_bytes_per_step": int(out_i.nbytes + out_d.nbytes)},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks,
+        }
+        # CPU baseline: the reference's exact CPU scan on a bounded sample, with
+        # our answers for the same queries compared against it.
+        threads = os.cpu_count() or 1
+        sample = int(os.environ.get("B2K_CPU_SAMPLE", str(max(64, 2 * threads))))
+        qps, (rd, ri), kind = cpu_reference_time(X, Q, sample, threads)
+        od, oi = index.query(Q[:sample], K, mode="bf16")
+        rel = np.max(np.abs(od - rd) / np.maximum(rd, 1e-300))
+        result["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads,
+                                  "kind": kind,
+                                  "sample": f"first {sample} queries of the batch, k={K}"}
+        result["parity_vs_cpu_reference"] = {"queries": sample,
+                                             "indices_bit_exact": bool(np.array_equal(oi, ri)),
+                                             "max_rel_dist_err": float(rel)}
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

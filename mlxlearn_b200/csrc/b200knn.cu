@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "internal.cuh"
+#include "sinks.cuh"
 
 struct b2k_index {
   b2k::Index ix;
@@ -319,12 +320,18 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
       CUtensorMap tmap_a;
       if (!tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
         return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
-      int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, k, exclude_self, q_offset, S, qp.E, so,
-                                status, st);
+      SinkArgs sa{};
+      sa.out = so;
+      sa.k = k;
+      int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
+                                kSinkKnn, sa, status, st);
       if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
                           cudaGetErrorString((cudaError_t)lr));
     } else {
-      launch_screen_simt(&ix, dQ, m, m_pad, k, exclude_self, q_offset, S, qp.E, so, st);
+      SinkArgs sa{};
+      sa.out = so;
+      sa.k = k;
+      launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, S, qp.E, kSinkKnn, sa, st);
       B2K_CUDA(cudaGetLastError());
     }
     if (stats) cudaEventRecord(ev[2], st);
@@ -595,6 +602,273 @@ int b2k_knn(b2k_index* h, const float* Q, int64_t m, int32_t k, int32_t exclude_
   if (dist)
     B2K_CUDA(cudaMemcpyAsync(dist, dd, (size_t)m * k * sizeof(double), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
+  return B2K_OK;
+}
+
+}  // extern "C"
+
+// =================================================================== radius
+struct b2k_radius_result {
+  int device = 0;
+  int64_t m = 0, nnz = 0;
+  int64_t* indptr = nullptr;   // device [m+1]
+  int64_t* indices = nullptr;  // device [nnz]
+  double* dist = nullptr;      // device [nnz] or null
+  int64_t exact_tests = 0;
+  int64_t candidates = 0;
+};
+
+namespace b2k {
+
+// One block of queries: screen (count + fill), classify, compact, sort.
+// Appends device CSR pieces to `res` (which then owns them).
+static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int exclude_self,
+                        int64_t q_offset, bool need_distance, bool sort_results, bool admit_all,
+                        cudaStream_t st, b2k_radius_result* res) {
+  StreamFree fr{st, {}};
+  int rc;
+  int mode = (!admit_all && ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16 : B2K_MODE_FP32;
+  if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
+  const bool tc = mode == B2K_MODE_BF16;
+  const int64_t bm = tc ? kTcBM : kSimtBM;
+  const int64_t m_pad = round_up(m, bm);
+  const int64_t n_tiles = tc ? ix.n_pad_tc / kTcBN : (ix.n + kSimtBN - 1) / kSimtBN;
+  const int sms = num_sms(ix.device);
+  const int S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
+
+  int* status = nullptr;
+  if ((rc = dalloc(&status, 8, st))) return rc;
+  fr.keep(status);
+  unsigned long long* counters = nullptr;
+  if ((rc = dalloc(&counters, 2, st))) return rc;
+  fr.keep(counters);
+  B2K_CUDA(cudaMemsetAsync(status, 0, 8 * sizeof(int), st));
+  B2K_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
+  QueryPrep qp{};
+  if ((rc = dalloc(&qp.E, (size_t)m_pad, st))) return rc;
+  fr.keep(qp.E);
+  if ((rc = dalloc(&qp.nq, (size_t)m_pad, st))) return rc;
+  fr.keep(qp.nq);
+  qp.flags = status + 4;
+  if (tc) {
+    if ((rc = dalloc(&qp.Ah, (size_t)m_pad * ix.dp, st))) return rc;
+    fr.keep(qp.Ah);
+  }
+  launch_prep_queries(&ix, dQ, m, m_pad, mode, qp, st);
+  float* thr = nullptr;
+  if ((rc = dalloc(&thr, (size_t)m_pad, st))) return rc;
+  fr.keep(thr);
+  launch_radius_threshold(qp.nq, qp.E, m, m_pad, admit_all ? INFINITY : R2, thr, st);
+  B2K_CUDA(cudaGetLastError());
+
+  SinkArgs sa{};
+  sa.thr = thr;
+  sa.m_pad = (int)m_pad;
+  if ((rc = dalloc(&sa.rcount, (size_t)S * m_pad, st))) return rc;
+  fr.keep(sa.rcount);
+  int64_t* roff = nullptr;
+  if ((rc = dalloc(&roff, (size_t)S * m_pad + 1, st))) return rc;
+  fr.keep(roff);
+  sa.roff = roff;
+  CUtensorMap tmap_a;
+  if (tc && !tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
+    return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
+  auto screen = [&](int kind) -> int {
+    if (tc) {
+      int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E, kind,
+                                sa, status, st);
+      if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
+                          cudaGetErrorString((cudaError_t)lr));
+      return B2K_OK;
+    }
+    launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, S, qp.E, kind, sa, st);
+    B2K_CUDA(cudaGetLastError());
+    return B2K_OK;
+  };
+  if ((rc = screen(kSinkRadiusCount))) return rc;
+  launch_scan_split_counts(sa.rcount, S, m, m_pad, roff, roff + (size_t)S * m_pad, st);
+  int64_t ncand = 0;
+  int hstatus[8];
+  B2K_CUDA(cudaMemcpyAsync(&ncand, roff + (size_t)S * m_pad, sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  if (hstatus[0] != DEV_OK)
+    return fail(B2K_ETIMEOUT, "a bounded device wait gave up (code %d)", hstatus[0]);
+  if ((hstatus[4] & 1) && !admit_all)
+    return radius_block(ix, dQ, m, R2, exclude_self, q_offset, need_distance, sort_results, true,
+                        st, res);
+  if ((rc = dalloc(&sa.rcols, (size_t)ncand, st))) return rc;
+  fr.keep(sa.rcols);
+  if ((rc = screen(kSinkRadiusFill))) return rc;
+
+  RadiusPlanArgs ra{};
+  ra.X = ix.X;
+  ra.Q = dQ;
+  ra.d = ix.d;
+  ra.m = m;
+  ra.m_pad = m_pad;
+  ra.S = S;
+  ra.roff = roff;
+  ra.rcount = sa.rcount;
+  ra.cols = sa.rcols;
+  ra.R2 = R2;
+  ra.exact_tests = counters;
+  if ((rc = dalloc(&ra.cdist, (size_t)ncand, st))) return rc;
+  fr.keep(ra.cdist);
+  if ((rc = dalloc(&ra.mcount, (size_t)m, st))) return rc;
+  fr.keep(ra.mcount);
+  launch_classify(ra, st);
+  int64_t* indptr = nullptr;
+  if ((rc = dalloc(&indptr, (size_t)m + 1, st))) return rc;
+  launch_scan_rows(ra.mcount, m, indptr, st);
+  B2K_CUDA(cudaGetLastError());
+  int64_t nnz = 0;
+  unsigned long long hc[2];
+  B2K_CUDA(cudaMemcpyAsync(&nnz, indptr + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  int64_t* indices = nullptr;
+  double* dist = nullptr;
+  if ((rc = dalloc(&indices, (size_t)nnz, st))) {
+    cudaFreeAsync(indptr, st);
+    return rc;
+  }
+  const bool keep_dist = need_distance || sort_results;
+  if (keep_dist && (rc = dalloc(&dist, (size_t)nnz, st))) {
+    cudaFreeAsync(indptr, st);
+    cudaFreeAsync(indices, st);
+    return rc;
+  }
+  launch_compact(ra, indptr, indices, dist, st);
+  B2K_CUDA(cudaGetLastError());
+  if (sort_results && nnz > 1) {
+    int* big = nullptr;
+    if ((rc = dalloc(&big, (size_t)m + 1, st))) return rc;
+    fr.keep(big);
+    B2K_CUDA(cudaMemsetAsync(big + m, 0, sizeof(int), st));
+    launch_sort_rows(indptr, m, indices, dist, big, big + m, std::min<int64_t>(m, 4 * sms), st);
+    int nbig = 0;
+    B2K_CUDA(cudaMemcpyAsync(&nbig, big + m, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2K_CUDA(cudaStreamSynchronize(st));
+    if (nbig > 0) {
+      // scratch sized for the longest row (<= n), one slot per CTA
+      int64_t P = 2;
+      while (P < ix.n) P <<= 1;
+      const int grid = std::min(nbig, 16);
+      double* td = nullptr;
+      int64_t* ti = nullptr;
+      if ((rc = dalloc(&td, (size_t)grid * P, st))) return rc;
+      fr.keep(td);
+      if ((rc = dalloc(&ti, (size_t)grid * P, st))) return rc;
+      fr.keep(ti);
+      launch_sort_big_rows(indptr, big, nbig, indices, dist, td, ti, P, grid, st);
+      B2K_CUDA(cudaGetLastError());
+    }
+  }
+  B2K_CUDA(cudaStreamSynchronize(st));
+  if (!need_distance && dist) {
+    cudaFree(dist);
+    dist = nullptr;
+  }
+  res->m = m;
+  res->nnz = nnz;
+  res->indptr = indptr;
+  res->indices = indices;
+  res->dist = dist;
+  res->exact_tests = (int64_t)hc[0];
+  res->candidates = ncand;
+  return B2K_OK;
+}
+
+}  // namespace b2k
+
+extern "C" {
+
+int b2k_radius(b2k_index* h, const float* Q, int64_t m, double radius, int32_t exclude_self,
+               int64_t q_offset, int32_t need_distance, int32_t sort_results,
+               b2k_radius_result** out) {
+  if (!h || !out) return fail(B2K_EINVAL, "index and out must not be NULL");
+  *out = nullptr;
+  Index& ix = h->ix;
+  if (std::isnan(radius)) return fail(B2K_EINVAL, "radius must not be NaN");
+  if (radius < 0) return fail(B2K_EINVAL, "radius must be non-negative, got %g", radius);
+  if (m < 0 || m >= ((int64_t)1 << 31)) return fail(B2K_EINVAL, "invalid query count");
+  if (exclude_self && (q_offset < 0 || q_offset + m > ix.n))
+    return fail(B2K_EINVAL,
+                "exclude_self requires the query matrix to be the training matrix: got %lld "
+                "query rows at offset %lld and %lld training rows.",
+                (long long)m, (long long)q_offset, (long long)ix.n);
+  if (m > 0 && !Q) return fail(B2K_EINVAL, "queries must not be NULL");
+  if (!host_finite(Q, (size_t)m * ix.d))
+    return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
+  if (fault_mode() == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
+  const double R2 = radius * radius;
+  cudaSetDevice(ix.device);
+  cudaStream_t st = ix.stream;
+  auto* res = new b2k_radius_result();
+  res->device = ix.device;
+  if (m == 0) {
+    res->m = 0;
+    if (cudaMalloc(&res->indptr, sizeof(int64_t)) != cudaSuccess ||
+        cudaMemset(res->indptr, 0, sizeof(int64_t)) != cudaSuccess) {
+      b2k_radius_result_release(res);
+      return fail(B2K_ENOMEM, "allocation failed");
+    }
+    *out = res;
+    return B2K_OK;
+  }
+  float* dQ = nullptr;
+  int rc = dalloc(&dQ, (size_t)m * ix.d, st);
+  if (rc) {
+    delete res;
+    return rc;
+  }
+  cudaMemcpyAsync(dQ, Q, (size_t)m * ix.d * sizeof(float), cudaMemcpyHostToDevice, st);
+  rc = radius_block(ix, dQ, m, R2, exclude_self, q_offset, need_distance != 0,
+                    sort_results != 0, !ix.range_ok, st, res);
+  cudaFreeAsync(dQ, st);
+  cudaStreamSynchronize(st);
+  if (rc) {
+    b2k_radius_result_release(res);
+    return rc;
+  }
+  *out = res;
+  return B2K_OK;
+}
+
+int b2k_radius_result_nnz(const b2k_radius_result* res, int64_t* nnz) {
+  if (!res || !nnz) return fail(B2K_EINVAL, "result and nnz must not be NULL");
+  *nnz = res->nnz;
+  return B2K_OK;
+}
+
+int b2k_radius_result_fetch(const b2k_radius_result* res, int64_t* indptr, int64_t* indices,
+                            double* dist) {
+  if (!res || !indptr) return fail(B2K_EINVAL, "result and indptr must not be NULL");
+  if (res->nnz && !indices) return fail(B2K_EINVAL, "indices must not be NULL");
+  if (dist && res->nnz && !res->dist)
+    return fail(B2K_EINVAL, "distances were not requested for this result");
+  cudaSetDevice(res->device);
+  B2K_CUDA(cudaMemcpy(indptr, res->indptr, (size_t)(res->m + 1) * sizeof(int64_t),
+                      cudaMemcpyDeviceToHost));
+  if (res->nnz) {
+    B2K_CUDA(cudaMemcpy(indices, res->indices, (size_t)res->nnz * sizeof(int64_t),
+                        cudaMemcpyDeviceToHost));
+    if (dist)
+      B2K_CUDA(cudaMemcpy(dist, res->dist, (size_t)res->nnz * sizeof(double),
+                          cudaMemcpyDeviceToHost));
+  }
+  return B2K_OK;
+}
+
+int b2k_radius_result_release(b2k_radius_result* res) {
+  if (!res) return B2K_OK;
+  cudaSetDevice(res->device);
+  cudaFree(res->indptr);
+  cudaFree(res->indices);
+  cudaFree(res->dist);
+  delete res;
   return B2K_OK;
 }
 

@@ -86,7 +86,7 @@ __device__ __forceinline__ void big5_add(uint64_t* r, const uint64_t* a, const u
 }
 
 // Exact key of S(q, x) for d features.
-__device__ __noinline__ void exact_key(const float* __restrict__ q, const float* __restrict__ x,
+static __device__ __noinline__ void exact_key(const float* __restrict__ q, const float* __restrict__ x,
                                        int d, ExactKey& out) {
   for (int i = 0; i < kKeyLimbs; ++i) out.w[i] = 0;
   for (int i = 0; i < d; ++i) {
@@ -159,7 +159,7 @@ __device__ __forceinline__ int key_cmp(const ExactKey& a, const ExactKey& b) {
 
 // Exact sign of S(q,a) - S(q,b).  Bitwise-identical rows are equal without
 // forming keys (duplicated training rows are the common source of ties).
-__device__ __noinline__ int exact_compare(const float* q, const float* a, const float* b, int d) {
+static __device__ __noinline__ int exact_compare(const float* q, const float* a, const float* b, int d) {
   bool same = true;
   for (int i = 0; i < d && same; ++i) same = __float_as_uint(a[i]) == __float_as_uint(b[i]);
   if (same) return 0;

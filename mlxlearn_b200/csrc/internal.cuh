@@ -66,17 +66,20 @@ struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
   uint16_t* Ah;    // [m_pad, dp] -2*bf16(q - center) (bf16 mode only)
   int* flags;      // [1]: bit 0 = some coordinate outside the screen range
+  double* nq;      // [m_pad] ||q - center||^2 (float64), optional
 };
 void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
                          QueryPrep qp, cudaStream_t st);
 
 // ---------------------------------------------------------- screen kernels
-int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad, int k,
-                     int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
-                     int* status, cudaStream_t st);
-void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int k,
-                        int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
-                        cudaStream_t st);
+constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
+struct SinkArgs;
+int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
+                     int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
+                     const SinkArgs& sa, int* status, cudaStream_t st);
+void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
+                        int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
+                        const SinkArgs& sa, cudaStream_t st);
 
 // -------------------------------------------------- certify + re-rank + exact
 struct CertifyArgs {
@@ -111,6 +114,36 @@ struct ExactArgs {
   int* status;
 };
 void launch_exact(const ExactArgs& a, cudaStream_t st);
+
+// ------------------------------------------------------------------ radius
+struct RadiusPlanArgs {
+  const float* X;
+  const float* Q;
+  int d;
+  int64_t m, m_pad;
+  int S;
+  const int64_t* roff;   // [S][m_pad] candidate offsets
+  const int* rcount;     // [S][m_pad] candidate counts
+  const int* cols;       // candidate columns
+  double* cdist;         // [ncand] member distance or -1
+  int64_t* mcount;       // [m] members per query
+  double R2;
+  unsigned long long* exact_tests;
+};
+void launch_radius_threshold(const double* nq, const float* E, int64_t m, int64_t m_pad,
+                             double R2, float* thr, cudaStream_t st);
+void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad, int64_t* off,
+                              int64_t* total, cudaStream_t st);
+void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, cudaStream_t st);
+void launch_classify(const RadiusPlanArgs& r, cudaStream_t st);
+void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* indices,
+                    double* dist, cudaStream_t st);
+void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
+                      int* big_rows, int* big_count, int grid, cudaStream_t st);
+void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
+                          double* dist, double* tmp_d, int64_t* tmp_i, int64_t tmp_stride,
+                          int grid, cudaStream_t st);
+int radius_sort_cap();
 
 // helpers
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,

@@ -144,7 +144,7 @@ __global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int6
                                     int d, int dp, int mode, const float* __restrict__ center,
                                     float xh_max, float nx_max, float ex_max,
                                     float* __restrict__ E, __nv_bfloat16* __restrict__ Ah,
-                                    int* __restrict__ flags) {
+                                    double* __restrict__ nq_out, int* __restrict__ flags) {
   int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   int lane = threadIdx.x & 31;
   if (row >= m_pad) return;
@@ -192,6 +192,7 @@ __global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int6
                    2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy;
     bound = bound * (1.0 + 0x1p-16) + (double)width * 0x1p-120;
     E[row] = __double2float_ru(bound);
+    if (nq_out) nq_out[row] = yy;
     if (!ok) atomicOr(flags, 1);
   }
 }
@@ -226,7 +227,8 @@ void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_p
   const bool bf16 = mode == B2K_MODE_BF16;
   prep_queries_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
       Q, m, m_pad, ix->d, ix->dp, mode, ix->center, bf16 ? ix->xh_max : ix->xn_max, ix->nx_max,
-      bf16 ? ix->ex_max : ix->ex32_max, qp.E, reinterpret_cast<__nv_bfloat16*>(qp.Ah), qp.flags);
+      bf16 ? ix->ex_max : ix->ex32_max, qp.E, reinterpret_cast<__nv_bfloat16*>(qp.Ah), qp.nq,
+      qp.flags);
 }
 
 }  // namespace b2k

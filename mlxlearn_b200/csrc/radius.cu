@@ -1,0 +1,417 @@
+// Radius search: exact membership S(q,x) <= R2 = fl64(r*r) as CSR.
+//
+// Pipeline (host side in b200knn.cu, b2k_radius):
+//   1. threshold : T = R2 - ||y_q||^2 + E per query (rounded up): a column with
+//                  v > T has S > R2 and is certainly not a neighbour.
+//   2. screen    : the kNN screen kernels with RadiusCountSink, then
+//                  RadiusFillSink at scanned offsets -> candidate columns per
+//                  query in ascending index order (sinks.cuh).
+//   3. classify  : canonical float64 value s of every candidate; member iff
+//                  s <= f64_in, non-member iff s > f64_out, otherwise the exact
+//                  integer test key(S) <= floor(R2 * 2^298) (exact.cuh) --
+//                  the reference's contract, src/mlxlearn/_kernels/radius_contract.py:129-217.
+//   4. compact   : warp ballots + per-query offsets -> indptr / indices /
+//                  distances sqrt(min(s, R2)), rows in ascending index order.
+//   5. sort      : optional per-row (distance, index) order
+//                  (src/mlxlearn/_kernels/radius_result.py:160-187).
+// Replaces the reference's Metal screen + host finisher
+// (src/mlxlearn/_kernels/radius_metal_v1.py:257-611, src/mlxlearn_device/_radius.py:54-330).
+#include <cfloat>
+
+#include "common.cuh"
+#include "exact.cuh"
+#include "internal.cuh"
+
+namespace b2k {
+
+namespace {
+
+__global__ void radius_threshold_kernel(const double* __restrict__ nq, const float* __restrict__ E,
+                                        int64_t m, int64_t m_pad, double R2,
+                                        float* __restrict__ thr) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m_pad) return;
+  if (r >= m) {
+    thr[r] = -INFINITY;
+    return;
+  }
+  if (isinf(R2)) {
+    thr[r] = INFINITY;
+    return;
+  }
+  // v <= R2 - nq + E  (float64 with upward rounding, then rounded up to fp32)
+  const double t = __dadd_ru(__dadd_ru(R2, -nq[r]), (double)E[r]);
+  thr[r] = __double2float_ru(t);
+}
+
+// Exclusive scan of per-(split, row) counts in row-major (row, split) order.
+// One CTA; each thread owns a contiguous block of rows.
+__global__ void scan_split_counts_kernel(const int* __restrict__ counts, int S, int64_t m,
+                                         int64_t m_pad, int64_t* __restrict__ off,
+                                         int64_t* __restrict__ total) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+  const int64_t r0 = min(m, (int64_t)t * per), r1 = min(m, r0 + per);
+  int64_t sum = 0;
+  for (int64_t r = r0; r < r1; ++r)
+    for (int s = 0; s < S; ++s) sum += counts[(size_t)s * m_pad + r];
+  part[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    int64_t acc = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      const int64_t v = part[i];
+      part[i] = acc;
+      acc += v;
+    }
+    *total = acc;
+  }
+  __syncthreads();
+  int64_t acc = part[t];
+  for (int64_t r = r0; r < r1; ++r)
+    for (int s = 0; s < S; ++s) {
+      off[(size_t)s * m_pad + r] = acc;
+      acc += counts[(size_t)s * m_pad + r];
+    }
+}
+
+// Exclusive scan of per-row counts into indptr[m+1].
+__global__ void scan_rows_kernel(const int64_t* __restrict__ counts, int64_t m,
+                                 int64_t* __restrict__ indptr) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+  const int64_t r0 = min(m, (int64_t)t * per), r1 = min(m, r0 + per);
+  int64_t sum = 0;
+  for (int64_t r = r0; r < r1; ++r) sum += counts[r];
+  part[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    int64_t acc = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      const int64_t v = part[i];
+      part[i] = acc;
+      acc += v;
+    }
+    indptr[m] = acc;
+  }
+  __syncthreads();
+  int64_t acc = part[t];
+  for (int64_t r = r0; r < r1; ++r) {
+    indptr[r] = acc;
+    acc += counts[r];
+  }
+}
+
+struct ClassifyArgs {
+  const float* X;
+  const float* Q;
+  int d;
+  int64_t m;
+  int S;
+  int64_t m_pad;
+  const int64_t* roff;   // [S][m_pad] candidate offsets
+  const int* rcount;     // [S][m_pad]
+  const int* cols;       // candidates
+  double* cdist;         // [ncand]: distance of members, -1 for non-members
+  int64_t* mcount;       // [m]
+  double R2, f_in, f_out;
+  int all;               // R2 = inf
+  int r2_huge;           // R2 * 2^298 exceeds every key
+  ExactKey r2key;        // floor(R2 * 2^298)
+  unsigned long long* exact_tests;
+};
+
+__device__ __forceinline__ bool key_le(const ExactKey& a, const ExactKey& b) {
+  return key_cmp(a, b) <= 0;
+}
+
+// One warp per query row.
+__global__ void classify_kernel(const ClassifyArgs a) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= a.m) return;
+  const float* q = a.Q + (size_t)row * a.d;
+  int64_t members = 0;
+  unsigned exact = 0;
+  for (int s = 0; s < a.S; ++s) {
+    const size_t slot = (size_t)s * a.m_pad + row;
+    const int64_t base = a.roff[slot];
+    const int cnt = a.rcount[slot];
+    for (int i = lane; i < cnt; i += 32) {
+      const int col = a.cols[base + i];
+      const float* x = a.X + (size_t)col * a.d;
+      double dist = -1.0;
+      if (a.all) {
+        dist = sqrt(canonical_d2(q, x, a.d));  // min(s, inf) = s
+      } else {
+        const double sv = canonical_d2(q, x, a.d);
+        bool in;
+        if (sv <= a.f_in) in = true;
+        else if (!(sv <= a.f_out)) in = false;
+        else if (a.r2_huge) in = true;
+        else {
+          ExactKey k;
+          exact_key(q, x, a.d, k);
+          in = key_le(k, a.r2key);
+          ++exact;
+        }
+        if (in) dist = sqrt(sv < a.R2 ? sv : a.R2);
+      }
+      a.cdist[base + i] = dist;
+      members += dist >= 0.0;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    members += __shfl_xor_sync(0xffffffffu, members, o);
+    exact += __shfl_xor_sync(0xffffffffu, exact, o);
+  }
+  if (lane == 0) {
+    a.mcount[row] = members;
+    if (exact) atomicAdd(a.exact_tests, (unsigned long long)exact);
+  }
+}
+
+// One warp per query row: order-preserving compaction of the members.
+__global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__ indptr,
+                               int64_t* __restrict__ indices, double* __restrict__ dist) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= a.m) return;
+  int64_t out = indptr[row];
+  for (int s = 0; s < a.S; ++s) {
+    const size_t slot = (size_t)s * a.m_pad + row;
+    const int64_t base = a.roff[slot];
+    const int cnt = a.rcount[slot];
+    for (int i0 = 0; i0 < cnt; i0 += 32) {
+      const int i = i0 + lane;
+      double dv = -1.0;
+      int col = 0;
+      if (i < cnt) {
+        dv = a.cdist[base + i];
+        col = a.cols[base + i];
+      }
+      const bool keep = dv >= 0.0;
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int64_t pos = out + __popc(bal & ((1u << lane) - 1));
+        indices[pos] = col;
+        if (dist) dist[pos] = dv;
+      }
+      out += __popc(bal);
+    }
+  }
+}
+
+// Per-row (distance, index) sort, one CTA per row, rows of at most kRadiusSortCap.
+constexpr int kRadiusSortCap = 4096;
+constexpr int kSortThreads = 512;
+
+__global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
+                                 int64_t* __restrict__ indices, double* __restrict__ dist,
+                                 int* __restrict__ big_rows, int* __restrict__ big_count) {
+  extern __shared__ uint8_t smem[];
+  double* sd = reinterpret_cast<double*>(smem);
+  int64_t* si = reinterpret_cast<int64_t*>(sd + kRadiusSortCap);
+  for (int64_t row = blockIdx.x; row < m; row += gridDim.x) {
+    const int64_t a0 = indptr[row], len = indptr[row + 1] - a0;
+    if (len <= 1) continue;
+    if (len > kRadiusSortCap) {
+      if (threadIdx.x == 0) big_rows[atomicAdd(big_count, 1)] = (int)row;
+      continue;
+    }
+    int P = 2;
+    while (P < len) P <<= 1;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+      sd[i] = i < len ? dist[a0 + i] : DBL_MAX;
+      si[i] = i < len ? indices[a0 + i] : INT64_MAX;
+    }
+    __syncthreads();
+    for (int size = 2; size <= P; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+          const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+          const bool up = (i & size) == 0;
+          const double x = sd[i], y = sd[j];
+          const int64_t xi = si[i], yi = si[j];
+          const bool gt = (x > y) || (x == y && xi > yi);
+          if (gt == up) {
+            sd[i] = y;
+            sd[j] = x;
+            si[i] = yi;
+            si[j] = xi;
+          }
+        }
+        __syncthreads();
+      }
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      dist[a0 + i] = sd[i];
+      indices[a0 + i] = si[i];
+    }
+    __syncthreads();
+  }
+}
+
+// Rows longer than the shared-memory sort: bitonic sort in global scratch
+// (padded to a power of two), one CTA per row.
+__global__ void sort_big_rows_kernel(const int64_t* __restrict__ indptr,
+                                     const int* __restrict__ rows, int count,
+                                     int64_t* __restrict__ indices, double* __restrict__ dist,
+                                     double* __restrict__ tmp_d, int64_t* __restrict__ tmp_i,
+                                     int64_t tmp_stride) {
+  for (int it = blockIdx.x; it < count; it += gridDim.x) {
+    const int64_t row = rows[it];
+    const int64_t a0 = indptr[row], len = indptr[row + 1] - a0;
+    int64_t P = 2;
+    while (P < len) P <<= 1;
+    double* sd = tmp_d + (size_t)blockIdx.x * tmp_stride;
+    int64_t* si = tmp_i + (size_t)blockIdx.x * tmp_stride;
+    for (int64_t i = threadIdx.x; i < P; i += blockDim.x) {
+      sd[i] = i < len ? dist[a0 + i] : DBL_MAX;
+      si[i] = i < len ? indices[a0 + i] : INT64_MAX;
+    }
+    __syncthreads();
+    for (int64_t size = 2; size <= P; size <<= 1)
+      for (int64_t stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int64_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+          const int64_t i = 2 * t - (t & (stride - 1)), j = i + stride;
+          const bool up = (i & size) == 0;
+          const double x = sd[i], y = sd[j];
+          const int64_t xi = si[i], yi = si[j];
+          const bool gt = (x > y) || (x == y && xi > yi);
+          if (gt == up) {
+            sd[i] = y;
+            sd[j] = x;
+            si[i] = yi;
+            si[j] = xi;
+          }
+        }
+        __syncthreads();
+      }
+    for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+      dist[a0 + i] = sd[i];
+      indices[a0 + i] = si[i];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host launchers
+
+void launch_radius_threshold(const double* nq, const float* E, int64_t m, int64_t m_pad,
+                             double R2, float* thr, cudaStream_t st) {
+  if (m_pad <= 0) return;
+  radius_threshold_kernel<<<(unsigned)((m_pad + 255) / 256), 256, 0, st>>>(nq, E, m, m_pad, R2,
+                                                                            thr);
+}
+
+void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad, int64_t* off,
+                              int64_t* total, cudaStream_t st) {
+  scan_split_counts_kernel<<<1, 1024, 0, st>>>(counts, S, m, m_pad, off, total);
+}
+
+void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, cudaStream_t st) {
+  scan_rows_kernel<<<1, 1024, 0, st>>>(counts, m, indptr);
+}
+
+// Thresholds of the float64 band (radius_contract.py:129-153) and the exact
+// key of R2.
+static double down(double v) { return nextafter(v, -INFINITY); }
+static double up(double v) { return nextafter(v, INFINITY); }
+
+void radius_band(int d, double R2, double* f_in, double* f_out, int* all, int* r2_huge,
+                 uint64_t* key10) {
+  *all = std::isinf(R2) ? 1 : 0;
+  *r2_huge = 0;
+  for (int i = 0; i < 10; ++i) key10[i] = 0;
+  if (*all) {
+    *f_in = *f_out = INFINITY;
+    return;
+  }
+  const double u = ldexp(1.0, -53);
+  const double g = (double)(d + 2) * u / (1.0 - (double)(d + 2) * u);
+  if (R2 == 0.0) {
+    *f_in = *f_out = 0.0;
+  } else {
+    const double fin = down(down(R2 * down(1.0 - 2.0 * g)));
+    *f_in = fin > 0.0 ? fin : 0.0;
+    *f_out = up(up(R2 * up(1.0 + 2.0 * g)));
+  }
+  // floor(R2 * 2^298), R2 = M * 2^E
+  int e2;
+  const double fr = frexp(R2, &e2);
+  const uint64_t M = (uint64_t)ldexp(fr, 53);
+  const int shift = e2 - 53 + 298;
+  if (shift >= 0) {
+    if (shift + 53 > 639) {
+      *r2_huge = 1;
+      return;
+    }
+    const int limb = shift >> 6, bit = shift & 63;
+    key10[limb] = M << bit;
+    if (bit && limb + 1 < 10) key10[limb + 1] = M >> (64 - bit);
+  } else if (-shift < 64) {
+    key10[0] = M >> (-shift);
+  }
+}
+
+void launch_classify(const RadiusPlanArgs& r, cudaStream_t st) {
+  ClassifyArgs a{};
+  a.X = r.X;
+  a.Q = r.Q;
+  a.d = r.d;
+  a.m = r.m;
+  a.S = r.S;
+  a.m_pad = r.m_pad;
+  a.roff = r.roff;
+  a.rcount = r.rcount;
+  a.cols = r.cols;
+  a.cdist = r.cdist;
+  a.mcount = r.mcount;
+  a.R2 = r.R2;
+  a.exact_tests = r.exact_tests;
+  radius_band(r.d, r.R2, &a.f_in, &a.f_out, &a.all, &a.r2_huge, a.r2key.w);
+  if (r.m <= 0) return;
+  const int warps = 8;
+  classify_kernel<<<(unsigned)((r.m + warps - 1) / warps), warps * 32, 0, st>>>(a);
+}
+
+void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* indices,
+                    double* dist, cudaStream_t st) {
+  ClassifyArgs a{};
+  a.m = r.m;
+  a.S = r.S;
+  a.m_pad = r.m_pad;
+  a.roff = r.roff;
+  a.rcount = r.rcount;
+  a.cols = r.cols;
+  a.cdist = r.cdist;
+  if (r.m <= 0) return;
+  const int warps = 8;
+  compact_kernel<<<(unsigned)((r.m + warps - 1) / warps), warps * 32, 0, st>>>(a, indptr,
+                                                                                 indices, dist);
+}
+
+void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
+                      int* big_rows, int* big_count, int grid, cudaStream_t st) {
+  if (m <= 0) return;
+  const size_t smem = (size_t)kRadiusSortCap * (sizeof(double) + sizeof(int64_t));
+  cudaFuncSetAttribute(sort_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  sort_rows_kernel<<<grid, kSortThreads, smem, st>>>(indptr, m, indices, dist, big_rows,
+                                                     big_count);
+}
+
+void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
+                          double* dist, double* tmp_d, int64_t* tmp_i, int64_t tmp_stride,
+                          int grid, cudaStream_t st) {
+  if (count <= 0) return;
+  sort_big_rows_kernel<<<grid, 1024, 0, st>>>(indptr, rows, count, indices, dist, tmp_d, tmp_i,
+                                              tmp_stride);
+}
+
+int radius_sort_cap() { return kRadiusSortCap; }
+
+}  // namespace b2k

@@ -16,7 +16,7 @@
 // one query row with its own tracker.
 #include "common.cuh"
 #include "internal.cuh"
-#include "tracker.cuh"
+#include "sinks.cuh"
 
 namespace b2k {
 
@@ -31,12 +31,12 @@ struct SimtParams {
   const float* nx;
   const float* E;
   const float* center;
-  int m, n, d, k, S, tiles_per_split, n_tiles, exclude_self;
+  int m, n, d, S, tiles_per_split, n_tiles, exclude_self;
   long long q_offset;
-  ScreenOut out;
+  SinkArgs sink;
 };
 
-template <int KMAX>
+template <class Sink>
 __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams p) {
   extern __shared__ float sm[];
   float* As = sm;                    // [2][BK][LDA]
@@ -50,13 +50,11 @@ __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams 
   const int j0 = s * p.tiles_per_split;
   const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
 
-  RowTracker<KMAX> tr;
+  Sink sink;
   const int my_row = row0 + tid;
   const bool scanner = tid < BM && my_row < p.m;
-  const size_t slot = (size_t)s * p.out.m_pad + my_row;
   if (scanner)
-    tr.init(p.k, p.E[my_row], p.exclude_self ? (int)(p.q_offset + my_row) : -1,
-            p.out.lists + slot * p.out.cap, p.out.cap);
+    sink.init(p.sink, my_row, s, p.E[my_row], p.exclude_self ? (int)(p.q_offset + my_row) : -1);
 
   // global -> register staging: thread loads 8 elements of each tile,
   // column c = tid % 16, rows r = tid / 16 + 16 i.
@@ -125,23 +123,26 @@ __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams 
       const float* vr = Vs + tid * LDV;
 #pragma unroll 4
       for (int c = 0; c < BN; ++c) {
-        float x = vr[c];
-        if (x <= tr.T && col_base + c != tr.self) tr.admit(x, col_base + c);
+        sink.offer1(vr[c], col_base + c);
       }
     }
     __syncthreads();
   }
-  if (scanner) {
-    p.out.counts[slot] = tr.cnt;
-    tr.write_kth(p.out.kth + slot * p.k, p.k);
-  }
+  if (scanner) sink.finish(p.sink);
+}
+
+template <class Sink>
+void launch_simt_variant(const SimtParams& p, int grid, size_t smem, cudaStream_t st) {
+  cudaFuncSetAttribute(screen_simt_kernel<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  screen_simt_kernel<Sink><<<grid, kThreads, smem, st>>>(p);
 }
 
 }  // namespace
 
-void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int k,
-                        int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
-                        cudaStream_t st) {
+void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
+                        int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
+                        const SinkArgs& sa, cudaStream_t st) {
   SimtParams p{};
   p.Q = Q;
   p.X = ix->X;
@@ -151,30 +152,21 @@ void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pa
   p.m = (int)m;
   p.n = (int)ix->n;
   p.d = ix->d;
-  p.k = k;
   p.S = S;
   p.n_tiles = (int)((ix->n + BN - 1) / BN);
   p.tiles_per_split = (p.n_tiles + S - 1) / S;
   p.exclude_self = exclude_self;
   p.q_offset = q_offset;
-  p.out = out;
+  p.sink = sa;
   const int m_tiles = (int)(m_pad / BM);
   const size_t smem = (size_t)(4 * BK * LDA + BM * LDV) * sizeof(float);
   const int grid = m_tiles * S;
   if (grid <= 0) return;
-  if (k <= 16) {
-    cudaFuncSetAttribute(screen_simt_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    screen_simt_kernel<16><<<grid, kThreads, smem, st>>>(p);
-  } else if (k <= 32) {
-    cudaFuncSetAttribute(screen_simt_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    screen_simt_kernel<32><<<grid, kThreads, smem, st>>>(p);
-  } else {
-    cudaFuncSetAttribute(screen_simt_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    screen_simt_kernel<64><<<grid, kThreads, smem, st>>>(p);
-  }
+  if (sink_kind == kSinkRadiusCount) return launch_simt_variant<RadiusCountSink>(p, grid, smem, st);
+  if (sink_kind == kSinkRadiusFill) return launch_simt_variant<RadiusFillSink>(p, grid, smem, st);
+  if (sa.k <= 16) return launch_simt_variant<KnnSink<16>>(p, grid, smem, st);
+  if (sa.k <= 32) return launch_simt_variant<KnnSink<32>>(p, grid, smem, st);
+  launch_simt_variant<KnnSink<64>>(p, grid, smem, st);
 }
 
 }  // namespace b2k

@@ -29,18 +29,18 @@
 
 #include "common.cuh"
 #include "internal.cuh"
-#include "tracker.cuh"
+#include "sinks.cuh"
 
 namespace b2k {
 
 namespace {
 
 struct TcParams {
-  int m, KB, n_tiles, S, tiles_per_split, m_tiles, k, exclude_self, stages;
+  int m, KB, n_tiles, S, tiles_per_split, m_tiles, exclude_self, stages;
   long long q_offset;
   const float* nx;  // [n_pad_tc], NaN on padding rows
   const float* E;   // [m_pad]
-  ScreenOut out;
+  SinkArgs sink;
   int* status;
 };
 
@@ -58,7 +58,7 @@ __host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_strea
   return 1024 /*alignment slack*/ + a + stage * stages + spill + nx + bars;
 }
 
-template <int KMAX, bool A_STREAM>
+template <class Sink, bool A_STREAM>
 __global__ void __launch_bounds__(kThreads, 1)
     screen_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                      const __grid_constant__ CUtensorMap tmB, const TcParams p) {
@@ -217,11 +217,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
       const int row = t * kTcBM + row_in_tile;
       const bool valid = row < p.m;
-      RowTracker<KMAX> tr;
-      const size_t slot = (size_t)s * p.out.m_pad + row;
-      tr.init(p.k, valid ? p.E[row] : 0.0f,
-              p.exclude_self ? (int)(p.q_offset + row) : -1,
-              p.out.lists + slot * p.out.cap, p.out.cap);
+      Sink sink;
+      if (valid)
+        sink.init(p.sink, row, s, p.E[row], p.exclude_self ? (int)(p.q_offset + row) : -1);
       // column norms of the unit's first tile
       {
         const float2 nn = __ldg(reinterpret_cast<const float2*>(p.nx + (size_t)j0 * kTcBN) + et);
@@ -254,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             v[4 * q4 + 2] = a2;
             v[4 * q4 + 3] = a3;
           }
-          if (valid) tr.offer32(v, j * kTcBN + c * 32, spill);
+          if (valid) sink.offer32(v, j * kTcBN + c * 32, spill);
         };
         // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
         uint32_t ra[32], rb[32];
@@ -282,8 +280,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         nb ^= 1;
       }
       if (valid) {
-        p.out.counts[slot] = tr.cnt;
-        tr.write_kth(p.out.kth + slot * p.k, p.k);
+        sink.finish(p.sink);
       }
     }
   epi_done:;
@@ -297,10 +294,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-template <int KMAX, bool A_STREAM>
+template <class Sink, bool A_STREAM>
 int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcParams& p, int grid,
                       size_t smem, cudaStream_t st) {
-  auto kern = screen_tc_kernel<KMAX, A_STREAM>;
+  auto kern = screen_tc_kernel<Sink, A_STREAM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
@@ -310,9 +307,9 @@ int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcPara
 
 }  // namespace
 
-int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad, int k,
-                     int exclude_self, int64_t q_offset, int S, const float* E, ScreenOut out,
-                     int* status, cudaStream_t st) {
+int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
+                     int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
+                     const SinkArgs& sa, int* status, cudaStream_t st) {
   TcParams p{};
   p.m = (int)m;
   p.KB = ix->dp / kTcBK;
@@ -320,12 +317,11 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   p.S = S;
   p.tiles_per_split = (p.n_tiles + S - 1) / S;
   p.m_tiles = (int)(m_pad / kTcBM);
-  p.k = k;
   p.exclude_self = exclude_self;
   p.q_offset = q_offset;
   p.nx = ix->nxh;
   p.E = E;
-  p.out = out;
+  p.sink = sa;
   p.status = status;
   const bool a_stream = p.KB > 4;
   const size_t budget = 227 * 1024;
@@ -336,15 +332,16 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   int units = p.m_tiles * S;
   int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
   if (grid <= 0) return 0;
-  if (k <= 16) {
-    return a_stream ? launch_tc_variant<16, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
-                    : launch_tc_variant<16, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
-  } else if (k <= 32) {
-    return a_stream ? launch_tc_variant<32, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
-                    : launch_tc_variant<32, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
-  }
-  return a_stream ? launch_tc_variant<64, true>(tmap_a, &ix->tmap_b, p, grid, smem, st)
-                  : launch_tc_variant<64, false>(tmap_a, &ix->tmap_b, p, grid, smem, st);
+  const CUtensorMap* tb = &ix->tmap_b;
+#define B2K_TC_LAUNCH(SINK) \
+  (a_stream ? launch_tc_variant<SINK, true>(tmap_a, tb, p, grid, smem, st) \
+            : launch_tc_variant<SINK, false>(tmap_a, tb, p, grid, smem, st))
+  if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink);
+  if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink);
+  if (sa.k <= 16) return B2K_TC_LAUNCH(KnnSink<16>);
+  if (sa.k <= 32) return B2K_TC_LAUNCH(KnnSink<32>);
+  return B2K_TC_LAUNCH(KnnSink<64>);
+#undef B2K_TC_LAUNCH
 }
 
 }  // namespace b2k

@@ -1,0 +1,99 @@
+// Per-row consumers of the screen values ("sinks").
+//
+// A screen kernel hands each row's values v (see prep.cu) to a sink, 32
+// columns at a time (offer32) or one at a time (offer1).  Columns flagged NaN
+// (padding) are never admitted, nor is the row's excluded self column.
+//   KnnSink        : the running k-smallest tracker + candidate list (tracker.cuh)
+//   RadiusCountSink: counts columns with v <= T (T fixed per row: R2 - ||y_q||^2 + E)
+//   RadiusFillSink : writes those columns, in ascending order, at a precomputed offset
+#pragma once
+#include "internal.cuh"
+#include "tracker.cuh"
+
+namespace b2k {
+
+struct SinkArgs {
+  // kNN
+  ScreenOut out;
+  int k;
+  // radius
+  const float* thr;      // [m_pad] admission threshold per row
+  int* rcount;           // [S][m_pad]
+  const int64_t* roff;   // [S][m_pad]
+  int* rcols;            // candidate columns
+  int m_pad;
+};
+
+// Shared 32-column prefilter: the 3-input-min tree over the chunk.
+__device__ __forceinline__ float min32(const float (&v)[32]) {
+  float a[11];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) a[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+  a[10] = fminf(v[30], v[31]);
+  const float b0 = min3f(a[0], a[1], a[2]), b1 = min3f(a[3], a[4], a[5]);
+  const float b2 = min3f(a[6], a[7], a[8]), b3 = fminf(a[9], a[10]);
+  return fminf(min3f(b0, b1, b2), b3);
+}
+
+template <int KMAX>
+struct KnnSink {
+  RowTracker<KMAX> tr;
+  size_t slot;
+  B2K_DEV void init(const SinkArgs& a, int row, int split, float E, int self) {
+    slot = (size_t)split * a.out.m_pad + row;
+    tr.init(a.k, E, self, a.out.lists + slot * a.out.cap, a.out.cap);
+  }
+  B2K_DEV void offer32(const float (&v)[32], int col0, float* spill) { tr.offer32(v, col0, spill); }
+  B2K_DEV void offer1(float x, int col) {
+    if (x <= tr.T && col != tr.self) tr.admit(x, col);
+  }
+  B2K_DEV void finish(const SinkArgs& a) {
+    a.out.counts[slot] = tr.cnt;
+    tr.write_kth(a.out.kth + slot * a.k, a.k);
+  }
+};
+
+struct RadiusCountSink {
+  float T;
+  int self, cnt;
+  size_t slot;
+  B2K_DEV void init(const SinkArgs& a, int row, int split, float /*E*/, int self_col) {
+    slot = (size_t)split * a.m_pad + row;
+    T = a.thr[row];
+    self = self_col;
+    cnt = 0;
+  }
+  B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
+    if (min32(v) <= T) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) cnt += (v[i] <= T && col0 + i != self) ? 1 : 0;
+    }
+  }
+  B2K_DEV void offer1(float x, int col) { cnt += (x <= T && col != self) ? 1 : 0; }
+  B2K_DEV void finish(const SinkArgs& a) { a.rcount[slot] = cnt; }
+};
+
+struct RadiusFillSink {
+  float T;
+  int self;
+  int* out;
+  B2K_DEV void init(const SinkArgs& a, int row, int split, float /*E*/, int self_col) {
+    const size_t slot = (size_t)split * a.m_pad + row;
+    T = a.thr[row];
+    self = self_col;
+    out = a.rcols + a.roff[slot];
+  }
+  B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
+    if (min32(v) <= T) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (v[i] <= T && col0 + i != self) *out++ = col0 + i;
+    }
+  }
+  B2K_DEV void offer1(float x, int col) {
+    if (x <= T && col != self) *out++ = col;
+  }
+  B2K_DEV void finish(const SinkArgs&) {}
+};
+
+}  // namespace b2k

@@ -107,13 +107,14 @@ class NeighborIndex:
                 f"got {n_query} query rows and {self.n_samples} training rows.")
 
     def query(self, Q, k, *, return_distance=True, exclude_self=False,
-              query_block_size=None, train_block_size=None, mode=None, stats=False):
+              query_block_size=None, train_block_size=None, mode=None, stats=False, out=None):
         """Float64 distances (or None) and int64 indices, each ``[n_query, k]``.
 
         ``query_block_size`` splits the queries into independent batches;
         results do not depend on it.  ``train_block_size`` is accepted for
         compatibility: the engine tiles the training rows itself and its
-        merge is exact, so blocking never changes an answer.
+        merge is exact, so blocking never changes an answer.  ``out`` may
+        supply preallocated (e.g. pinned) ``(dist, idx)`` host arrays.
         """
         Q = _as_f32_c(Q)
         k = int(k)
@@ -121,8 +122,18 @@ class NeighborIndex:
             raise ValueError(f"Q must have shape (n, {self.n_features})")
         m = Q.shape[0]
         self._check_query(m, k, exclude_self)
-        idx = np.empty((m, k), dtype=INDEX_DTYPE)
-        dist = np.empty((m, k), dtype=np.float64) if return_distance else None
+        if out is not None:
+            dist, idx = out
+            if idx.shape != (m, k) or idx.dtype != INDEX_DTYPE or not idx.flags.c_contiguous:
+                raise ValueError("out indices must be a C-contiguous int64 array of shape (m, k)")
+            if dist is not None and (dist.shape != (m, k) or dist.dtype != np.float64
+                                     or not dist.flags.c_contiguous):
+                raise ValueError("out distances must be a C-contiguous float64 array (m, k)")
+            if not return_distance:
+                dist = None
+        else:
+            idx = np.empty((m, k), dtype=INDEX_DTYPE)
+            dist = np.empty((m, k), dtype=np.float64) if return_distance else None
         if m:
             h = self._ensure_device()
             lib = _lib.load()
@@ -173,6 +184,94 @@ class NeighborIndex:
             self.last_stats = st.as_dict() if stats else None
         self.last_query_backend = "cuda"
         return dist, idx
+
+
+    # ----------------------------------------------------------------- radius
+    def query_radius_csr(self, Q, radius, *, need_distance=True, exclude_self=False,
+                         sort_results=False, algorithm="auto", n_jobs=None, patched=False,
+                         query_block_size=None, raw=False):
+        """Neighbourhoods within an inclusive Euclidean radius, as CSR batches.
+
+        A training row is returned iff its exact squared distance is at most
+        ``fl64(radius ** 2)`` (reference distance.py:285-342).  Rows hold
+        ascending training indices, or ``(distance, index)`` order with
+        ``sort_results``.  ``algorithm``/``n_jobs``/``patched``/``raw`` are
+        accepted for signature compatibility.
+        """
+        from .radius_result import RadiusCSR
+
+        radius = validate_radius(radius)
+        Q = _as_f32_c(Q)
+        if Q.ndim != 2 or Q.shape[1] != self.n_features:
+            raise ValueError(f"Q must have shape (n, {self.n_features})")
+        n_query = int(Q.shape[0])
+        if exclude_self and n_query != self.n_samples:
+            raise ValueError(
+                "exclude_self requires the query matrix to be the training matrix: "
+                f"got {n_query} query rows and {self.n_samples} training rows.")
+        step = n_query if not query_block_size else max(1, int(query_block_size))
+        parts = []
+        lib = _lib.load()
+        h = self._ensure_device()
+        for start in range(0, max(n_query, 1), max(step, 1)):
+            stop = min(n_query, start + step)
+            block = Q[start:stop]
+            res = ctypes.c_void_p()
+            rc = lib.b2k_radius(h, block.ctypes.data if len(block) else None, stop - start,
+                                float(radius), int(bool(exclude_self)), start,
+                                int(bool(need_distance or sort_results)),
+                                int(bool(sort_results)), ctypes.byref(res))
+            _lib.check(rc, "b2k_radius")
+            try:
+                nnz = ctypes.c_int64()
+                _lib.check(lib.b2k_radius_result_nnz(res, ctypes.byref(nnz)))
+                indptr = np.empty(stop - start + 1, INDEX_DTYPE)
+                indices = np.empty(nnz.value, INDEX_DTYPE)
+                dist = (np.empty(nnz.value, np.float64)
+                        if (need_distance or sort_results) else None)
+                _lib.check(lib.b2k_radius_result_fetch(
+                    res, indptr.ctypes.data, indices.ctypes.data,
+                    None if dist is None else dist.ctypes.data))
+            finally:
+                lib.b2k_radius_result_release(res)
+            parts.append(RadiusCSR(indptr, indices, dist if need_distance else None))
+        self.last_query_backend = "cuda"
+        return parts
+
+    def query_radius(self, Q, radius, *, return_distance=True, exclude_self=False,
+                     sort_results=False, query_block_size=None, train_block_size=None,
+                     algorithm="auto"):
+        """scikit-learn's ragged form of :meth:`query_radius_csr`."""
+        from .radius_result import to_ragged
+
+        if Q.shape[0] == 0:
+            empty = np.empty(0, dtype=object)
+            return (np.empty(0, dtype=object), empty) if return_distance else empty
+        parts = self.query_radius_csr(Q, radius, need_distance=return_distance or sort_results,
+                                      exclude_self=exclude_self, sort_results=sort_results,
+                                      query_block_size=query_block_size)
+        return to_ragged(parts, return_distance=return_distance)
+
+
+def validate_radius(radius) -> float:
+    """A radius as a float; rejects NaN, negatives, booleans and arrays
+    (reference src/mlxlearn/_kernels/radius_contract.py:75-95)."""
+    import math
+    from numbers import Real
+
+    if isinstance(radius, np.ndarray):
+        if radius.ndim != 0:
+            raise TypeError(f"radius must be a scalar, got an array of shape {radius.shape}")
+        radius = radius[()]
+    if isinstance(radius, (bool, np.bool_)) or not isinstance(radius, (Real, np.floating,
+                                                                        np.integer)):
+        raise TypeError(f"radius must be a real number, got {type(radius).__name__}")
+    value = float(radius)
+    if math.isnan(value):
+        raise ValueError("radius must not be NaN")
+    if value < 0:
+        raise ValueError(f"radius must be non-negative, got {value}")
+    return value + 0.0
 
 
 def build_index(X, *, backend: str = "cuda", _owned: bool = False, device: int = 0,

@@ -1,0 +1,115 @@
+"""Radius search parity: exact membership, CSR layout, canonical distances.
+
+Checked against the reference's own outputs (tests/golden) and the oracle,
+bit-exact: indptr, indices and distances (the canonical float64 value is
+deterministic)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+from datasets import mixture
+
+pytestmark = pytest.mark.gpu
+
+
+def make_index(X):
+    from mlxlearn_b200.index import build_index
+
+    return build_index(X)
+
+
+def csr(parts):
+    from mlxlearn_b200.radius_result import concatenate
+
+    j = concatenate(parts)
+    return j.indptr, j.indices, j.distances
+
+
+def test_radius_matches_reference_fixture():
+    rng = np.random.default_rng(4)
+    cen = rng.normal(0, 2.0, (10, 32))
+    X, y = mixture(rng, 20000, cen, 1.0)
+    Q, _ = mixture(np.random.default_rng(44), 500, cen, 1.0)
+    Q[:5] += 40.0
+    g = golden("radius_mixture32.npz")
+    r = float(g["radius"])
+    index = make_index(X)
+    ip, ix, dd = csr(index.query_radius_csr(Q, r))
+    np.testing.assert_array_equal(ip, g["indptr"])
+    np.testing.assert_array_equal(ix, g["indices"])
+    np.testing.assert_array_equal(dd, g["dist"])
+    ip, ix, dd = csr(index.query_radius_csr(Q, r, sort_results=True))
+    np.testing.assert_array_equal(ix, g["sorted_indices"])
+    np.testing.assert_array_equal(dd, g["sorted_dist"])
+
+
+@pytest.mark.parametrize("n,d,m", [(3000, 8, 200), (5000, 32, 300), (2500, 130, 64),
+                                   (40, 3, 40)])
+def test_radius_matches_oracle(n, d, m, rng):
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    Q = rng.normal(size=(m, d)).astype(np.float32)
+    _, oi = oracle.knn(X, Q[:20], min(20, n))
+    r = float(np.median(oracle.knn(X, Q[:20], min(20, n))[0][:, -1]))
+    index = make_index(X)
+    for sort in (False, True):
+        op, oix, od = oracle.radius(X, Q, r, sort_results=sort)
+        ip, ix, dd = csr(index.query_radius_csr(Q, r, sort_results=sort))
+        np.testing.assert_array_equal(ip, op)
+        np.testing.assert_array_equal(ix, oix)
+        np.testing.assert_array_equal(dd, od)
+
+
+def test_radius_exact_boundary_lattice(rng):
+    """Integer lattice with radius exactly on many squared distances: the band
+    must be resolved exactly (S <= R2 inclusive)."""
+    X = rng.integers(-4, 5, size=(4000, 6)).astype(np.float32)
+    Q = rng.integers(-4, 5, size=(100, 6)).astype(np.float32)
+    index = make_index(X)
+    for r in (0.0, 1.0, 2.0, np.sqrt(3.0), 3.0):
+        op, oix, od = oracle.radius(X, Q, r)
+        ip, ix, dd = csr(index.query_radius_csr(Q, r))
+        np.testing.assert_array_equal(ip, op)
+        np.testing.assert_array_equal(ix, oix)
+        np.testing.assert_array_equal(dd, od)
+
+
+def test_radius_self_exclusion_and_infinite_radius(rng):
+    X = rng.normal(size=(600, 5)).astype(np.float32)
+    X[10:20] = X[:10]
+    index = make_index(X)
+    op, oix, od = oracle.radius(X, X, 1.5, exclude_self=True)
+    ip, ix, dd = csr(index.query_radius_csr(X, 1.5, exclude_self=True))
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    ip, ix, _ = csr(index.query_radius_csr(X[:30], np.inf, need_distance=False))
+    assert (np.diff(ip) == 600).all()
+    np.testing.assert_array_equal(ix[:600], np.arange(600))
+
+
+def test_radius_empty_and_zero_neighbours(rng):
+    X = rng.normal(size=(100, 4)).astype(np.float32)
+    index = make_index(X)
+    ip, ix, dd = csr(index.query_radius_csr(np.empty((0, 4), np.float32), 1.0))
+    assert ip.tolist() == [0] and len(ix) == 0
+    ip, ix, dd = csr(index.query_radius_csr(X[:5] + 100, 1.0))
+    assert (ip == 0).all()
+    with pytest.raises(ValueError, match="non-negative"):
+        index.query_radius_csr(X, -1.0)
+    with pytest.raises(TypeError):
+        index.query_radius_csr(X, "1")
+
+
+def test_radius_big_rows_sort(rng):
+    """Rows longer than the shared-memory sort capacity take the global path."""
+    X = rng.normal(size=(9000, 4)).astype(np.float32)
+    Q = rng.normal(size=(3, 4)).astype(np.float32)
+    index = make_index(X)
+    op, oix, od = oracle.radius(X, Q, 3.0, sort_results=True)
+    ip, ix, dd = csr(index.query_radius_csr(Q, 3.0, sort_results=True))
+    assert np.diff(op).max() > 4096
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    np.testing.assert_array_equal(dd, od)
