@@ -119,6 +119,23 @@ B2K_API int b2k_knn_device(b2k_index *index, const float *dQ, int64_t m, int32_t
                    int32_t exclude_self, int64_t q_offset, int32_t mode, double *d_dist,
                    int64_t *d_idx, void *stream, b2k_stats *stats);
 
+/* kNN on device pointers that allocates no memory.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory
+ * during a query (a process whose GPU memory is owned by another allocator or
+ * arena, or a latency-critical path where cudaMalloc/cudaFree and their
+ * implicit synchronisation are not allowed).  Its scratch is a fixed 32 MiB
+ * array in the library's device image, reserved on every GPU that loads the
+ * library until the process exits; a batch that needs more is rejected with
+ * B2K_EINVAL and a message giving the largest allowed query count for that k.
+ * The first call on a device looks up the array's device address: make it
+ * before any stream capture.  Calls share the array, so calls whose GPU work
+ * overlaps race; issue them in order on one stream.  Same results as
+ * b2k_knn_device (fp32 screen, certified float64 re-rank, exact ties); the
+ * call synchronises `stream` before returning. */
+B2K_API int b2k_knn_device_noalloc(b2k_index *index, const float *dQ, int64_t m, int32_t k,
+                                   int32_t exclude_self, int64_t q_offset, double *d_dist,
+                                   int64_t *d_idx, void *stream);
+
 /* ----------------------------------------------------------------- radius */
 
 typedef struct b2k_radius_result b2k_radius_result;

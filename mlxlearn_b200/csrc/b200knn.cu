@@ -411,6 +411,14 @@ static int validate_knn(const Index& ix, int64_t m, int32_t k, int32_t exclude_s
   return B2K_OK;
 }
 
+// Shared with the other host translation units (internal.cuh).
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
+                   int64_t q_offset) {
+  return validate_knn(ix, m, k, exclude_self, q_offset, B2K_MODE_AUTO);
+}
+Index* index_of(b2k_index* h) { return h ? &h->ix : nullptr; }
+
 static bool host_finite(const float* v, size_t count) {
   for (size_t i = 0; i < count; ++i) {
     uint32_t b;

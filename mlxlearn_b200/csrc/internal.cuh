@@ -146,6 +146,10 @@ void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int
 int radius_sort_cap();
 
 // helpers
+int report_error(int code, const char* msg);  // sets b2k_last_error(), returns code
+int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
+                   int64_t q_offset);
+Index* index_of(b2k_index* h);
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
                         uint32_t box_inner, uint32_t box_outer);
 int num_sms(int device);
