@@ -198,6 +198,24 @@ static int ensure_bf16(Index& ix) {
   return B2K_OK;
 }
 
+static int ensure_pivots(Index& ix) {
+  std::lock_guard<std::mutex> lock(ix.mu);
+  if (ix.pivots) return B2K_OK;
+  ix.n_pivots = pivot_count(ix.n);
+  B2K_CUDA(cudaMalloc(&ix.pivots, (size_t)ix.n_pivots * ix.d * sizeof(float)));
+  B2K_CUDA(cudaMalloc(&ix.pivot_norms, (size_t)ix.n_pivots * sizeof(float)));
+  launch_pivots(&ix, ix.stream);
+  B2K_CUDA(cudaGetLastError());
+  B2K_CUDA(cudaStreamSynchronize(ix.stream));
+  return B2K_OK;
+}
+
+// Query grouping is on unless B2K_REORDER=0 (tests run both ways).
+static bool reorder_enabled() {
+  const char* e = getenv("B2K_REORDER");
+  return !(e && e[0] == '0');
+}
+
 // Reference splits: fill the GPU with (query tile, split) work units while
 // keeping the number of candidate lists per query small.
 static int choose_splits(int64_t m_tiles, int64_t n_tiles, int64_t slots) {
@@ -220,8 +238,10 @@ static int choose_splits(int64_t m_tiles, int64_t n_tiles, int64_t slots) {
 static int run_exact(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
                      int64_t q_offset, double* d_dist, int64_t* d_idx, const int* rows,
                      const int* row_count, unsigned long long* counters, int* status,
-                     cudaStream_t st, StreamFree& fr, bool use_scratch) {
+                     cudaStream_t st, StreamFree& fr, bool use_scratch,
+                     const int* perm = nullptr) {
   ExactArgs ea{};
+  ea.perm = perm;
   ea.X = ix.X;
   ea.Q = dQ;
   ea.n = ix.n;
@@ -296,6 +316,32 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     const int64_t n_tiles = tc ? ix.n_pad_tc / kTcBN : (ix.n + kSimtBN - 1) / kSimtBN;
     const int sms = num_sms(ix.device);
     S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
+    // lists per query: one per (split, column group of the screen)
+    const int S_lists = S * (tc ? tc_column_groups(k) : 1);
+    // Group nearby queries (reorder.cu); results go back to the original rows.
+    const int* perm = nullptr;
+    const float* Qs = dQ;
+    if (m >= 2048 && reorder_enabled()) {
+      if ((rc = ensure_pivots(ix))) return rc;
+      int *key = nullptr, *hist = nullptr, *pm = nullptr;
+      float* Qp = nullptr;
+      if ((rc = dalloc(&key, (size_t)m, st))) return rc;
+      fr.keep(key);
+      if ((rc = dalloc(&hist, (size_t)ix.n_pivots, st))) return rc;
+      fr.keep(hist);
+      if ((rc = dalloc(&pm, (size_t)m, st))) return rc;
+      fr.keep(pm);
+      if ((rc = dalloc(&Qp, (size_t)m * ix.d, st))) return rc;
+      fr.keep(Qp);
+      launch_query_order(&ix, dQ, m, key, hist, pm, Qp, st);
+      B2K_CUDA(cudaGetLastError());
+      perm = pm;
+      Qs = Qp;
+    }
+    uint32_t* shared_kth = nullptr;
+    if ((rc = dalloc(&shared_kth, (size_t)m_pad, st))) return rc;
+    fr.keep(shared_kth);
+    B2K_CUDA(cudaMemsetAsync(shared_kth, 0xff, (size_t)m_pad * sizeof(uint32_t), st));
     QueryPrep qp{};
     if ((rc = dalloc(&qp.E, (size_t)m_pad, st))) return rc;
     fr.keep(qp.E);
@@ -304,34 +350,33 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
       if ((rc = dalloc(&qp.Ah, (size_t)m_pad * ix.dp, st))) return rc;
       fr.keep(qp.Ah);
     }
-    launch_prep_queries(&ix, dQ, m, m_pad, mode, qp, st);
+    launch_prep_queries(&ix, Qs, m, m_pad, mode, qp, st);
     B2K_CUDA(cudaGetLastError());
     ScreenOut so{};
     so.cap = kListCap;
     so.m_pad = (int)m_pad;
-    if ((rc = dalloc(&so.lists, (size_t)S * m_pad * kListCap, st))) return rc;
+    if ((rc = dalloc(&so.lists, (size_t)S_lists * m_pad * kListCap, st))) return rc;
     fr.keep(so.lists);
-    if ((rc = dalloc(&so.counts, (size_t)S * m_pad, st))) return rc;
+    if ((rc = dalloc(&so.counts, (size_t)S_lists * m_pad, st))) return rc;
     fr.keep(so.counts);
-    if ((rc = dalloc(&so.kth, (size_t)S * m_pad * k, st))) return rc;
+    if ((rc = dalloc(&so.kth, (size_t)S_lists * m_pad * k, st))) return rc;
     fr.keep(so.kth);
+    SinkArgs sa{};
+    sa.out = so;
+    sa.k = k;
+    sa.shared_kth = shared_kth;
     if (stats) cudaEventRecord(ev[1], st);
     if (tc) {
       CUtensorMap tmap_a;
       if (!tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
         return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
-      SinkArgs sa{};
-      sa.out = so;
-      sa.k = k;
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
-                                kSinkKnn, sa, status, st);
+                                kSinkKnn, sa, status, st, perm);
       if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
                           cudaGetErrorString((cudaError_t)lr));
     } else {
-      SinkArgs sa{};
-      sa.out = so;
-      sa.k = k;
-      launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, S, qp.E, kSinkKnn, sa, st);
+      launch_screen_simt(&ix, Qs, m, m_pad, exclude_self, q_offset, S, qp.E, kSinkKnn, sa, st,
+                         perm);
       B2K_CUDA(cudaGetLastError());
     }
     if (stats) cudaEventRecord(ev[2], st);
@@ -340,12 +385,12 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     fr.keep(fb_list);
     CertifyArgs ca{};
     ca.X = ix.X;
-    ca.Q = dQ;
+    ca.Q = Qs;
     ca.n = ix.n;
     ca.m = m;
     ca.d = ix.d;
     ca.k = k;
-    ca.S = S;
+    ca.S = S_lists;
     ca.scr = so;
     ca.E = qp.E;
     ca.dist = d_dist;
@@ -353,12 +398,13 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.fallback_list = fb_list;
     ca.fallback_count = status + 2;
     ca.counters = counters;
+    ca.perm = perm;
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
     // Rows the screen could not certify (list overflow, or query coordinates
     // outside the screen's safe range: see the flag check below).
-    rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
-                   counters, status, st, fr, false);
+    rc = run_exact(ix, Qs, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
+                   counters, status, st, fr, false, perm);
     if (rc) return rc;
   }
   if (stats) cudaEventRecord(ev[3], st);
@@ -538,6 +584,8 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.stats_dev);
   cudaFree(ix.Xh);
   cudaFree(ix.nxh);
+  cudaFree(ix.pivots);
+  cudaFree(ix.pivot_norms);
   if (ix.stream) cudaStreamDestroy(ix.stream);
   delete h;
   return B2K_OK;

@@ -27,7 +27,11 @@ namespace b2k {
 
 namespace {
 
-constexpr int kCertWarps = 4;
+constexpr int kCertWarps = 8;
+constexpr int kSurvivorCap = 256;  // candidates that can still reach the top k
+constexpr size_t kCertWarpBytes =
+    (size_t)kCertifyCap * (sizeof(int) + sizeof(float)) +
+    (size_t)kSurvivorCap * (sizeof(double) + sizeof(int));
 
 // |canonical - S| <= g S with g = (d+2)u/(1-(d+2)u), u = 2^-53, for a
 // sequential sum of d non-negative rounded terms (reference
@@ -115,14 +119,58 @@ __device__ unsigned warp_sort_resolve(double* s, int* id, int C, int k, const fl
   return compares;
 }
 
+// fp32 direct squared distance of candidate rows, 8 lanes per row (coalesced
+// 16-byte loads), so each warp handles 4 candidates per step.  Sum of d
+// non-negative terms, each (fl(q_i - x_i))^2 accumulated with FMA: the result
+// is within (d + 5) u (1.01) S + d 2^-126 of the exact S, u = 2^-24, whatever
+// the order of the additions.
+__device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
+                                            const float* __restrict__ X, int d, const int* ci,
+                                            float* cv, int C, int lane) {
+  const int grp = lane >> 3, l8 = lane & 7;
+  const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(q) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  for (int c0 = 0; c0 < C; c0 += 4) {
+    const int c = c0 + grp;
+    float acc0 = 0.f, acc1 = 0.f;
+    if (c < C) {
+      const float* x = X + (size_t)ci[c] * d;
+      if (vec) {
+        const float4* q4 = reinterpret_cast<const float4*>(q);
+        const float4* x4 = reinterpret_cast<const float4*>(x);
+        for (int f = l8; f < d / 4; f += 8) {
+          const float4 a = __ldg(q4 + f), b = __ldg(x4 + f);
+          const float e0 = a.x - b.x, e1 = a.y - b.y, e2 = a.z - b.z, e3 = a.w - b.w;
+          acc0 = fmaf(e0, e0, acc0);
+          acc1 = fmaf(e1, e1, acc1);
+          acc0 = fmaf(e2, e2, acc0);
+          acc1 = fmaf(e3, e3, acc1);
+        }
+      } else {
+        for (int f = l8; f < d; f += 8) {
+          const float e = __ldg(q + f) - __ldg(x + f);
+          acc0 = fmaf(e, e, acc0);
+        }
+      }
+    }
+    float acc = acc0 + acc1;
+    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    if (l8 == 0 && c < C) cv[c] = acc;
+  }
+}
+
 __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyArgs a) {
   extern __shared__ uint8_t smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * kCertWarps + w;
   if (row >= a.m) return;
-  double* cs = reinterpret_cast<double*>(smem) + (size_t)w * kCertifyCap;
-  int* ci = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + kCertWarps * kCertifyCap) +
-            (size_t)w * kCertifyCap;
+  uint8_t* wbase = smem + (size_t)w * kCertWarpBytes;
+  int* ci = reinterpret_cast<int*>(wbase);                          // [kCertifyCap]
+  float* cv = reinterpret_cast<float*>(ci + kCertifyCap);           // [kCertifyCap]
+  double* cs = reinterpret_cast<double*>(cv + kCertifyCap);         // [kSurvivorCap]
+  int* si = reinterpret_cast<int*>(cs + kSurvivorCap);              // [kSurvivorCap]
   const ScreenOut& so = a.scr;
   const int k = a.k, S = a.S;
 
@@ -189,14 +237,48 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
     return;
   }
   __syncwarp();
-  // 4. canonical float64 values
+  // 4. fp32 refine of every candidate with a certified relative bound
   const float* q = a.Q + (size_t)row * a.d;
-  for (int c = lane; c < C; c += 32) cs[c] = canonical_d2(q, a.X + (size_t)ci[c] * a.d, a.d);
+  refine_fp32(q, a.X, a.d, ci, cv, C, lane);
   __syncwarp();
-  const unsigned cmp = warp_sort_resolve(cs, ci, C, k, q, a.X, a.d, lane);
+  const float g32 = (float)((double)(a.d + 5) * 0x1p-24 * 1.01);
+  const float abs32 = (float)a.d * 0x1p-126f;
+  const float up_f = 1.0f + g32, lo_f = 1.0f - g32;
+  // 5. U = k-th smallest upper bound (bisection over ordered keys)
+  uint32_t ulo = 0, uhi = 0xffffffffu;
+  while (ulo < uhi) {
+    const uint32_t mid = ulo + ((uhi - ulo) >> 1);
+    unsigned cnt = 0;
+    for (int c = lane; c < C; c += 32)
+      cnt += float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)) <= mid;
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if (cnt >= (unsigned)k) uhi = mid;
+    else ulo = mid + 1;
+  }
+  const float U = key_float(ulo);
+  // 6. survivors: lower bound <= U (everything that can still be in the top k)
+  int Cs = 0;
+  for (int base = 0; base < C; base += 32) {
+    const int c = base + lane;
+    const bool keep = c < C && __fsub_rd(__fmul_rd(cv[c], lo_f), abs32) <= U;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    const int pos = Cs + __popc(bal & ((1u << lane) - 1));
+    if (keep && pos < kSurvivorCap) si[pos] = ci[c];
+    Cs += __popc(bal);
+  }
+  if (Cs > kSurvivorCap) {
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    return;
+  }
+  __syncwarp();
+  // 7. canonical float64 values of the survivors, sort, exact near-tie runs
+  for (int c = lane; c < Cs; c += 32) cs[c] = canonical_d2(q, a.X + (size_t)si[c] * a.d, a.d);
+  __syncwarp();
+  const unsigned cmp = warp_sort_resolve(cs, si, Cs, k, q, a.X, a.d, lane);
+  const int64_t orow = a.perm ? a.perm[row] : row;
   for (int t = lane; t < k; t += 32) {
-    a.idx[row * k + t] = ci[t];
-    if (a.dist) a.dist[row * k + t] = sqrt(cs[t]);
+    a.idx[orow * k + t] = si[t];
+    if (a.dist) a.dist[orow * k + t] = sqrt(cs[t]);
   }
   if (lane == 0) {
     atomicAdd(&a.counters[0], (unsigned long long)C);
@@ -212,10 +294,11 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
 // ---------------------------------------------------------------------------
 constexpr int kExactThreads = 256;
 
-__device__ __forceinline__ double exact_value(const ExactArgs& a, const float* q, int64_t row,
+// `orow` is the query's original row (the one exclude_self refers to).
+__device__ __forceinline__ double exact_value(const ExactArgs& a, const float* q, int64_t orow,
                                               int64_t j, const double* sc) {
   if (sc) return sc[j];
-  if (a.exclude_self && j == a.q_offset + row) return INFINITY;
+  if (a.exclude_self && j == a.q_offset + orow) return INFINITY;
   return canonical_d2(q, a.X + (size_t)j * a.d, a.d);
 }
 
@@ -231,10 +314,11 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a)
   double* sc = a.scratch ? a.scratch + (size_t)blockIdx.x * a.n : nullptr;
   for (int it = blockIdx.x; it < count; it += gridDim.x) {
     const int64_t row = a.rows ? a.rows[it] : it;
+    const int64_t orow = a.perm ? a.perm[row] : row;
     const float* q = a.Q + (size_t)row * a.d;
     if (sc) {
       for (int64_t j = tid; j < a.n; j += kExactThreads) {
-        sc[j] = (a.exclude_self && j == a.q_offset + row)
+        sc[j] = (a.exclude_self && j == a.q_offset + orow)
                     ? INFINITY
                     : canonical_d2(q, a.X + (size_t)j * a.d, a.d);
       }
@@ -248,7 +332,7 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a)
       hist[tid] = 0;
       __syncthreads();
       for (int64_t j = tid; j < a.n; j += kExactThreads) {
-        const unsigned long long b = __double_as_longlong(exact_value(a, q, row, j, sc));
+        const unsigned long long b = __double_as_longlong(exact_value(a, q, orow, j, sc));
         if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
       }
       __syncthreads();
@@ -273,7 +357,7 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a)
     if (tid == 0) s_count = 0;
     __syncthreads();
     for (int64_t j = tid; j < a.n; j += kExactThreads) {
-      const double v = exact_value(a, q, row, j, sc);
+      const double v = exact_value(a, q, orow, j, sc);
       if (v != INFINITY && __dmul_rd(v, 1.0 - g2) <= reach) {
         const int pos = atomicAdd(&s_count, 1);
         if (pos < kExactCap) {
@@ -289,8 +373,8 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a)
     } else if (tid < 32) {
       const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
       for (int t = tid; t < a.k; t += 32) {
-        a.idx[row * a.k + t] = ci[t];
-        if (a.dist) a.dist[row * a.k + t] = sqrt(cs[t]);
+        a.idx[orow * a.k + t] = ci[t];
+        if (a.dist) a.dist[orow * a.k + t] = sqrt(cs[t]);
       }
       if (tid == 0) {
         atomicAdd(&a.counters[3], 1ull);
@@ -305,7 +389,7 @@ __global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a)
 
 void launch_certify(const CertifyArgs& a, cudaStream_t st) {
   if (a.m <= 0) return;
-  const size_t smem = (size_t)kCertWarps * kCertifyCap * (sizeof(double) + sizeof(int));
+  const size_t smem = (size_t)kCertWarps * kCertWarpBytes;
   cudaFuncSetAttribute(certify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const unsigned grid = (unsigned)((a.m + kCertWarps - 1) / kCertWarps);
   certify_kernel<<<grid, kCertWarps * 32, smem, st>>>(a);

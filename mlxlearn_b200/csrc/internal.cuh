@@ -54,6 +54,10 @@ struct Index {
   float* nxh = nullptr;          // [n_pad_tc] fl32(||x||^2), NaN on padding rows
   float xh_max = 0, ex_max = 0;  // max ||bf16 operand||, max ||(x - center) - bf16 operand||
   CUtensorMap tmap_b;            // TMA map over Xh, box 64 x 256
+  // pivots for query ordering (reorder.cu)
+  int n_pivots = 0;
+  float* pivots = nullptr;       // [n_pivots, d] centred rows
+  float* pivot_norms = nullptr;  // [n_pivots]
   cudaStream_t stream = nullptr;
   std::mutex mu;
 };
@@ -76,10 +80,19 @@ constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
 struct SinkArgs;
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                     const SinkArgs& sa, int* status, cudaStream_t st);
+                     const SinkArgs& sa, int* status, cudaStream_t st,
+                     const int* perm = nullptr);
+int tc_column_groups(int k);
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
                         int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                        const SinkArgs& sa, cudaStream_t st);
+                        const SinkArgs& sa, cudaStream_t st, const int* perm = nullptr);
+
+// ----------------------------------------------------------- query order
+int pivot_count(int64_t n);
+void launch_pivots(Index* ix, cudaStream_t st);
+// perm[i] = original row of sorted position i; Qp = Q[perm]
+void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,
+                        int* perm, float* Qp, cudaStream_t st);
 
 // -------------------------------------------------- certify + re-rank + exact
 struct CertifyArgs {
@@ -94,6 +107,7 @@ struct CertifyArgs {
   int* fallback_list;  // [m] query ids needing the exhaustive scan
   int* fallback_count; // [1]
   unsigned long long* counters;  // [4]: candidates, entries, exact compares, -
+  const int* perm;     // row -> output row (or null)
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
 
@@ -112,6 +126,7 @@ struct ExactArgs {
   int64_t* idx;
   unsigned long long* counters;
   int* status;
+  const int* perm;      // row -> original query row for output and self (or null)
 };
 void launch_exact(const ExactArgs& a, cudaStream_t st);
 

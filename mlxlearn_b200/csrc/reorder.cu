@@ -1,0 +1,152 @@
+// Query ordering for the screens.
+//
+// A screen tile holds 128 query rows and each epilogue warp 32 of them; the
+// warp leaves its fast path whenever ANY of its rows admits a column.  With
+// queries in arbitrary order the rows of a warp come from unrelated parts of
+// the space and the admissions of the different rows hit different column
+// chunks, so nearly every chunk takes the slow path.  Grouping queries that
+// are close to each other makes their admissions coincide.
+//
+// Method: P pivots (every (n/P)-th training row), each query goes to its
+// nearest pivot (fp32 Gram form, the assignment only affects speed), then a
+// counting sort by pivot gives the permutation `perm` (sorted position ->
+// original query row) and the permuted query matrix.  Results are written
+// back to the original rows by the certify / exact kernels, so the answer
+// does not depend on the order.
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace b2k {
+
+namespace {
+
+constexpr int kPivTile = 32;     // pivots per shared-memory tile
+constexpr int kDChunk = 64;      // features per shared-memory chunk
+constexpr int kAssignThreads = 128;
+
+__global__ void pivot_rows_kernel(const float* __restrict__ X, int64_t n, int d, int P,
+                                  const float* __restrict__ center, float* __restrict__ piv,
+                                  float* __restrict__ pnorm) {
+  const int p = blockIdx.x;
+  if (p >= P) return;
+  const int64_t row = (int64_t)p * (n / P);
+  double s = 0.0;
+  for (int i = threadIdx.x; i < d; i += 32) {
+    const float y = X[row * d + i] - center[i];
+    piv[(size_t)p * d + i] = y;
+    s += (double)y * (double)y;
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) pnorm[p] = (float)s;
+}
+
+// One thread per query: argmin_p ||p||^2 - 2 <y_q, p>.
+__global__ void __launch_bounds__(kAssignThreads)
+    assign_kernel(const float* __restrict__ Q, int64_t m, int d, const float* __restrict__ center,
+                  const float* __restrict__ piv, const float* __restrict__ pnorm, int P,
+                  int* __restrict__ key, int* __restrict__ hist) {
+  __shared__ float sp[kPivTile][kDChunk + 1];
+  __shared__ float sq[kDChunk][kAssignThreads + 1];  // query tile, transposed
+  const int64_t q0 = (int64_t)blockIdx.x * kAssignThreads;
+  const int64_t q = q0 + threadIdx.x;
+  const bool valid = q < m;
+  float best = INFINITY;
+  int best_p = 0;
+  for (int p0 = 0; p0 < P; p0 += kPivTile) {
+    float acc[kPivTile];
+#pragma unroll
+    for (int j = 0; j < kPivTile; ++j) acc[j] = 0.0f;
+    for (int k0 = 0; k0 < d; k0 += kDChunk) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < kPivTile * kDChunk; i += kAssignThreads) {
+        const int j = i / kDChunk, k = i % kDChunk;
+        sp[j][k] = (p0 + j < P && k0 + k < d) ? piv[(size_t)(p0 + j) * d + k0 + k] : 0.0f;
+      }
+      // coalesced: consecutive threads read consecutive features of one query
+      for (int i = threadIdx.x; i < kAssignThreads * kDChunk; i += kAssignThreads) {
+        const int r = i / kDChunk, k = i % kDChunk;
+        const int64_t qr = q0 + r;
+        sq[k][r] = (qr < m && k0 + k < d) ? Q[qr * d + k0 + k] - center[k0 + k] : 0.0f;
+      }
+      __syncthreads();
+      if (valid) {
+        const int kend = min(kDChunk, d - k0);
+        for (int k = 0; k < kend; ++k) {
+          const float y = sq[k][threadIdx.x];
+#pragma unroll
+          for (int j = 0; j < kPivTile; ++j) acc[j] = fmaf(y, sp[j][k], acc[j]);
+        }
+      }
+    }
+    if (valid) {
+#pragma unroll
+      for (int j = 0; j < kPivTile; ++j) {
+        if (p0 + j < P) {
+          const float v = fmaf(-2.0f, acc[j], pnorm[p0 + j]);
+          if (v < best) {
+            best = v;
+            best_p = p0 + j;
+          }
+        }
+      }
+    }
+  }
+  if (valid) {
+    key[q] = best_p;
+    atomicAdd(hist + best_p, 1);
+  }
+}
+
+__global__ void bin_scan_kernel(int* __restrict__ hist, int P) {
+  // exclusive scan in place (P small), single thread
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int acc = 0;
+    for (int p = 0; p < P; ++p) {
+      const int v = hist[p];
+      hist[p] = acc;
+      acc += v;
+    }
+  }
+}
+
+__global__ void scatter_kernel(const int* __restrict__ key, int64_t m, int* __restrict__ cursor,
+                               int* __restrict__ perm) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  perm[atomicAdd(cursor + key[q], 1)] = (int)q;
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ Q, const int* __restrict__ perm,
+                                   int64_t m, int d, float* __restrict__ Qp) {
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= m) return;
+  const float* src = Q + (size_t)perm[row] * d;
+  float* dst = Qp + (size_t)row * d;
+  for (int i = threadIdx.x & 31; i < d; i += 32) dst[i] = src[i];
+}
+
+}  // namespace
+
+int pivot_count(int64_t n) {
+  int P = 512;
+  while (P > 1 && (int64_t)P * 64 > n) P >>= 1;
+  return P;
+}
+
+void launch_pivots(Index* ix, cudaStream_t st) {
+  pivot_rows_kernel<<<ix->n_pivots, 32, 0, st>>>(ix->X, ix->n, ix->d, ix->n_pivots, ix->center,
+                                                 ix->pivots, ix->pivot_norms);
+}
+
+void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,
+                        int* perm, float* Qp, cudaStream_t st) {
+  const int P = ix->n_pivots;
+  cudaMemsetAsync(hist, 0, (size_t)P * sizeof(int), st);
+  assign_kernel<<<(unsigned)((m + kAssignThreads - 1) / kAssignThreads), kAssignThreads, 0, st>>>(
+      Q, m, ix->d, ix->center, ix->pivots, ix->pivot_norms, P, key, hist);
+  bin_scan_kernel<<<1, 32, 0, st>>>(hist, P);
+  scatter_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(key, m, hist, perm);
+  gather_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(Q, perm, m, ix->d, Qp);
+}
+
+}  // namespace b2k

@@ -33,6 +33,7 @@ struct SimtParams {
   const float* center;
   int m, n, d, S, tiles_per_split, n_tiles, exclude_self;
   long long q_offset;
+  const int* perm;  // row -> original query row (or null)
   SinkArgs sink;
 };
 
@@ -54,7 +55,8 @@ __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams 
   const int my_row = row0 + tid;
   const bool scanner = tid < BM && my_row < p.m;
   if (scanner)
-    sink.init(p.sink, my_row, s, p.E[my_row], p.exclude_self ? (int)(p.q_offset + my_row) : -1);
+    sink.init(p.sink, my_row, s, p.E[my_row],
+              p.exclude_self ? (int)(p.q_offset + (p.perm ? p.perm[my_row] : my_row)) : -1);
 
   // global -> register staging: thread loads 8 elements of each tile,
   // column c = tid % 16, rows r = tid / 16 + 16 i.
@@ -120,6 +122,7 @@ __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams 
     }
     __syncthreads();
     if (scanner) {
+      sink.tile_sync();
       const float* vr = Vs + tid * LDV;
 #pragma unroll 4
       for (int c = 0; c < BN; ++c) {
@@ -142,7 +145,7 @@ void launch_simt_variant(const SimtParams& p, int grid, size_t smem, cudaStream_
 
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
                         int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                        const SinkArgs& sa, cudaStream_t st) {
+                        const SinkArgs& sa, cudaStream_t st, const int* perm) {
   SimtParams p{};
   p.Q = Q;
   p.X = ix->X;
@@ -157,6 +160,7 @@ void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pa
   p.tiles_per_split = (p.n_tiles + S - 1) / S;
   p.exclude_self = exclude_self;
   p.q_offset = q_offset;
+  p.perm = perm;
   p.sink = sa;
   const int m_tiles = (int)(m_pad / BM);
   const size_t smem = (size_t)(4 * BK * LDA + BM * LDV) * sizeof(float);

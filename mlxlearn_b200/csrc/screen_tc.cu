@@ -6,20 +6,24 @@
 // memory.  Here the tile lives only in TMEM.
 //
 // One persistent CTA per SM, warp-specialised:
-//   warp 0      TMA producer: query tile A (128 rows x dp, bf16, -2*q) once
-//               per work unit; reference tiles B (256 rows x 64 cols) into an
+//   warp 0      TMA producer: query tile A (128 rows x dp, bf16) once per
+//               work unit; reference tiles B (256 rows x 64 columns) into an
 //               NST-deep shared-memory ring (128-byte swizzle).
-//   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16,
-//               fp32 accumulators in TMEM, double-buffered (2 x 256 columns).
-//   warps 2..5  epilogue: tcgen05.ld 32 columns at a time (two loads in
-//               flight), add ||x||^2 (staged per tile in shared memory, the
-//               next tile's norms prefetched), 3-input min over the chunk,
-//               and only when the minimum passes the row's threshold, admit
-//               columns to the candidate list (tracker.cuh).  The accumulator
-//               is handed back to the MMA warp as soon as its last chunk is in
-//               registers.  The 128 x 256 distance tile never reaches HBM.
+//   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16, fp32
+//               accumulators in TMEM, double-buffered (2 x 256 columns).
+//   warps 2..   EW epilogue warps.  Warp w reads TMEM lane group w % 4 (the
+//               hardware's rule); with EW = 8 the two warps of a lane group
+//               take the two 128-column halves of each tile.  Per 32-column
+//               chunk: tcgen05.ld (two loads in flight), add ||x||^2 (staged
+//               per tile in shared memory, the next tile's prefetched),
+//               3-input min over the chunk, and only when the minimum passes
+//               the row's threshold, admit columns (sinks.cuh).  The
+//               accumulator is handed back to the MMA warp as soon as its
+//               last chunk is in registers.  The distance tile never reaches
+//               HBM.
 // A work unit is (query tile of 128 rows, split s of the reference tiles);
-// units are dealt round-robin over the persistent CTAs.
+// units are dealt round-robin over the persistent CTAs.  Candidate lists are
+// kept per (split, column half, row).
 //
 // Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
 // B = bf16(x - c)); the certified error bound of v = fl32(acc + ||x - c||^2) is
@@ -38,30 +42,33 @@ namespace {
 struct TcParams {
   int m, KB, n_tiles, S, tiles_per_split, m_tiles, exclude_self, stages;
   long long q_offset;
-  const float* nx;  // [n_pad_tc], NaN on padding rows
-  const float* E;   // [m_pad]
+  const float* nx;   // [n_pad_tc], NaN on padding rows
+  const float* E;    // [m_pad]
+  const int* perm;   // tile row -> original query row (or null)
   SinkArgs sink;
   int* status;
 };
 
 constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;  // 16 KB per 64-column block
 constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;  // 32 KB per 64-column block
-constexpr int kThreads = 192;
-constexpr int kSpillStride = 33;
+constexpr int kSpillStride = 9;  // 8 spilled values per thread, conflict-free stride
 
-__host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream) {
+__host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream, int ew) {
   size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
   size_t stage = a_stream ? kATileBytes + kBTileBytes : kBTileBytes;
-  size_t spill = 128 * kSpillStride * sizeof(float);
-  size_t nx = 2 * kTcBN * sizeof(float);
+  size_t spill = (size_t)ew * 32 * kSpillStride * sizeof(float);
+  size_t nx = 8 * kTcBN * sizeof(float);  // per-warp double buffers (EW x 2 x 256/halves)
   size_t bars = (2 * (size_t)stages + 6) * sizeof(uint64_t) + 16;
   return 1024 /*alignment slack*/ + a + stage * stages + spill + nx + bars;
 }
 
-template <class Sink, bool A_STREAM>
-__global__ void __launch_bounds__(kThreads, 1)
+template <class Sink, bool A_STREAM, int EW>
+__global__ void __launch_bounds__(64 + 32 * EW, 1)
     screen_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                      const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+  constexpr int kEpiThreads = 32 * EW;
+  constexpr int kHalves = EW / 4;                 // column groups per tile
+  constexpr int kChunks = kTcBN / 32 / kHalves;   // 32-column chunks per epilogue warp
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -71,8 +78,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* b_smem = smem + (A_STREAM ? 0 : KB * kATileBytes);
   const uint32_t stage_bytes = A_STREAM ? kATileBytes + kBTileBytes : kBTileBytes;
   float* spill_all = reinterpret_cast<float*>(b_smem + (size_t)nst * stage_bytes);
-  float* nx_all = spill_all + 128 * kSpillStride;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(nx_all + 2 * kTcBN);
+  float* nx_all = spill_all + kEpiThreads * kSpillStride;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(nx_all + 8 * kTcBN);
   uint64_t* full = bars;
   uint64_t* empty = bars + nst;
   uint64_t* a_full = bars + 2 * nst;
@@ -94,8 +101,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(a_empty, 1);
     mbar_init(&acc_full[0], 1);
     mbar_init(&acc_full[1], 1);
-    mbar_init(&acc_empty[0], 128);
-    mbar_init(&acc_empty[1], 128);
+    mbar_init(&acc_empty[0], kEpiThreads);
+    mbar_init(&acc_empty[1], kEpiThreads);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -205,11 +212,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // ----------------------------------------------------------- epilogue
+    const int ew = warp - 2;                // 0 .. EW-1
     const int g = warp & 3;                 // TMEM lane group this warp may access
+    const int half = ew / 4;                // column group of this warp
     const int row_in_tile = g * 32 + lane;
-    const int et = threadIdx.x - 64;        // 0..127
+    const int et = threadIdx.x - 64;        // 0 .. kEpiThreads-1
     float* spill = spill_all + et * kSpillStride;
-    float* nx_smem = nx_all;                // [2][kTcBN] column norms of the current / next tile
+    // Warp-private double buffer of this warp's column norms (kWarpCols per
+    // tile): no barrier with the other epilogue warps is ever needed.
+    constexpr int kWarpCols = kChunks * 32;
+    float* nxw = nx_all + ew * 2 * kWarpCols;
     uint32_t acc_it = 0;
     for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
       const int t = u / p.S, s = u % p.S;
@@ -217,26 +229,32 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
       const int row = t * kTcBM + row_in_tile;
       const bool valid = row < p.m;
+      const int c0 = half * kChunks;  // first 32-column chunk of this warp
       Sink sink;
-      if (valid)
-        sink.init(p.sink, row, s, p.E[row], p.exclude_self ? (int)(p.q_offset + row) : -1);
-      // column norms of the unit's first tile
-      {
-        const float2 nn = __ldg(reinterpret_cast<const float2*>(p.nx + (size_t)j0 * kTcBN) + et);
-        reinterpret_cast<float2*>(nx_smem)[et] = nn;
+      if (valid) {
+        const int orig = p.perm ? p.perm[row] : row;
+        sink.init(p.sink, row, s * kHalves + half, p.E[row],
+                  p.exclude_self ? (int)(p.q_offset + orig) : -1);
       }
-      named_bar_sync(1, 128);
+      // column norms of the unit's first tile
+      for (int i = lane; i < kWarpCols; i += 32)
+        nxw[i] = __ldg(p.nx + (size_t)j0 * kTcBN + c0 * 32 + i);
+      __syncwarp();
       int nb = 0;
       for (int j = j0; j < j1; ++j) {
         // prefetch the next tile's norms; they land in smem after this tile
-        float2 nn_next = make_float2(0.f, 0.f);
-        if (j + 1 < j1)
-          nn_next = __ldg(reinterpret_cast<const float2*>(p.nx + (size_t)(j + 1) * kTcBN) + et);
-        const float* nxs = nx_smem + nb * kTcBN;
+        float nn_next[kWarpCols / 32];
+#pragma unroll
+        for (int i = 0; i < kWarpCols / 32; ++i)
+          nn_next[i] = (j + 1 < j1) ? __ldg(p.nx + (size_t)(j + 1) * kTcBN + c0 * 32 + lane + 32 * i)
+                                    : 0.0f;
+        // the other warps' k-th values for this query: consumed after the tile
+        const uint32_t shared_key = valid ? sink.tile_fetch() : 0u;
+        const float* nxs = nxw + nb * kWarpCols;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
         if (!mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)) goto epi_done;
         tc_fence_after();
-        const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN;
+        const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN + c0 * 32;
         auto process = [&](const uint32_t(&r)[32], int c) {
           const float4* np = reinterpret_cast<const float4*>(nxs + c * 32);
           float v[32];
@@ -252,34 +270,37 @@ __global__ void __launch_bounds__(kThreads, 1)
             v[4 * q4 + 2] = a2;
             v[4 * q4 + 3] = a3;
           }
-          if (valid) sink.offer32(v, j * kTcBN + c * 32, spill);
+          if (valid) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
         };
         // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
         uint32_t ra[32], rb[32];
         tmem_ld_32x32b_x32(tbase, ra);
         tmem_ld_wait_regs(ra);
 #pragma unroll 1
-        for (int c = 0; c < kTcBN / 32; c += 2) {
+        for (int c = 0; c < kChunks; c += 2) {
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, rb);
           process(ra, c);
           tmem_ld_wait_regs(rb);
-          if (c + 2 < kTcBN / 32) {
+          if (c + 2 < kChunks) {
             tmem_ld_32x32b_x32(tbase + (c + 2) * 32, ra);
             process(rb, c + 1);
             tmem_ld_wait_regs(ra);
           } else {
-            // every column of this accumulator is in registers: hand it back
+            // all of this warp's columns are in registers: hand the buffer back
             tc_fence_before();
             mbar_arrive(&acc_empty[buf]);
             process(rb, c + 1);
           }
         }
         ++acc_it;
-        reinterpret_cast<float2*>(nx_smem + (nb ^ 1) * kTcBN)[et] = nn_next;
-        named_bar_sync(1, 128);
+        if (valid) sink.tile_apply(shared_key);
+#pragma unroll
+        for (int i = 0; i < kWarpCols / 32; ++i) nxw[(nb ^ 1) * kWarpCols + lane + 32 * i] = nn_next[i];
+        __syncwarp();
         nb ^= 1;
       }
       if (valid) {
+        sink.tile_sync();
         sink.finish(p.sink);
       }
     }
@@ -294,22 +315,32 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-template <class Sink, bool A_STREAM>
+template <class Sink, bool A_STREAM, int EW>
 int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcParams& p, int grid,
-                      size_t smem, cudaStream_t st) {
-  auto kern = screen_tc_kernel<Sink, A_STREAM>;
+                      cudaStream_t st) {
+  const size_t budget = 227 * 1024;
+  int stages = 8;
+  while (stages > 2 && tc_smem_bytes(p.KB, stages, A_STREAM, EW) > budget) --stages;
+  TcParams q = p;
+  q.stages = stages;
+  const size_t smem = tc_smem_bytes(p.KB, stages, A_STREAM, EW);
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
-  kern<<<grid, kThreads, smem, st>>>(*ta, *tb, p);
+  kern<<<grid, 64 + 32 * EW, smem, st>>>(*ta, *tb, q);
   return (int)cudaGetLastError();
 }
 
 }  // namespace
 
+// Column groups (epilogue warps per TMEM lane group) of the kNN screen for k:
+// each group keeps its own candidate lists.
+int tc_column_groups(int k) { return k <= 16 ? 2 : 1; }
+
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                     const SinkArgs& sa, int* status, cudaStream_t st) {
+                     const SinkArgs& sa, int* status, cudaStream_t st, const int* perm) {
   TcParams p{};
   p.m = (int)m;
   p.KB = ix->dp / kTcBK;
@@ -321,26 +352,24 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   p.q_offset = q_offset;
   p.nx = ix->nxh;
   p.E = E;
+  p.perm = perm;
   p.sink = sa;
   p.status = status;
   const bool a_stream = p.KB > 4;
-  const size_t budget = 227 * 1024;
-  int stages = 8;
-  while (stages > 2 && tc_smem_bytes(p.KB, stages, a_stream) > budget) --stages;
-  p.stages = stages;
-  size_t smem = tc_smem_bytes(p.KB, stages, a_stream);
-  int units = p.m_tiles * S;
-  int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
+  const int units = p.m_tiles * S;
+  const int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
   if (grid <= 0) return 0;
   const CUtensorMap* tb = &ix->tmap_b;
-#define B2K_TC_LAUNCH(SINK) \
-  (a_stream ? launch_tc_variant<SINK, true>(tmap_a, tb, p, grid, smem, st) \
-            : launch_tc_variant<SINK, false>(tmap_a, tb, p, grid, smem, st))
-  if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink);
-  if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink);
-  if (sa.k <= 16) return B2K_TC_LAUNCH(KnnSink<16>);
-  if (sa.k <= 32) return B2K_TC_LAUNCH(KnnSink<32>);
-  return B2K_TC_LAUNCH(KnnSink<64>);
+#define B2K_TC_LAUNCH(SINK, EW)                                          \
+  (a_stream ? launch_tc_variant<SINK, true, EW>(tmap_a, tb, p, grid, st) \
+            : launch_tc_variant<SINK, false, EW>(tmap_a, tb, p, grid, st))
+  if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, 4);
+  if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
+  if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 8);
+  if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 8);
+  if (sa.k <= 16) return B2K_TC_LAUNCH(KnnSink<16>, 8);
+  if (sa.k <= 32) return B2K_TC_LAUNCH(KnnSink<32>, 4);
+  return B2K_TC_LAUNCH(KnnSink<64>, 4);
 #undef B2K_TC_LAUNCH
 }
 

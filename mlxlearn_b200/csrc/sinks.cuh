@@ -16,6 +16,7 @@ struct SinkArgs {
   // kNN
   ScreenOut out;
   int k;
+  uint32_t* shared_kth;  // [m_pad] per-query shared k-th key, or null
   // radius
   const float* thr;      // [m_pad] admission threshold per row
   int* rcount;           // [S][m_pad]
@@ -41,8 +42,12 @@ struct KnnSink {
   size_t slot;
   B2K_DEV void init(const SinkArgs& a, int row, int split, float E, int self) {
     slot = (size_t)split * a.out.m_pad + row;
-    tr.init(a.k, E, self, a.out.lists + slot * a.out.cap, a.out.cap);
+    tr.init(a.k, E, self, a.out.lists + slot * a.out.cap, a.out.cap,
+            a.shared_kth ? a.shared_kth + row : nullptr);
   }
+  B2K_DEV void tile_sync() { tr.sync_shared(); }
+  B2K_DEV uint32_t tile_fetch() const { return tr.fetch_shared(); }
+  B2K_DEV void tile_apply(uint32_t key) { tr.apply_shared(key); }
   B2K_DEV void offer32(const float (&v)[32], int col0, float* spill) { tr.offer32(v, col0, spill); }
   B2K_DEV void offer1(float x, int col) {
     if (x <= tr.T && col != tr.self) tr.admit(x, col);
@@ -70,6 +75,9 @@ struct RadiusCountSink {
     }
   }
   B2K_DEV void offer1(float x, int col) { cnt += (x <= T && col != self) ? 1 : 0; }
+  B2K_DEV void tile_sync() {}
+  B2K_DEV uint32_t tile_fetch() const { return 0; }
+  B2K_DEV void tile_apply(uint32_t) {}
   B2K_DEV void finish(const SinkArgs& a) { a.rcount[slot] = cnt; }
 };
 
@@ -93,6 +101,9 @@ struct RadiusFillSink {
   B2K_DEV void offer1(float x, int col) {
     if (x <= T && col != self) *out++ = col;
   }
+  B2K_DEV void tile_sync() {}
+  B2K_DEV uint32_t tile_fetch() const { return 0; }
+  B2K_DEV void tile_apply(uint32_t) {}
   B2K_DEV void finish(const SinkArgs&) {}
 };
 

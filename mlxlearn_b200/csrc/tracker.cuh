@@ -25,26 +25,74 @@
 
 namespace b2k {
 
+// Order-preserving map of floats to unsigned keys (for atomicMin / bisection).
+__device__ __forceinline__ uint32_t float_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+constexpr uint32_t kNoKey = 0xffffffffu;  // "nothing published yet"
+
+// The screens of one query run in several places at once (reference splits
+// on different CTAs, column halves on different warps).  Each publishes its
+// own k-th smallest value to a per-query word in global memory (atomicMin on
+// the ordered key) and reads the others' back once per tile.  Any published
+// value is the k-th smallest of a subset of the query's values, hence >= the
+// final V_k, so min(own, shared) + 2E is still a valid admission threshold.
 template <int KMAX>
 struct RowTracker {
   float kv[KMAX];
   float T;
   float E2;
+  float shared_kth;   // last value read from the shared word
   int cnt;
   int self;
   int cap;
   int2* list;
+  uint32_t* shared;   // per-query shared k-th key (may be null)
+  bool dirty;         // own k-th improved since the last publish
 
-  B2K_DEV void init(int k, float E, int self_col, int2* lst, int cap_) {
+  B2K_DEV void init(int k, float E, int self_col, int2* lst, int cap_, uint32_t* shared_word) {
 #pragma unroll
     for (int i = 0; i < KMAX; ++i) kv[i] = (i < KMAX - k) ? -INFINITY : INFINITY;
     T = INFINITY;
     E2 = __fmul_ru(2.0f, E);
+    shared_kth = INFINITY;
     cnt = 0;
     self = self_col;
     list = lst;
     cap = cap_;
+    shared = shared_word;
+    dirty = false;
   }
+
+  B2K_DEV void update_threshold() { T = __fadd_ru(fminf(kv[KMAX - 1], shared_kth), E2); }
+
+  // Once per tile, in two halves so the L2 round trip overlaps the tile's
+  // work: fetch_shared() issues the load (start of tile), apply_shared()
+  // publishes our k-th if it improved and folds the fetched value in (end).
+  B2K_DEV uint32_t fetch_shared() const {
+    uint32_t key = kNoKey;
+    if (shared) asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(key) : "l"(shared));
+    return key;
+  }
+  B2K_DEV void apply_shared(uint32_t key) {
+    if (!shared) return;
+    if (dirty) {
+      atomicMin(shared, float_key(kv[KMAX - 1]));
+      dirty = false;
+    }
+    if (key != kNoKey) {
+      const float g = key_float(key);
+      if (g < shared_kth) {
+        shared_kth = g;
+        update_threshold();
+      }
+    }
+  }
+  B2K_DEV void sync_shared() { apply_shared(fetch_shared()); }
 
   // Caller guarantees v <= T and col is not the excluded self column.
   B2K_DEV void admit(float v, int col) {
@@ -54,34 +102,44 @@ struct RowTracker {
 #pragma unroll
       for (int i = KMAX - 1; i > 0; --i) kv[i] = fminf(kv[i], fmaxf(kv[i - 1], v));
       kv[0] = fminf(kv[0], v);
-      T = __fadd_ru(kv[KMAX - 1], E2);
+      update_threshold();
+      dirty = true;
     }
   }
 
   // Offer 32 consecutive columns col0.. whose values are in v[]; `spill` is
   // this thread's 33-float scratch in shared memory (slow path only).
+  // Minima of the four 8-column groups, then of the chunk; only groups whose
+  // minimum passes are spilled and scanned (a warp pays for a group if any of
+  // its 32 rows admits there).
   B2K_DEV void offer32(const float (&v)[32], int col0, float* spill) {
-    float a[11];
+    float g[4];
 #pragma unroll
-    for (int i = 0; i < 10; ++i) a[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
-    a[10] = fminf(v[30], v[31]);
-    float b0 = min3f(a[0], a[1], a[2]), b1 = min3f(a[3], a[4], a[5]);
-    float b2 = min3f(a[6], a[7], a[8]), b3 = fminf(a[9], a[10]);
-    float mn = fminf(min3f(b0, b1, b2), b3);
-    if (mn <= T) {
-      // T only decreases while admitting, so `mask` is a superset of the
-      // columns that will be admitted.
-      uint32_t mask = 0;
+    for (int q = 0; q < 4; ++q) {
+      const float a = min3f(v[8 * q], v[8 * q + 1], v[8 * q + 2]);
+      const float b = min3f(v[8 * q + 3], v[8 * q + 4], v[8 * q + 5]);
+      g[q] = min3f(a, b, fminf(v[8 * q + 6], v[8 * q + 7]));
+    }
+    if (fminf(min3f(g[0], g[1], g[2]), g[3]) <= T) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        mask |= (v[i] <= T ? 1u : 0u) << i;
-        spill[i] = v[i];
-      }
-      while (mask) {
-        const int i = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const float x = spill[i];
-        if (x <= T && col0 + i != self) admit(x, col0 + i);
+      for (int q = 0; q < 4; ++q) {
+        if (g[q] <= T) {
+          // T only decreases while admitting, so `mask` is a superset of the
+          // columns that will be admitted.
+          uint32_t mask = 0;
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            mask |= (v[8 * q + e] <= T ? 1u : 0u) << e;
+            spill[e] = v[8 * q + e];
+          }
+          while (mask) {
+            const int e = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float x = spill[e];
+            const int col = col0 + 8 * q + e;
+            if (x <= T && col != self) admit(x, col);
+          }
+        }
       }
     }
   }

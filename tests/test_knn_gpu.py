@@ -200,3 +200,23 @@ def test_device_query_matches_host(rng):
     dd, di = index.query_device(torch.from_numpy(Q).cuda(), 8)
     np.testing.assert_array_equal(di.cpu().numpy(), hi)
     np.testing.assert_array_equal(dd.cpu().numpy(), hd)
+
+
+@pytest.mark.parametrize("reorder", ["0", "1"])
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_query_grouping_both_ways(mode, reorder, monkeypatch):
+    """Queries are grouped by nearest pivot before the screen (results are
+    written back to the original rows); both orders give the oracle's answer."""
+    monkeypatch.setenv("B2K_REORDER", reorder)
+    C = np.random.default_rng(12).uniform(-1, 1, (64, 40))
+    X, _ = mixture(np.random.default_rng(13), 20000, C, 0.15)
+    Q, _ = mixture(np.random.default_rng(14), 5000, C, 0.15)
+    index = make_index(X)
+    od, oi = oracle.knn(X, Q, 12)
+    dist, idx = index.query(Q, 12, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+    od, oi = oracle.knn(X, X, 6, exclude_self=True)
+    dist, idx = index.query(X, 6, exclude_self=True, mode=mode)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
