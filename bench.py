@@ -315,15 +315,193 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Secondary workloads (not the headline line): --workload pixels|radius|small
+# ---------------------------------------------------------------------------
+
+def _radius_threshold_tuple(d, R2):
+    """(R2, f64_in, f64_out, prune_above, bulk_below) as the reference's
+    radius extension takes it (src/mlxlearn/_kernels/radius_contract.py:129-153,
+    radius_cpu.py:137-140)."""
+    import math
+
+    down = lambda v: math.nextafter(v, -math.inf)  # noqa: E731
+    up = lambda v: math.nextafter(v, math.inf)  # noqa: E731
+    u = 2.0 ** -53
+    g = (d + 2) * u / (1.0 - (d + 2) * u)
+    f_in = max(down(down(R2 * down(1.0 - 2.0 * g))), 0.0)
+    f_out = up(up(R2 * up(1.0 + 2.0 * g)))
+    prune = up(up(R2 * up(1.0 + 4.0 * g)))
+    bulk = max(down(down(R2 * down(1.0 - 4.0 * g))), 0.0)
+    return (float(R2), f_in, f_out, prune, bulk)
+
+
+def _timed_wall(fn, steps, warmup):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        out = fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / steps, out
+
+
+def run_secondary(args):
+    import torch
+
+    from mlxlearn_b200.index import build_index
+    from mlxlearn_b200.neighbors import KNeighborsClassifier, NearestNeighbors
+    from mlxlearn_b200.neighbors import RadiusNeighborsClassifier
+
+    torch.cuda.set_device(0)
+    threads = os.cpu_count() or 1
+    line = {"metric": None, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "workload_kind": "secondary"}
+    import oracle
+
+    ref = oracle.ref_native()
+    if args.workload == "pixels":
+        from datasets import cfg2b
+
+        X, Q, y = cfg2b()
+        k = 5
+        clf = KNeighborsClassifier(n_neighbors=k).fit(X, y)
+        Qd = torch.from_numpy(Q).cuda()
+        ms = 1000 * _timed_wall(lambda: clf._index_.query_device(Qd, k, mode="bf16"),
+                                args.steps, args.warmup)[0]
+        e2e_s, pred = _timed_wall(lambda: clf.predict(Q), args.steps, args.warmup)
+        st = clf._index_.query_device(Qd, k, mode="bf16", stats=True) and clf._index_.last_stats
+        sample = min(len(Q), 4 * threads)
+        rd = np.empty((sample, k)); ri = np.empty((sample, k), np.int64)
+        t0 = time.perf_counter()
+        _ref_knn_threads(ref, X, Q[:sample], k, rd, ri, threads)
+        cpu_qps = sample / (time.perf_counter() - t0)
+        od, oi = clf.kneighbors(Q[:sample])
+        line.update({"metric": "KNeighborsClassifier(k=5).predict queries/s, 60k x 784 pixels",
+                     "value": len(Q) / (ms / 1000), "ms_per_step": ms, "dtype": "bf16",
+                     "config": {"workload": "knn_pixels_60000x784_10000q_k5"},
+                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
+                             "api": "KNeighborsClassifier.predict (host arrays)"},
+                     "screen_stats": st,
+                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
+                                      "kind": "reference" if ref else "port",
+                                      "sample": f"first {sample} queries"},
+                     "parity_vs_cpu_reference": {"indices_bit_exact": bool(np.array_equal(oi, ri)),
+                                                 "max_rel_dist_err": float(np.max(
+                                                     np.abs(od - rd) / np.maximum(rd, 1e-300)))}})
+    elif args.workload == "radius":
+        from datasets import cfg3
+
+        X, y, Q = cfg3()
+        index = build_index(X)
+        # radius: median 50th-neighbour distance over a 1000-query sample
+        d50, _ = index.query(Q[:1000], 50)
+        r = float(np.median(d50[:, -1]))
+        clf = RadiusNeighborsClassifier(radius=r, outlier_label="most_frequent").fit(X, y)
+        e2e_s, pred = _timed_wall(lambda: clf.predict(Q), args.steps, args.warmup)
+        csr_s, parts = _timed_wall(lambda: clf._index_.query_radius_csr(Q, r),
+                                   args.steps, args.warmup)
+        p = parts[0]
+        sample = min(len(Q), 16 * threads)
+        t0 = time.perf_counter()
+        ok = None
+        if ref is not None:
+            thr = _radius_threshold_tuple(X.shape[1], r * r)
+            res = ref.radius.brute_query(X, np.ascontiguousarray(Q[:sample]), thr, 0, False, 1,
+                                         threads)
+            cpu_qps = sample / (time.perf_counter() - t0)
+            nq, nnz = ref.radius.result_sizes(res)
+            counts = np.empty(nq, np.int64)
+            ref.radius.result_counts(res, counts)
+            ip = np.zeros(nq + 1, np.int64)
+            np.cumsum(counts, out=ip[1:])
+            ix = np.empty(nnz, np.int64); dd = np.empty(nnz)
+            ref.radius.result_fill_csr(res, ip, ix, dd, threads)
+            ok = (bool(np.array_equal(ip, p.indptr[:sample + 1]))
+                  and bool(np.array_equal(ix, p.indices[:ip[-1]]))
+                  and bool(np.array_equal(dd, p.distances[:ip[-1]])))
+        else:
+            oracle.radius(X, Q[:sample], r)
+            cpu_qps = sample / (time.perf_counter() - t0)
+        line.update({"metric": "RadiusNeighborsClassifier.predict queries/s, 200k x 32",
+                     "value": len(Q) / csr_s, "ms_per_step": 1000 * csr_s, "dtype": "bf16",
+                     "config": {"workload": "radius_200000x32_50000q", "radius": r,
+                                "median_neighbours": float(np.median(p.lengths())),
+                                "zero_neighbour_queries": int((p.lengths() == 0).sum()),
+                                "nnz": p.nnz,
+                                "value_note": "query_radius_csr through the host C ABI "
+                                              "(upload, screen, exact classify, CSR download)"},
+                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
+                             "api": "RadiusNeighborsClassifier.predict (host arrays)"},
+                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
+                                      "kind": "reference" if ref else "port",
+                                      "sample": f"first {sample} queries, brute_query"},
+                     "parity_vs_cpu_reference": {"csr_bit_exact": ok}})
+    else:  # small: config 1
+        from datasets import cfg1
+
+        X, Q = cfg1()
+        nn = NearestNeighbors(n_neighbors=5, algorithm="brute", metric="euclidean").fit(X)
+        Qd = torch.from_numpy(Q).cuda()
+        ms = 1000 * _timed_wall(lambda: nn._index_.query_device(Qd, 5), args.steps,
+                                args.warmup)[0]
+        e2e_s, (od, oi) = _timed_wall(lambda: nn.kneighbors(Q), args.steps, args.warmup)
+        rd = np.empty((len(Q), 5)); ri = np.empty((len(Q), 5), np.int64)
+        t0 = time.perf_counter()
+        _ref_knn_threads(ref, X, Q, 5, rd, ri, threads)
+        cpu_qps = len(Q) / (time.perf_counter() - t0)
+        line.update({"metric": "NearestNeighbors(k=5).kneighbors queries/s, 10000 x 64",
+                     "value": len(Q) / (ms / 1000), "ms_per_step": ms, "dtype": "auto",
+                     "config": {"workload": "knn_gauss_10000x64_2000q_k5"},
+                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
+                             "api": "NearestNeighbors.kneighbors (host arrays)"},
+                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
+                                      "kind": "reference" if ref else "port",
+                                      "sample": "all 2000 queries"},
+                     "parity_vs_cpu_reference": {"indices_bit_exact": bool(np.array_equal(oi, ri))}})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _ref_knn_threads(ref, X, Q, k, dist, idx, threads):
+    """The reference's exact native kNN scan over query blocks in threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+
+    if ref is None:
+        d, i = oracle.knn(X, Q, k, nthreads=threads)
+        dist[:] = d
+        idx[:] = i
+        return
+    Q = np.ascontiguousarray(Q)
+    chunks = np.array_split(np.arange(len(Q)), threads)
+
+    def run(rows):
+        if len(rows):
+            a, b = rows[0], rows[-1] + 1
+            ref.neighbors.query(X, Q[a:b], k, False, 0, dist[a:b], idx[a:b])
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(run, chunks))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="knn", choices=["knn", "pixels", "radius", "small"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload != "knn":
+        return run_secondary(args)
     return run_ours(args)
 
 

@@ -1,0 +1,165 @@
+"""Estimator API: parity with the reference's outputs (GPU) and its
+validation / error behaviour (CPU)."""
+from __future__ import annotations
+
+import pickle
+import warnings
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from datasets import mixture, pixels
+from mlxlearn_b200.exceptions import (
+    SparseInputError,
+    UnsupportedInputError,
+    UnsupportedParameterError,
+)
+from mlxlearn_b200.neighbors import (
+    KNeighborsClassifier,
+    KNeighborsRegressor,
+    NearestNeighbors,
+    RadiusNeighborsClassifier,
+    RadiusNeighborsRegressor,
+)
+
+gpu = pytest.mark.gpu
+
+
+def radius_data():
+    rng = np.random.default_rng(4)
+    cen = rng.normal(0, 2.0, (10, 32))
+    X, y = mixture(rng, 20000, cen, 1.0)
+    Q, _ = mixture(np.random.default_rng(44), 500, cen, 1.0)
+    Q[:5] += 40.0
+    return X, y, Q
+
+
+# ------------------------------------------------------------------ CPU side
+
+@pytest.mark.parametrize("kw,param", [({"metric": "manhattan"}, "metric"),
+                                      ({"metric": "minkowski", "p": 1}, "p"),
+                                      ({"metric_params": {"w": 1}}, "metric_params"),
+                                      ({"algorithm": "kd_tree"}, "algorithm")])
+def test_capability_errors_raise_before_any_device_use(kw, param):
+    X = np.random.default_rng(0).random((10, 3))
+    with pytest.raises(UnsupportedParameterError) as e:
+        NearestNeighbors(**kw).fit(X)
+    assert e.value.parameter == param
+    assert isinstance(e.value, ValueError)
+
+
+def test_callable_weights_and_sparse_and_overflow_rejected():
+    from scipy import sparse
+
+    X = np.random.default_rng(0).random((10, 3))
+    y = np.arange(10) % 2
+    with pytest.raises(UnsupportedParameterError):
+        KNeighborsClassifier(weights=lambda d: d).fit(X, y)
+    with pytest.raises(SparseInputError, match="sparse"):
+        NearestNeighbors().fit(sparse.csr_matrix(X))
+    big = X.copy()
+    big[0, 0] = 1e300
+    with pytest.raises(UnsupportedInputError):
+        NearestNeighbors().fit(big)
+
+
+def test_sklearn_estimator_protocol():
+    from sklearn.base import clone
+
+    est = KNeighborsClassifier(n_neighbors=7, weights="distance")
+    c = clone(est)
+    assert c.get_params()["n_neighbors"] == 7 and c.get_params()["weights"] == "distance"
+    assert NearestNeighbors().get_params()["radius"] == 1.0
+
+
+# ------------------------------------------------------------------ GPU side
+
+@gpu
+def test_classifier_regressor_match_reference_predictions():
+    X, y, Q = radius_data()
+    g = golden("predict_mixture32.npz")
+    clf = KNeighborsClassifier(n_neighbors=9, weights="distance").fit(X, y)
+    np.testing.assert_array_equal(clf.predict(Q), g["cls"])
+    np.testing.assert_allclose(clf.predict_proba(Q), g["proba"], rtol=1e-12, atol=1e-12)
+    reg = KNeighborsRegressor(n_neighbors=9).fit(X, y.astype(np.float64) * 0.5)
+    np.testing.assert_allclose(reg.predict(Q), g["reg"], rtol=1e-12)
+    assert clf.last_query_backend_ == "cuda"
+
+
+@gpu
+def test_pixel_classifier_matches_reference():
+    rng = np.random.default_rng(7)
+    X, y, T = pixels(rng, 8000)
+    Q, _, _ = pixels(rng, 200, templates=T)
+    g = golden("knn_pixels784.npz")
+    clf = KNeighborsClassifier(n_neighbors=5).fit(X, y)
+    d, i = clf.kneighbors(Q)
+    np.testing.assert_array_equal(i, g["idx"])
+    np.testing.assert_array_equal(clf.predict(Q), g["pred"])
+
+
+@gpu
+def test_radius_classifier_matches_reference():
+    X, y, Q = radius_data()
+    g = golden("radius_mixture32.npz")
+    r = float(g["radius"])
+    clf = RadiusNeighborsClassifier(radius=r, outlier_label="most_frequent").fit(X, y)
+    np.testing.assert_array_equal(clf.predict(Q), g["pred"])
+    np.testing.assert_allclose(clf.predict_proba(Q), g["proba"], rtol=1e-12, atol=1e-12)
+    rd, ri = clf.radius_neighbors(Q)
+    assert rd.dtype == object and ri.dtype == object and len(ri) == len(Q)
+    np.testing.assert_array_equal(np.concatenate(ri), g["indices"])
+    np.testing.assert_array_equal(np.concatenate(rd), g["dist"])
+    with pytest.raises(ValueError, match="No neighbors found"):
+        RadiusNeighborsClassifier(radius=r).fit(X, y).predict(Q)
+
+
+@gpu
+def test_radius_regressor_nan_and_warning():
+    X, y, Q = radius_data()
+    reg = RadiusNeighborsRegressor(radius=6.25).fit(X, y.astype(np.float64))
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        pred = reg.predict(Q)
+    counts = np.array([len(r) for r in reg.radius_neighbors(Q, return_distance=False)])
+    assert np.isnan(pred[:5]).all()
+    np.testing.assert_array_equal(np.isnan(pred), counts == 0)
+    assert any("no neighbors" in str(x.message) for x in w)
+
+
+@gpu
+def test_kneighbors_self_query_graph_and_errors(rng):
+    X = rng.normal(size=(1500, 4)).astype(np.float32)
+    nn = NearestNeighbors(n_neighbors=3).fit(X)
+    d, i = nn.kneighbors()
+    assert not np.any(i == np.arange(1500)[:, None])
+    from sklearn.neighbors import NearestNeighbors as SkNN
+
+    sd, si = SkNN(n_neighbors=3, algorithm="brute").fit(X.astype(np.float64)).kneighbors()
+    np.testing.assert_array_equal(i, si)
+    np.testing.assert_allclose(d, sd, rtol=1e-6, atol=1e-6)
+    G = nn.kneighbors_graph(X[:10], mode="distance")
+    assert G.shape == (10, 1500) and G.nnz == 30
+    with pytest.raises(ValueError, match="Expected n_neighbors <= n_samples_fit"):
+        nn.kneighbors(X[:2], n_neighbors=1501)
+    with pytest.raises(ValueError, match="Expected n_neighbors < n_samples_fit"):
+        nn.kneighbors(n_neighbors=1500)
+    with pytest.raises(ValueError, match="Expected n_neighbors > 0"):
+        nn.kneighbors(X[:2], n_neighbors=0)
+    with pytest.raises(TypeError, match="does not take"):
+        nn.kneighbors(X[:2], n_neighbors=2.5)
+    Gr = nn.radius_neighbors_graph(X[:10], radius=0.5, mode="connectivity")
+    assert Gr.shape == (10, 1500)
+    with pytest.raises(ValueError, match="return_distance must be True"):
+        nn.radius_neighbors(X[:2], return_distance=False, sort_results=True)
+
+
+@gpu
+def test_pickle_roundtrip(rng):
+    X = rng.normal(size=(800, 6)).astype(np.float32)
+    y = (X[:, 0] > 0).astype(int)
+    clf = KNeighborsClassifier(n_neighbors=4).fit(X, y)
+    before = clf.predict(X[:50])
+    clone = pickle.loads(pickle.dumps(clf))
+    np.testing.assert_array_equal(clone.predict(X[:50]), before)
