@@ -136,6 +136,32 @@ B2K_API int b2k_knn_device_noalloc(b2k_index *index, const float *dQ, int64_t m,
                                    int32_t exclude_self, int64_t q_offset, double *d_dist,
                                    int64_t *d_idx, void *stream);
 
+/* Backward of selected kNN distances, all pointers on the device, enqueued on
+ * `stream` (no synchronisation).  idx int64[m, k] fixes the neighbours;
+ * grad float32[m, k] is d(loss)/d(distance); squared != 0 differentiates
+ * s = ||q - x||^2, else e = sqrt(s) (dist = the forward e, float32[m, k]).
+ * Writes grad_q float32[m, d] and/or grad_x float32[n, d] (either may be
+ * NULL).  The reference scatter-add is deterministic (no float atomics).
+ * No counterpart in the reference (mlxlearn has no differentiable kNN); it
+ * backs the torch.autograd.Function in mlxlearn_b200/autograd.py. */
+B2K_API int b2k_knn_backward(const float *dQ, int64_t m, const float *dX, int64_t n, int32_t d,
+                             int32_t k, const int64_t *d_idx, const float *d_grad,
+                             const float *d_dist, int32_t squared, float *d_grad_q,
+                             float *d_grad_x, void *stream);
+
+/* Class votes of kNN results on the device (all pointers device, on
+ * `stream`; the call synchronises).  codes int32[n_train] are class codes
+ * 0..n_classes-1; votes float64[m, n_classes] receives per-class totals (1 or
+ * 1/d, zero-distance rows use the 0/1 indicator of their zero entries);
+ * pred int64[m] (or NULL) the first maximum (ties -> smallest code).
+ * Returns B2K_EINVAL "All neighbors of some sample are getting zero weights."
+ * when a row's weights sum to zero.  Replaces the reference's device votes
+ * (src/mlxlearn_device/_neighbors_votes.py:12-244) and host np.add.at path
+ * (src/mlxlearn/neighbors/_classification.py:150-163). */
+B2K_API int b2k_class_votes(const int64_t *d_idx, const double *d_dist, int64_t m, int32_t k,
+                            const int32_t *d_codes, int32_t n_classes, int32_t weighted,
+                            double *d_votes, int64_t *d_pred, void *stream);
+
 /* ----------------------------------------------------------------- radius */
 
 typedef struct b2k_radius_result b2k_radius_result;

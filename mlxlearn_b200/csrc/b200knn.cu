@@ -918,6 +918,50 @@ int b2k_radius_result_fetch(const b2k_radius_result* res, int64_t* indptr, int64
   return B2K_OK;
 }
 
+int b2k_knn_backward(const float* dQ, int64_t m, const float* dX, int64_t n, int32_t d,
+                     int32_t k, const int64_t* d_idx, const float* d_grad, const float* d_dist,
+                     int32_t squared, float* d_grad_q, float* d_grad_x, void* stream) {
+  if (m < 0 || n <= 0 || d <= 0 || k <= 0) return fail(B2K_EINVAL, "invalid backward shapes");
+  if (m > 0 && (!dQ || !dX || !d_idx || !d_grad))
+    return fail(B2K_EINVAL, "backward inputs must not be NULL");
+  if (!squared && !d_dist)
+    return fail(B2K_EINVAL, "the euclidean backward needs the forward distances");
+  if (fault_mode() == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* ws = nullptr;
+  int rc = 0;
+  if (d_grad_x) {
+    if ((rc = dalloc(&ws, knn_backward_workspace_ints(m, n, k), st))) return rc;
+  }
+  const int e = knn_backward(dQ, m, dX, n, d, k, d_idx, d_grad, squared ? nullptr : d_dist,
+                             squared, d_grad_q, d_grad_x, ws, st);
+  if (ws) cudaFreeAsync(ws, st);
+  if (e) return fail(B2K_ECUDA, "backward launch failed: %s", cudaGetErrorString((cudaError_t)e));
+  return B2K_OK;
+}
+
+int b2k_class_votes(const int64_t* d_idx, const double* d_dist, int64_t m, int32_t k,
+                    const int32_t* d_codes, int32_t n_classes, int32_t weighted,
+                    double* d_votes, int64_t* d_pred, void* stream) {
+  if (m < 0 || k <= 0 || n_classes <= 0) return fail(B2K_EINVAL, "invalid vote shapes");
+  if (m > 0 && (!d_idx || !d_codes || !d_votes)) return fail(B2K_EINVAL, "NULL vote buffer");
+  if (weighted && !d_dist) return fail(B2K_EINVAL, "distance weights need distances");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* status = nullptr;
+  int rc = dalloc(&status, 1, st);
+  if (rc) return rc;
+  B2K_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+  launch_votes(d_idx, d_dist, m, k, d_codes, n_classes, weighted, d_votes, d_pred, status, st);
+  int h = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(status, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(B2K_ECUDA, "votes failed: %s", cudaGetErrorString(e));
+  if (h) return fail(B2K_EINVAL, "All neighbors of some sample are getting zero weights.");
+  return B2K_OK;
+}
+
 int b2k_radius_result_release(b2k_radius_result* res) {
   if (!res) return B2K_OK;
   cudaSetDevice(res->device);

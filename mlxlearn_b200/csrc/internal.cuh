@@ -160,6 +160,17 @@ void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int
                           int grid, cudaStream_t st);
 int radius_sort_cap();
 
+// ------------------------------------------------------------------- votes
+void launch_votes(const int64_t* idx, const double* dist, int64_t m, int k, const int* codes,
+                  int n_classes, int weighted, double* votes, int64_t* pred, int* status,
+                  cudaStream_t st);
+
+// ---------------------------------------------------------------- backward
+int knn_backward(const float* Q, int64_t m, const float* X, int64_t n, int d, int k,
+                 const int64_t* idx, const float* G, const float* E, int squared, float* dQ,
+                 float* dX, int* workspace, cudaStream_t st);
+size_t knn_backward_workspace_ints(int64_t m, int64_t n, int k);
+
 // helpers
 int report_error(int code, const char* msg);  // sets b2k_last_error(), returns code
 int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,

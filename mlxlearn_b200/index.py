@@ -39,12 +39,40 @@ class NeighborIndex:
         if X.shape[0] >= 2**31:
             raise ValueError("training row count must fit int32 indices")
         self._host_X = X
+        self._n, self._d = int(X.shape[0]), int(X.shape[1])
         self.device = int(device)
         self.mode = mode
         self._handle = None
         self._lock = threading.Lock()
         self.last_query_backend = None
         self.last_stats = None
+
+    @classmethod
+    def from_device(cls, X, *, mode: str = "auto") -> "NeighborIndex":
+        """Index over a CUDA float32 tensor ``[n, d]`` (copied on the current
+        stream; no host round trip).  ``training_data`` is downloaded lazily."""
+        import torch
+
+        if not (isinstance(X, torch.Tensor) and X.is_cuda and X.dim() == 2):
+            raise TypeError("from_device expects a 2-D CUDA tensor")
+        if 0 in X.shape:
+            raise ValueError("X must be a nonempty two-dimensional matrix")
+        Xc = X.detach().to(torch.float32).contiguous()
+        self = cls.__new__(cls)
+        self._host_X = None
+        self._n, self._d = int(Xc.shape[0]), int(Xc.shape[1])
+        self.device = Xc.device.index or 0
+        self.mode = mode
+        self._lock = threading.Lock()
+        self.last_query_backend = None
+        self.last_stats = None
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        stream = torch.cuda.current_stream(Xc.device).cuda_stream
+        _lib.check(lib.b2k_index_create_device(Xc.data_ptr(), self._n, self._d, stream,
+                                               ctypes.byref(h)), "b2k_index_create_device")
+        self._handle = h
+        return self
 
     # ------------------------------------------------------------ lifetime
     def _ensure_device(self):
@@ -74,7 +102,7 @@ class NeighborIndex:
     def __getstate__(self):
         # Host rows and parameters only; the device index is rebuilt lazily
         # (reference distance.py:191-209).
-        return {"X": self._host_X, "device": self.device, "mode": self.mode}
+        return {"X": self.training_data, "device": self.device, "mode": self.mode}
 
     def __setstate__(self, state):
         self.__init__(state["X"], device=state.get("device", 0), mode=state.get("mode", "auto"))
@@ -82,19 +110,24 @@ class NeighborIndex:
     # ----------------------------------------------------------- properties
     @property
     def training_data(self) -> np.ndarray:
+        if self._host_X is None:
+            X = np.empty((self._n, self._d), dtype=NUMPY_FLOAT)
+            _lib.check(_lib.load().b2k_index_download(self._handle, X.ctypes.data),
+                       "b2k_index_download")
+            self._host_X = X
         return self._host_X
 
     @property
     def X(self) -> np.ndarray:
-        return self._host_X
+        return self.training_data
 
     @property
     def n_samples(self) -> int:
-        return int(self._host_X.shape[0])
+        return self._n
 
     @property
     def n_features(self) -> int:
-        return int(self._host_X.shape[1])
+        return self._d
 
     # -------------------------------------------------------------- queries
     def _check_query(self, n_query: int, k: int, exclude_self: bool):

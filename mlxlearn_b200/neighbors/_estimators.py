@@ -10,7 +10,6 @@ from sklearn.base import BaseEstimator, ClassifierMixin, RegressorMixin
 from sklearn.utils.validation import check_is_fitted
 
 from ._base import NeighborsMixin, RadiusMixin, compute_weights
-from ._votes import class_votes
 
 __all__ = ["NearestNeighbors", "KNeighborsClassifier", "KNeighborsRegressor",
            "RadiusNeighborsClassifier", "RadiusNeighborsRegressor"]
@@ -64,26 +63,50 @@ class KNeighborsClassifier(NeighborsMixin, ClassifierMixin, BaseEstimator):
         return self
 
     def _votes(self, X):
+        """Search and vote on the GPU; one host transfer of the result
+        (reference _classification.py:126-186)."""
+        import torch
+
+        from .. import _lib
+
         if self.weights not in (None, "uniform", "distance"):
             raise ValueError("weights not recognized: should be 'uniform' or 'distance', "
                              f"got {self.weights!r}")
-        need_distance = self.weights == "distance"
-        if need_distance:
-            dist, idx = self.kneighbors(X, return_distance=True)
-        else:
-            dist, idx = None, self.kneighbors(X, return_distance=False)
-        w = compute_weights(dist, self.weights)
-        return class_votes(idx, self._y, len(self.classes_), w)
+        weighted = self.weights == "distance"
+        Q, k, query_is_train = self._prepare_neighbor_query(X)
+        dev = torch.device("cuda", self._index_.device)
+        codes = self.__dict__.get("_codes_dev")
+        if codes is None:
+            codes = torch.from_numpy(self._y.astype(np.int32)).to(dev)
+            self.__dict__["_codes_dev"] = codes
+        Qd = torch.from_numpy(np.ascontiguousarray(Q)).to(dev)
+        dist, idx = self._index_.query_device(Qd, k, return_distance=weighted,
+                                              exclude_self=query_is_train)
+        m, n_classes = idx.shape[0], len(self.classes_)
+        votes = torch.empty((m, n_classes), dtype=torch.float64, device=dev)
+        pred = torch.empty(m, dtype=torch.int64, device=dev)
+        rc = _lib.load().b2k_class_votes(
+            idx.data_ptr(), None if dist is None else dist.data_ptr(), m, k, codes.data_ptr(),
+            n_classes, int(weighted), votes.data_ptr(), pred.data_ptr(),
+            torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(rc, "b2k_class_votes")
+        self._last_query_backend = "cuda"
+        return votes.cpu().numpy(), pred.cpu().numpy()
 
     def predict(self, X):
         check_is_fitted(self, "_index_")
-        votes = self._votes(X)
-        return self.classes_.take(votes.argmax(axis=1))
+        _, pred = self._votes(X)
+        return self.classes_.take(pred)
 
     def predict_proba(self, X):
         check_is_fitted(self, "_index_")
-        votes = self._votes(X)
+        votes, _ = self._votes(X)
         return votes / votes.sum(axis=1, keepdims=True)
+
+    def __getstate__(self):
+        state = dict(self.__dict__)
+        state.pop("_codes_dev", None)  # device copy of the labels, rebuilt lazily
+        return state
 
 
 class KNeighborsRegressor(NeighborsMixin, RegressorMixin, BaseEstimator):

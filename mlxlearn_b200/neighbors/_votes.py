@@ -1,9 +1,6 @@
 """Vote and mean reductions over neighbour sets.
 
-kNN votes follow the reference's host path (src/mlxlearn/neighbors/
-_classification.py:150-163): per-query class totals of 1 or 1/d weights,
-accumulated in neighbour order; ``argmax`` then picks the first maximum, i.e.
-ties go to the smallest class code.  Radius votes/means follow
+kNN votes run on the GPU (csrc/votes.cu, b2k_class_votes).  Radius votes/means follow
 src/mlxlearn/_kernels/radius_reduce.py:19-94 (``bincount`` in ascending
 training-index order, so the result does not depend on batching).
 """
@@ -12,14 +9,6 @@ from __future__ import annotations
 import numpy as np
 
 from ..radius_result import RadiusCSR
-
-
-def class_votes(idx: np.ndarray, codes: np.ndarray, n_classes: int,
-                weights: np.ndarray | None) -> np.ndarray:
-    votes = np.zeros((len(idx), n_classes), dtype=np.float64)
-    rows = np.arange(len(idx))[:, None]
-    np.add.at(votes, (rows, codes[idx]), 1.0 if weights is None else weights)
-    return votes
 
 
 def _distance_weights(result: RadiusCSR, rows: np.ndarray) -> np.ndarray:
