@@ -38,6 +38,10 @@ sys.path.insert(0, os.path.join(REPO, "tests"))
 METRIC = ("exact kNN queries/s at 1M×128 k=10: BF16-screen+certified vs FP32; % TC peak")
 N_REF, N_QUERY, D, K = 1_000_000, 100_000, 128, 10
 WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
+# Our kernels per kNN call: assign, bin_scan, scatter, gather (query grouping),
+# prep_queries, screen_tc, certify, exact (fallback rows; no-op when none).
+LAUNCHES_PER_STEP = 8
+SCREEN_TRAFFIC_BYTES = 5.03e10
 
 
 def peaks():
@@ -262,7 +266,9 @@ def run_ours(args):
         total_timed_s = ms_bf16 * args.steps / 1000.0
         peak = tf_sust if total_timed_s > 1.0 else tf_burst
         fp32_screen_ms = statistics.median(s["screen_ms"] for s in st_fp32)
-        traffic = os.environ.get("B2K_SCREEN_TRAFFIC_BYTES")
+        # DRAM bytes (read + write) of one screen launch, from the ncu capture in
+        # profiles/screen_tc_knn_gauss1Mx128.txt (10k queries, scaled by tile pairs)
+        traffic = os.environ.get("B2K_SCREEN_TRAFFIC_BYTES", SCREEN_TRAFFIC_BYTES)
         result = {
             "metric": METRIC,
             "value": ws * N_QUERY / (ms_bf16 / 1000.0),
@@ -291,7 +297,7 @@ def run_ours(args):
             "e2e": {"value": ws * N_QUERY / e2e_s, "unit": "queries/s",
                     "h2d_bytes_per_step": int(Qh.nbytes),
                     "d2h_bytes_per_step": int(out_i.nbytes + out_d.nbytes)},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": clocks,
         }
         # CPU baseline: the reference's exact CPU scan on a bounded sample, with
@@ -497,12 +503,40 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="knn", choices=["knn", "pixels", "radius", "small"])
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling driver: only the bf16 device-resident steps of the "
+                         "headline workload (no fp32 leg, e2e or CPU baseline)")
+    ap.add_argument("--queries", type=int, default=N_QUERY,
+                    help="query count for --profile (the headline uses 100,000)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile:
+        return run_profile(args)
     if args.workload != "knn":
         return run_secondary(args)
     return run_ours(args)
+
+
+def run_profile(args):
+    """bf16 screen + certify on the headline index, `--queries` queries."""
+    import torch
+
+    from datasets import cfg2a
+    from mlxlearn_b200.index import build_index
+
+    torch.cuda.set_device(0)
+    X, Q = cfg2a(N_REF, args.queries, D)
+    index = build_index(X)
+    Qd = torch.from_numpy(Q).cuda()
+    for _ in range(args.warmup):
+        index.query_device(Qd, K, mode="bf16")
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        index.query_device(Qd, K, mode="bf16", stats=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": True, "queries": args.queries, "stats": index.last_stats}))
+    return 0
 
 
 if __name__ == "__main__":

@@ -22,8 +22,10 @@
 //               last chunk is in registers.  The distance tile never reaches
 //               HBM.
 // A work unit is (query tile of 128 rows, split s of the reference tiles);
-// units are dealt round-robin over the persistent CTAs.  Candidate lists are
-// kept per (split, column half, row).
+// units are dealt round-robin over the persistent CTAs in split-major order,
+// so the CTAs of a wave stream the same reference range (it stays in L2) and
+// later splits start from the k-th values the earlier ones published.
+// Candidate lists are kept per (split, column half, row).
 //
 // Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
 // B = bf16(x - c)); the certified error bound of v = fl32(acc + ||x - c||^2) is
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       prefetch_tmap(&tmB);
       uint32_t stage = 0, phase = 0, a_phase = 0;
       for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const int t = u / p.S, s = u % p.S;
+        const int s = u / p.m_tiles, t = u % p.m_tiles;
         const int j0 = s * p.tiles_per_split;
         const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
         if (!A_STREAM) {
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
       uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0;
       for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const int s = u % p.S;
+        const int s = u / p.m_tiles;
         const int j0 = s * p.tiles_per_split;
         const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
         if (!A_STREAM) {
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     float* nxw = nx_all + ew * 2 * kWarpCols;
     uint32_t acc_it = 0;
     for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-      const int t = u / p.S, s = u % p.S;
+      const int s = u / p.m_tiles, t = u % p.m_tiles;
       const int j0 = s * p.tiles_per_split;
       const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
       const int row = t * kTcBM + row_in_tile;
