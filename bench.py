@@ -199,6 +199,7 @@ def run_ours(args):
     from datasets import cfg2a
     from mlxlearn_b200 import _lib
     from mlxlearn_b200.index import build_index
+    from mlxlearn_b200.sharding import max_over_ranks
 
     X, _ = cfg2a(N_REF, 1, D)
     # each rank answers its own query shard (weak scaling)
@@ -230,9 +231,7 @@ def run_ours(args):
         barrier()
         ms = ev0.elapsed_time(ev1) / steps
         if pg is not None:
-            t = torch.tensor([ms], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms)
         return ms, stats
 
     with ClockSampler(local) as clk:
@@ -253,9 +252,7 @@ def run_ours(args):
     barrier()
     e2e_s = (time.perf_counter() - t0) / args.steps
     if pg is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s)
 
     result = None
     if rank == 0:

@@ -95,17 +95,19 @@ static EncodeTiledFn encode_fn() {
 }
 
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
-                        uint32_t box_inner, uint32_t box_outer) {
+                        uint32_t box_inner, uint32_t box_outer, int swizzle_bytes) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {inner, outer};
   cuuint64_t strides[1] = {inner * 2};
   cuuint32_t box[2] = {box_inner, box_outer};
   cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapSwizzle sw = swizzle_bytes == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                : swizzle_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                      : CU_TENSOR_MAP_SWIZZLE_128B;
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
-                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
@@ -194,6 +196,16 @@ static int ensure_bf16(Index& ix) {
   ix.ex_max = stats[4];
   if (!tensor_map_2d_bf16(&ix.tmap_b, ix.Xh, (uint64_t)ix.dp, (uint64_t)ix.n_pad_tc, kTcBK, kTcBN))
     return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the reference rows");
+  // norm columns of the reference rows and the matching query-side ones
+  B2K_CUDA(cudaMalloc(&ix.Xaug, (size_t)ix.n_pad_tc * kTcAug * sizeof(uint16_t)));
+  B2K_CUDA(cudaMalloc(&ix.aug_ones, (size_t)kTcBM * kTcAug * sizeof(uint16_t)));
+  launch_prep_aug(&ix, st);
+  B2K_CUDA(cudaGetLastError());
+  B2K_CUDA(cudaStreamSynchronize(st));
+  if (!tensor_map_2d_bf16(&ix.tmap_baug, ix.Xaug, kTcAug, (uint64_t)ix.n_pad_tc, kTcAug, kTcBN,
+                          32) ||
+      !tensor_map_2d_bf16(&ix.tmap_aaug, ix.aug_ones, kTcAug, kTcBM, kTcAug, kTcBM, 32))
+    return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the norm columns");
   ix.bf16_ready = true;
   return B2K_OK;
 }
@@ -586,6 +598,8 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.nxh);
   cudaFree(ix.pivots);
   cudaFree(ix.pivot_norms);
+  cudaFree(ix.Xaug);
+  cudaFree(ix.aug_ones);
   if (ix.stream) cudaStreamDestroy(ix.stream);
   delete h;
   return B2K_OK;

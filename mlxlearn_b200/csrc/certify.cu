@@ -31,7 +31,7 @@ constexpr int kCertWarps = 8;
 constexpr int kSurvivorCap = 256;  // candidates that can still reach the top k
 constexpr size_t kCertWarpBytes =
     (size_t)kCertifyCap * (sizeof(int) + sizeof(float)) +
-    (size_t)kSurvivorCap * (sizeof(double) + sizeof(int));
+    (size_t)kSurvivorCap * (sizeof(double) + sizeof(int)) + 256 * sizeof(unsigned);
 
 // |canonical - S| <= g S with g = (d+2)u/(1-(d+2)u), u = 2^-53, for a
 // sequential sum of d non-negative rounded terms (reference
@@ -119,6 +119,59 @@ __device__ unsigned warp_sort_resolve(double* s, int* id, int C, int k, const fl
   return compares;
 }
 
+// k-th smallest (1-based) of `count` unsigned keys, by one warp: four 8-bit
+// radix passes with a 256-bin shared-memory histogram (`hist`).
+template <class KeyFn>
+__device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* hist, int lane) {
+  uint32_t prefix = 0, mask = 0;
+  unsigned rank = (unsigned)k;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = lane; b < 256; b += 32) hist[b] = 0;
+    __syncwarp();
+    for (int i = lane; i < count; i += 32) {
+      const uint32_t key = key_of(i);
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncwarp();
+    unsigned local[8], s = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      local[b] = hist[lane * 8 + b];
+      s += local[b];
+    }
+    unsigned incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const unsigned excl = incl - s;
+    const unsigned owners = __ballot_sync(0xffffffffu, excl < rank && rank <= incl);
+    const int owner = __ffs(owners) - 1;
+    int digit = 0;
+    unsigned before = 0;
+    if (lane == owner) {
+      unsigned acc = excl;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (acc + local[b] >= rank) {
+          digit = lane * 8 + b;
+          break;
+        }
+        acc += local[b];
+      }
+      before = acc;
+    }
+    digit = __shfl_sync(0xffffffffu, digit, owner);
+    before = __shfl_sync(0xffffffffu, before, owner);
+    rank -= before;
+    prefix |= (uint32_t)digit << shift;
+    mask |= 255u << shift;
+    __syncwarp();
+  }
+  return prefix;
+}
+
 // fp32 direct squared distance of candidate rows, 8 lanes per row (coalesced
 // 16-byte loads), so each warp handles 4 candidates per step.  Sum of d
 // non-negative terms, each (fl(q_i - x_i))^2 accumulated with FMA: the result
@@ -130,6 +183,43 @@ __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
   const int grp = lane >> 3, l8 = lane & 7;
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(q) & 15) == 0 &&
                    (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  if (vec && d <= 256) {
+    // the query's 16-byte pieces this lane needs stay in registers
+    const int d4 = d / 4;
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    float4 qr[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int f = l8 + 8 * i;
+      qr[i] = f < d4 ? __ldg(q4 + f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int c0 = 0; c0 < C; c0 += 4) {
+      const int c = c0 + grp;
+      float acc0 = 0.f, acc1 = 0.f;
+      if (c < C) {
+        const float4* x4 = reinterpret_cast<const float4*>(X + (size_t)ci[c] * d);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int f = l8 + 8 * i;
+          if (f < d4) {
+            const float4 b = __ldg(x4 + f);
+            const float e0 = qr[i].x - b.x, e1 = qr[i].y - b.y;
+            const float e2 = qr[i].z - b.z, e3 = qr[i].w - b.w;
+            acc0 = fmaf(e0, e0, acc0);
+            acc1 = fmaf(e1, e1, acc1);
+            acc0 = fmaf(e2, e2, acc0);
+            acc1 = fmaf(e3, e3, acc1);
+          }
+        }
+      }
+      float acc = acc0 + acc1;
+      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      if (l8 == 0 && c < C) cv[c] = acc;
+    }
+    return;
+  }
   for (int c0 = 0; c0 < C; c0 += 4) {
     const int c = c0 + grp;
     float acc0 = 0.f, acc1 = 0.f;
@@ -171,6 +261,7 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
   float* cv = reinterpret_cast<float*>(ci + kCertifyCap);           // [kCertifyCap]
   double* cs = reinterpret_cast<double*>(cv + kCertifyCap);         // [kSurvivorCap]
   int* si = reinterpret_cast<int*>(cs + kSurvivorCap);              // [kSurvivorCap]
+  unsigned* hist = reinterpret_cast<unsigned*>(si + kSurvivorCap);  // [256] radix histogram
   const ScreenOut& so = a.scr;
   const int k = a.k, S = a.S;
 
@@ -189,21 +280,26 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
   }
   entries = __reduce_add_sync(0xffffffffu, entries);
 
-  // 2. V_k by bisection over the splits' k smallest values
+  // 2. V_k = k-th smallest of the lists' k smallest values (radix select)
   const int total = S * k;
-  uint32_t lo = 0, hi = 0xffffffffu;
-  while (lo < hi) {
-    const uint32_t mid = lo + ((hi - lo) >> 1);
-    unsigned cnt = 0;
+  float Vk;
+  if (total <= kCertifyCap) {
+    uint32_t* keys = reinterpret_cast<uint32_t*>(ci);  // ci is free until step 3
     for (int i = lane; i < total; i += 32) {
       const int s = i / k, t = i % k;
-      cnt += float_key(so.kth[((size_t)s * so.m_pad + row) * k + t]) <= mid;
+      keys[i] = float_key(so.kth[((size_t)s * so.m_pad + row) * k + t]);
     }
-    cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (cnt >= (unsigned)k) hi = mid;
-    else lo = mid + 1;
+    __syncwarp();
+    Vk = key_float(warp_radix_kth([&](int i) { return keys[i]; }, total, k, hist, lane));
+    __syncwarp();
+  } else {
+    Vk = key_float(warp_radix_kth(
+        [&](int i) {
+          const int s = i / k, t = i % k;
+          return float_key(so.kth[((size_t)s * so.m_pad + row) * k + t]);
+        },
+        total, k, hist, lane));
   }
-  const float Vk = key_float(lo);
   const float Tf = __fadd_ru(Vk, __fmul_ru(2.0f, a.E[row]));
 
   // 3. gather candidates v <= Tf
@@ -244,18 +340,10 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
   const float g32 = (float)((double)(a.d + 5) * 0x1p-24 * 1.01);
   const float abs32 = (float)a.d * 0x1p-126f;
   const float up_f = 1.0f + g32, lo_f = 1.0f - g32;
-  // 5. U = k-th smallest upper bound (bisection over ordered keys)
-  uint32_t ulo = 0, uhi = 0xffffffffu;
-  while (ulo < uhi) {
-    const uint32_t mid = ulo + ((uhi - ulo) >> 1);
-    unsigned cnt = 0;
-    for (int c = lane; c < C; c += 32)
-      cnt += float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)) <= mid;
-    cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (cnt >= (unsigned)k) uhi = mid;
-    else ulo = mid + 1;
-  }
-  const float U = key_float(ulo);
+  // 5. U = k-th smallest upper bound (radix select over ordered keys)
+  const float U = key_float(warp_radix_kth(
+      [&](int c) { return float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)); }, C, k, hist,
+      lane));
   // 6. survivors: lower bound <= U (everything that can still be in the top k)
   int Cs = 0;
   for (int base = 0; base < C; base += 32) {

@@ -13,6 +13,7 @@ namespace b2k {
 constexpr int kTcBM = 128;   // query rows per tcgen05 tile (TMEM lanes)
 constexpr int kTcBN = 256;   // reference rows per tcgen05 tile (TMEM columns)
 constexpr int kTcBK = 64;    // 16-bit elements per 128-byte swizzle row
+constexpr int kTcAug = 16;   // norm columns appended to every operand row (one K=16 step)
 constexpr int kSimtBM = 128; // query rows per CUDA-core tile
 constexpr int kSimtBN = 128; // reference rows per CUDA-core tile
 constexpr int kListCap = 512;      // screen list entries per (split, query)
@@ -54,6 +55,10 @@ struct Index {
   float* nxh = nullptr;          // [n_pad_tc] fl32(||x||^2), NaN on padding rows
   float xh_max = 0, ex_max = 0;  // max ||bf16 operand||, max ||(x - center) - bf16 operand||
   CUtensorMap tmap_b;            // TMA map over Xh, box 64 x 256
+  uint16_t* Xaug = nullptr;      // [n_pad_tc, 16] bf16 [n_hi, n_mid, n_lo, 0...] of ||x - c||^2
+  uint16_t* aug_ones = nullptr;  // [128, 16] bf16 [1, 1, 1, 0...] (query side)
+  CUtensorMap tmap_baug;         // over Xaug, box 16 x 256, 32-byte swizzle
+  CUtensorMap tmap_aaug;         // over aug_ones, box 16 x 128, 32-byte swizzle
   // pivots for query ordering (reorder.cu)
   int n_pivots = 0;
   float* pivots = nullptr;       // [n_pivots, d] centred rows
@@ -65,6 +70,7 @@ struct Index {
 // ------------------------------------------------------------ prep kernels
 void launch_prep_index(Index* ix, cudaStream_t st);
 void launch_prep_index_bf16(Index* ix, cudaStream_t st);
+void launch_prep_aug(Index* ix, cudaStream_t st);  // Xaug (norm split) and aug_ones
 // Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
 struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
@@ -177,7 +183,7 @@ int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
                    int64_t q_offset);
 Index* index_of(b2k_index* h);
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
-                        uint32_t box_inner, uint32_t box_outer);
+                        uint32_t box_inner, uint32_t box_outer, int swizzle_bytes = 128);
 int num_sms(int device);
 
 }  // namespace b2k

@@ -140,6 +140,37 @@ __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, i
   }
 }
 
+// Norm columns for the tensor-core screen: ||y_x||^2 (float64) as three bf16
+// parts hi + mid + lo (residual below 2^-26 of the value), NaN on padding
+// rows; the query side is [1, 1, 1, 0, ...].
+__global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int64_t n_pad,
+                                __nv_bfloat16* __restrict__ Xaug,
+                                __nv_bfloat16* __restrict__ ones) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < kTcBM) {
+    for (int c = 0; c < kTcAug; ++c)
+      ones[row * kTcAug + c] = __float2bfloat16_rn(c < 3 ? 1.0f : 0.0f);
+  }
+  if (row >= n_pad) return;
+  __nv_bfloat16* a = Xaug + row * kTcAug;
+  for (int c = 3; c < kTcAug; ++c) a[c] = __float2bfloat16_rn(0.0f);
+  if (row >= n) {
+    const __nv_bfloat16 nan = __ushort_as_bfloat16((unsigned short)0x7fc0);
+    a[0] = nan;
+    a[1] = __float2bfloat16_rn(0.0f);
+    a[2] = __float2bfloat16_rn(0.0f);
+    return;
+  }
+  const double v = nx64[row];
+  const __nv_bfloat16 hi = __float2bfloat16_rn((float)v);
+  const double r1 = v - (double)__bfloat162float(hi);
+  const __nv_bfloat16 mid = __float2bfloat16_rn((float)r1);
+  const double r2 = r1 - (double)__bfloat162float(mid);
+  a[0] = hi;
+  a[1] = mid;
+  a[2] = __float2bfloat16_rn((float)r2);
+}
+
 __global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int64_t m_pad,
                                     int d, int dp, int mode, const float* __restrict__ center,
                                     float xh_max, float nx_max, float ex_max,
@@ -187,9 +218,11 @@ __global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int6
     const double qh = sqrt(hn) * (1.0 + 1e-15);
     const double eq = sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy);
     const double XH = xh_max, EX = ex_max, NX = nx_max;
-    const double g = bf16 ? (double)(dp + 16) * 0x1p-20 : (double)(d + 4) * u * 1.01;
+    // tensor cores: dp feature columns + 16 norm columns accumulated in fp32;
+    // the accumulation also carries ||y_x||^2 itself (the g * NX term)
+    const double g = bf16 ? (double)(dp + kTcAug + 16) * 0x1p-20 : (double)(d + 4) * u * 1.01;
     double bound = 2.0 * (qh * EX + eq * XH + eq * EX) + 2.0 * g * qh * XH + 2.0 * u * NX +
-                   2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy;
+                   2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy + (bf16 ? g * NX * 1.01 : 0.0);
     bound = bound * (1.0 + 0x1p-16) + (double)width * 0x1p-120;
     E[row] = __double2float_ru(bound);
     if (nq_out) nq_out[row] = yy;
@@ -217,6 +250,13 @@ void launch_prep_index_bf16(Index* ix, cudaStream_t st) {
   prep_index_bf16_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
       ix->X, ix->n, ix->d, ix->n_pad_tc, ix->dp, ix->center, ix->nx32,
       reinterpret_cast<__nv_bfloat16*>(ix->Xh), ix->nxh, ix->stats_dev);
+}
+
+void launch_prep_aug(Index* ix, cudaStream_t st) {
+  const int64_t rows = ix->n_pad_tc > kTcBM ? ix->n_pad_tc : kTcBM;
+  prep_aug_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
+      ix->nx64, ix->n, ix->n_pad_tc, reinterpret_cast<__nv_bfloat16*>(ix->Xaug),
+      reinterpret_cast<__nv_bfloat16*>(ix->aug_ones));
 }
 
 void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,

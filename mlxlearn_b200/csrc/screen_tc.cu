@@ -5,22 +5,26 @@
 // screen _neighbors_integer.py:40-201), which materialise the distance tile in
 // memory.  Here the tile lives only in TMEM.
 //
+// The accumulator holds the screen value itself, v = ||y_x||^2 - 2 <q^, x^>:
+// besides the dp feature columns, every reference row carries 16 extra bf16
+// columns [n_hi, n_mid, n_lo, 0...] (||y_x||^2 split into three bf16 parts)
+// and every query [1, 1, 1, 0...], so one more K=16 MMA per tile adds the norm.
+//
 // One persistent CTA per SM, warp-specialised:
 //   warp 0      TMA producer: query tile A (128 rows x dp, bf16) once per
-//               work unit; reference tiles B (256 rows x 64 columns) into an
-//               NST-deep shared-memory ring (128-byte swizzle).
+//               work unit; reference tiles B (256 rows x 64 columns, 128-byte
+//               swizzle) into an NST-deep shared-memory ring, the norm
+//               columns (256 rows x 16, 32-byte swizzle) with the last block.
 //   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16, fp32
 //               accumulators in TMEM, double-buffered (2 x 256 columns).
 //   warps 2..   EW epilogue warps.  Warp w reads TMEM lane group w % 4 (the
 //               hardware's rule); with EW = 8 the two warps of a lane group
 //               take the two 128-column halves of each tile.  Per 32-column
-//               chunk: tcgen05.ld (two loads in flight), add ||x||^2 (staged
-//               per tile in shared memory, the next tile's prefetched),
-//               3-input min over the chunk, and only when the minimum passes
-//               the row's threshold, admit columns (sinks.cuh).  The
-//               accumulator is handed back to the MMA warp as soon as its
-//               last chunk is in registers.  The distance tile never reaches
-//               HBM.
+//               chunk: tcgen05.ld (two loads in flight), 3-input min over
+//               8-column groups, and only when a group passes the row's
+//               threshold, admit its columns (sinks.cuh).  The accumulator is
+//               handed back to the MMA warp as soon as its last chunk is in
+//               registers.  The distance tile never reaches HBM.
 // A work unit is (query tile of 128 rows, split s of the reference tiles);
 // units are dealt round-robin over the persistent CTAs in split-major order,
 // so the CTAs of a wave stream the same reference range (it stays in L2) and
@@ -28,9 +32,8 @@
 // Candidate lists are kept per (split, column half, row).
 //
 // Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
-// B = bf16(x - c)); the certified error bound of v = fl32(acc + ||x - c||^2) is
-// derived in prep.cu with g = (dp + 16) 2^-20 for the tensor-core fp32
-// accumulation.
+// B = bf16(x - c)); the certified error bound of v is derived in prep.cu with
+// g = (dp + 32) 2^-20 for the tensor-core fp32 accumulation.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -44,30 +47,49 @@ namespace {
 struct TcParams {
   int m, KB, n_tiles, S, tiles_per_split, m_tiles, exclude_self, stages;
   long long q_offset;
-  const float* nx;   // [n_pad_tc], NaN on padding rows
   const float* E;    // [m_pad]
   const int* perm;   // tile row -> original query row (or null)
   SinkArgs sink;
   int* status;
 };
 
-constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;  // 16 KB per 64-column block
-constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;  // 32 KB per 64-column block
+constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;     // 16 KB per 64-column block
+constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;     // 32 KB per 64-column block
+constexpr uint32_t kAAugBytes = kTcBM * kTcAug * 2;     // 4 KB (query ones)
+constexpr uint32_t kBAugBytes = kTcBN * kTcAug * 2;     // 8 KB (reference norms)
 constexpr int kSpillStride = 9;  // 8 spilled values per thread, conflict-free stride
+
+__host__ __device__ inline uint32_t tc_stage_bytes(bool a_stream) {
+  return (a_stream ? kATileBytes : 0) + kBTileBytes + kBAugBytes;
+}
 
 __host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream, int ew) {
   size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
-  size_t stage = a_stream ? kATileBytes + kBTileBytes : kBTileBytes;
   size_t spill = (size_t)ew * 32 * kSpillStride * sizeof(float);
-  size_t nx = 8 * kTcBN * sizeof(float);  // per-warp double buffers (EW x 2 x 256/halves)
-  size_t bars = (2 * (size_t)stages + 6) * sizeof(uint64_t) + 16;
-  return 1024 /*alignment slack*/ + a + stage * stages + spill + nx + bars;
+  size_t bars = (2 * (size_t)stages + 7) * sizeof(uint64_t) + 16;
+  return 1024 /*alignment slack*/ + kAAugBytes + a + (size_t)tc_stage_bytes(a_stream) * stages +
+         spill + bars;
+}
+
+// Shared-memory descriptor of a K-major operand in the 32-byte swizzled layout
+// (rows of 32 B = 16 bf16, 8-row / 256 B atoms), as TMA writes it.
+B2K_DEV uint64_t smem_desc_sw32(const void* smem_tile) {
+  uint64_t addr = smem_u32(smem_tile);
+  uint64_t desc = 0;
+  desc |= (addr & 0x3FFFFull) >> 4;     // start address
+  desc |= (uint64_t)1 << 16;            // leading byte offset (unused, K fits the atom)
+  desc |= (uint64_t)(256 >> 4) << 32;   // stride byte offset: 8 rows x 32 B
+  desc |= (uint64_t)1 << 46;            // descriptor version (tcgen05)
+  desc |= (uint64_t)6 << 61;            // layout: 32-byte swizzle
+  return desc;
 }
 
 template <class Sink, bool A_STREAM, int EW>
 __global__ void __launch_bounds__(64 + 32 * EW, 1)
     screen_tc_kernel(const __grid_constant__ CUtensorMap tmA,
-                     const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+                     const __grid_constant__ CUtensorMap tmB,
+                     const __grid_constant__ CUtensorMap tmAaug,
+                     const __grid_constant__ CUtensorMap tmBaug, const TcParams p) {
   constexpr int kEpiThreads = 32 * EW;
   constexpr int kHalves = EW / 4;                 // column groups per tile
   constexpr int kChunks = kTcBN / 32 / kHalves;   // 32-column chunks per epilogue warp
@@ -76,19 +98,22 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int KB = p.KB;
   const int nst = p.stages;
-  uint8_t* a_smem = smem;
-  uint8_t* b_smem = smem + (A_STREAM ? 0 : KB * kATileBytes);
-  const uint32_t stage_bytes = A_STREAM ? kATileBytes + kBTileBytes : kBTileBytes;
+  uint8_t* aaug_smem = smem;                                   // 4 KB, 1024-aligned
+  uint8_t* a_smem = smem + kAAugBytes;                         // KB x 16 KB (1024-aligned)
+  uint8_t* b_smem = a_smem + (A_STREAM ? 0 : KB * kATileBytes);
+  const uint32_t stage_bytes = tc_stage_bytes(A_STREAM);
+  const uint32_t b_off = A_STREAM ? kATileBytes : 0;           // B tile inside a stage
+  const uint32_t baug_off = b_off + kBTileBytes;               // norm columns inside a stage
   float* spill_all = reinterpret_cast<float*>(b_smem + (size_t)nst * stage_bytes);
-  float* nx_all = spill_all + kEpiThreads * kSpillStride;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(nx_all + 8 * kTcBN);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(spill_all + kEpiThreads * kSpillStride);
   uint64_t* full = bars;
   uint64_t* empty = bars + nst;
   uint64_t* a_full = bars + 2 * nst;
   uint64_t* a_empty = a_full + 1;
   uint64_t* acc_full = a_empty + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2; // [2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  uint64_t* aaug_full = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(aaug_full + 1);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -105,6 +130,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     mbar_init(&acc_full[1], 1);
     mbar_init(&acc_empty[0], kEpiThreads);
     mbar_init(&acc_empty[1], kEpiThreads);
+    mbar_init(aaug_full, 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -123,6 +149,11 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     if (lane == 0) {
       prefetch_tmap(&tmA);
       prefetch_tmap(&tmB);
+      prefetch_tmap(&tmAaug);
+      prefetch_tmap(&tmBaug);
+      // the query-side norm columns are the same for every tile: load once
+      mbar_arrive_expect_tx(aaug_full, kAAugBytes);
+      tma_load_2d(aaug_smem, &tmAaug, aaug_full, 0, 0);
       uint32_t stage = 0, phase = 0, a_phase = 0;
       for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
         const int s = u / p.m_tiles, t = u % p.m_tiles;
@@ -139,14 +170,12 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
           for (int kb = 0; kb < KB; ++kb) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) goto prod_done;
             uint8_t* st = b_smem + (size_t)stage * stage_bytes;
-            if (A_STREAM) {
-              mbar_arrive_expect_tx(&full[stage], kATileBytes + kBTileBytes);
-              tma_load_2d(st, &tmA, &full[stage], kb * kTcBK, t * kTcBM);
-              tma_load_2d(st + kATileBytes, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
-            } else {
-              mbar_arrive_expect_tx(&full[stage], kBTileBytes);
-              tma_load_2d(st, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
-            }
+            const bool last = kb == KB - 1;
+            mbar_arrive_expect_tx(&full[stage], (A_STREAM ? kATileBytes : 0) + kBTileBytes +
+                                                    (last ? kBAugBytes : 0));
+            if (A_STREAM) tma_load_2d(st, &tmA, &full[stage], kb * kTcBK, t * kTcBM);
+            tma_load_2d(st + b_off, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
+            if (last) tma_load_2d(st + baug_off, &tmBaug, &full[stage], 0, j * kTcBN);
             if (++stage == (uint32_t)nst) {
               stage = 0;
               phase ^= 1;
@@ -163,6 +192,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
           phase ^= 1;
         }
       }
+      mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A);
     prod_done:;
     }
   } else if (warp == 1) {
@@ -170,45 +200,50 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
       uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0;
-      for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const int s = u / p.m_tiles;
-        const int j0 = s * p.tiles_per_split;
-        const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
-        if (!A_STREAM) {
-          if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto mma_done;
-          a_phase ^= 1;
-          tc_fence_after();
-        }
-        for (int j = j0; j < j1; ++j) {
-          const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
-          if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto mma_done;
-          tc_fence_after();
-          const uint32_t d_tmem = tmem_base + buf * kTcBN;
-          for (int kb = 0; kb < KB; ++kb) {
-            if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto mma_done;
+      if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto mma_done;
+      {
+        const uint64_t aaug_desc = smem_desc_sw32(aaug_smem);
+        for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
+          const int s = u / p.m_tiles;
+          const int j0 = s * p.tiles_per_split;
+          const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+          if (!A_STREAM) {
+            if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto mma_done;
+            a_phase ^= 1;
             tc_fence_after();
-            uint8_t* st = b_smem + (size_t)stage * stage_bytes;
-            const uint8_t* a_tile = A_STREAM ? st : a_smem + kb * kATileBytes;
-            const uint8_t* b_tile = A_STREAM ? st + kATileBytes : st;
-            const uint64_t adesc = smem_desc_sw128(a_tile);
-            const uint64_t bdesc = smem_desc_sw128(b_tile);
-#pragma unroll
-            for (int kk = 0; kk < kTcBK / 16; ++kk) {
-              // advance 16 bf16 = 32 bytes inside the swizzle atom: +2 in 16-byte units
-              mma_f16(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, idesc, (kb | kk) != 0);
-            }
-            mma_commit(&empty[stage]);
-            if (++stage == (uint32_t)nst) {
-              stage = 0;
-              phase ^= 1;
-            }
           }
-          mma_commit(&acc_full[buf]);
-          ++acc_it;
+          for (int j = j0; j < j1; ++j) {
+            const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
+            if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto mma_done;
+            tc_fence_after();
+            const uint32_t d_tmem = tmem_base + buf * kTcBN;
+            for (int kb = 0; kb < KB; ++kb) {
+              if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto mma_done;
+              tc_fence_after();
+              uint8_t* st = b_smem + (size_t)stage * stage_bytes;
+              const uint8_t* a_tile = A_STREAM ? st : a_smem + kb * kATileBytes;
+              const uint64_t adesc = smem_desc_sw128(a_tile);
+              const uint64_t bdesc = smem_desc_sw128(st + b_off);
+#pragma unroll
+              for (int kk = 0; kk < kTcBK / 16; ++kk) {
+                // advance 16 bf16 = 32 bytes inside the swizzle atom: +2 in 16-byte units
+                mma_f16(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, idesc, (kb | kk) != 0);
+              }
+              if (kb == KB - 1)  // + ||y_x||^2 through the norm columns
+                mma_f16(d_tmem, aaug_desc, smem_desc_sw32(st + baug_off), idesc, 1);
+              mma_commit(&empty[stage]);
+              if (++stage == (uint32_t)nst) {
+                stage = 0;
+                phase ^= 1;
+              }
+            }
+            mma_commit(&acc_full[buf]);
+            ++acc_it;
+          }
+          // Release the query tile for the next unit (not after the last one, so
+          // no arrival can land after the CTA has exited).
+          if (!A_STREAM && u + (int)gridDim.x < total_units) mma_commit(a_empty);
         }
-        // Release the query tile for the next unit (not after the last one, so
-        // no arrival can land after the CTA has exited).
-        if (!A_STREAM && u + (int)gridDim.x < total_units) mma_commit(a_empty);
       }
     mma_done:;
     }
@@ -220,10 +255,6 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     const int row_in_tile = g * 32 + lane;
     const int et = threadIdx.x - 64;        // 0 .. kEpiThreads-1
     float* spill = spill_all + et * kSpillStride;
-    // Warp-private double buffer of this warp's column norms (kWarpCols per
-    // tile): no barrier with the other epilogue warps is ever needed.
-    constexpr int kWarpCols = kChunks * 32;
-    float* nxw = nx_all + ew * 2 * kWarpCols;
     uint32_t acc_it = 0;
     for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
       const int s = u / p.m_tiles, t = u % p.m_tiles;
@@ -238,40 +269,17 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
         sink.init(p.sink, row, s * kHalves + half, p.E[row],
                   p.exclude_self ? (int)(p.q_offset + orig) : -1);
       }
-      // column norms of the unit's first tile
-      for (int i = lane; i < kWarpCols; i += 32)
-        nxw[i] = __ldg(p.nx + (size_t)j0 * kTcBN + c0 * 32 + i);
-      __syncwarp();
-      int nb = 0;
       for (int j = j0; j < j1; ++j) {
-        // prefetch the next tile's norms; they land in smem after this tile
-        float nn_next[kWarpCols / 32];
-#pragma unroll
-        for (int i = 0; i < kWarpCols / 32; ++i)
-          nn_next[i] = (j + 1 < j1) ? __ldg(p.nx + (size_t)(j + 1) * kTcBN + c0 * 32 + lane + 32 * i)
-                                    : 0.0f;
         // the other warps' k-th values for this query: consumed after the tile
         const uint32_t shared_key = valid ? sink.tile_fetch() : 0u;
-        const float* nxs = nxw + nb * kWarpCols;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
         if (!mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)) goto epi_done;
         tc_fence_after();
         const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN + c0 * 32;
         auto process = [&](const uint32_t(&r)[32], int c) {
-          const float4* np = reinterpret_cast<const float4*>(nxs + c * 32);
           float v[32];
 #pragma unroll
-          for (int q4 = 0; q4 < 8; ++q4) {
-            const float4 nn = np[q4];
-            float a0 = __uint_as_float(r[4 * q4]), a1 = __uint_as_float(r[4 * q4 + 1]);
-            float a2 = __uint_as_float(r[4 * q4 + 2]), a3 = __uint_as_float(r[4 * q4 + 3]);
-            add_f32x2(a0, a1, nn.x, nn.y);
-            add_f32x2(a2, a3, nn.z, nn.w);
-            v[4 * q4] = a0;
-            v[4 * q4 + 1] = a1;
-            v[4 * q4 + 2] = a2;
-            v[4 * q4 + 3] = a3;
-          }
+          for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
           if (valid) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
         };
         // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
@@ -296,10 +304,6 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
         }
         ++acc_it;
         if (valid) sink.tile_apply(shared_key);
-#pragma unroll
-        for (int i = 0; i < kWarpCols / 32; ++i) nxw[(nb ^ 1) * kWarpCols + lane + 32 * i] = nn_next[i];
-        __syncwarp();
-        nb ^= 1;
       }
       if (valid) {
         sink.tile_sync();
@@ -317,9 +321,15 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
   }
 }
 
+struct TcMaps {
+  const CUtensorMap* a;
+  const CUtensorMap* b;
+  const CUtensorMap* aaug;
+  const CUtensorMap* baug;
+};
+
 template <class Sink, bool A_STREAM, int EW>
-int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcParams& p, int grid,
-                      cudaStream_t st) {
+int launch_tc_variant(const TcMaps& maps, const TcParams& p, int grid, cudaStream_t st) {
   const size_t budget = 227 * 1024;
   int stages = 8;
   while (stages > 2 && tc_smem_bytes(p.KB, stages, A_STREAM, EW) > budget) --stages;
@@ -330,7 +340,7 @@ int launch_tc_variant(const CUtensorMap* ta, const CUtensorMap* tb, const TcPara
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
-  kern<<<grid, 64 + 32 * EW, smem, st>>>(*ta, *tb, q);
+  kern<<<grid, 64 + 32 * EW, smem, st>>>(*maps.a, *maps.b, *maps.aaug, *maps.baug, q);
   return (int)cudaGetLastError();
 }
 
@@ -352,7 +362,6 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   p.m_tiles = (int)(m_pad / kTcBM);
   p.exclude_self = exclude_self;
   p.q_offset = q_offset;
-  p.nx = ix->nxh;
   p.E = E;
   p.perm = perm;
   p.sink = sa;
@@ -361,10 +370,10 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   const int units = p.m_tiles * S;
   const int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
   if (grid <= 0) return 0;
-  const CUtensorMap* tb = &ix->tmap_b;
-#define B2K_TC_LAUNCH(SINK, EW)                                          \
-  (a_stream ? launch_tc_variant<SINK, true, EW>(tmap_a, tb, p, grid, st) \
-            : launch_tc_variant<SINK, false, EW>(tmap_a, tb, p, grid, st))
+  const TcMaps maps{tmap_a, &ix->tmap_b, &ix->tmap_aaug, &ix->tmap_baug};
+#define B2K_TC_LAUNCH(SINK, EW)                                  \
+  (a_stream ? launch_tc_variant<SINK, true, EW>(maps, p, grid, st) \
+            : launch_tc_variant<SINK, false, EW>(maps, p, grid, st))
   if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, 4);
   if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
   if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 8);
