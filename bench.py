@@ -470,6 +470,119 @@ def run_secondary(args):
     return 0
 
 
+def run_batch(args):
+    """256 uneven problems (seed 5) as one planned batch vs one call per problem."""
+    import torch
+
+    from datasets import cfg4
+    from mlxlearn_b200.batch import KnnBatch
+    from mlxlearn_b200.index import build_index
+
+    import oracle
+
+    torch.cuda.set_device(0)
+    threads = os.cpu_count() or 1
+    problems = cfg4()
+    total_q = sum(Q.shape[0] for _, Q, _ in problems)
+    flops = sum(2.0 * X.shape[0] * Q.shape[0] * X.shape[1] for X, Q, _ in problems)
+    t0 = time.perf_counter()
+    indexes = [build_index(X) for X, _, _ in problems]
+    for ix in indexes:
+        ix._ensure_device()
+    fit_s = time.perf_counter() - t0
+    Qd = [torch.from_numpy(Q).cuda() for _, Q, _ in problems]
+    items = [(ix, q, k) for ix, q, (_, _, k) in zip(indexes, Qd, problems)]
+    t0 = time.perf_counter()
+    batch = KnnBatch(items, autotune=True)
+    plan_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        batch.run()
+    batch.finish()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            batch.run()
+        ev1.record(stream)
+        stats = batch.finish()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # one call per problem through the single-problem device API
+    for ix, q, (_, _, k) in zip(indexes, Qd, problems):
+        ix.query_device(q, k)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for ix, q, (_, _, k) in zip(indexes, Qd, problems):
+        ix.query_device(q, k)
+    torch.cuda.synchronize()
+    one_s = time.perf_counter() - t0
+    # e2e: pinned host queries in, results out, through the batch object
+    Qh = [torch.from_numpy(Q).pin_memory() for _, Q, _ in problems]
+    Dh = [torch.empty(d.shape, dtype=d.dtype).pin_memory() for d in batch.dist]
+    Ih = [torch.empty(i.shape, dtype=i.dtype).pin_memory() for i in batch.idx]
+
+    def e2e_step():
+        for dst, src in zip(batch.queries, Qh):
+            dst.copy_(src, non_blocking=True)
+        batch.run()
+        batch.finish()
+        for dst, src in zip(Dh, batch.dist):
+            dst.copy_(src, non_blocking=True)
+        for dst, src in zip(Ih, batch.idx):
+            dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_s = _timed_wall(e2e_step, args.steps, 1)[0]
+    h2d = sum(q.numel() * 4 for q in Qh)
+    d2h = sum(d.numel() * 8 for d in Dh) + sum(i.numel() * 8 for i in Ih)
+    # parity + CPU baseline: the reference's exact scan on a few queries of every problem
+    ref = oracle.ref_native()
+    per = int(os.environ.get("B2K_BATCH_CPU_QUERIES", "4"))
+    est_cpu_s, sample_q, exact = 0.0, 0, True
+    for (X, Q, k), d, i in zip(problems, batch.dist, batch.idx):
+        s = min(per, Q.shape[0])
+        rd = np.empty((s, k)); ri = np.empty((s, k), np.int64)
+        t1 = time.perf_counter()
+        _ref_knn_threads(ref, X, Q[:s], k, rd, ri, min(threads, s))
+        est_cpu_s += (time.perf_counter() - t1) * Q.shape[0] / s
+        sample_q += s
+        exact &= bool(np.array_equal(ri, i[:s].cpu().numpy()))
+        exact &= bool(np.array_equal(rd, d[:s].cpu().numpy()))
+    tf_burst, tf_sust, hbm, peak_kind = peaks()
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "batched uneven kNN: aggregate queries/s, 256 problems (one graph) vs one "
+                  "call per problem",
+        "value": total_q / (ms / 1000), "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic: cfg4 recipe (seed 5)",
+        "workload_kind": "secondary",
+        "config": {"workload": "knn_batch_256_uneven_seed5", "problems": len(problems),
+                   "queries": total_q, "flops": flops,
+                   "l2": "operands 1.9 GB bf16, larger than L2"},
+        "one_call_per_problem": {"value": total_q / one_s, "unit": "queries/s",
+                                 "ms_per_step": 1000 * one_s,
+                                 "batch_speedup": one_s / (ms / 1000)},
+        "roofline": {"kernel": "whole batched run (prep, screens, certify, exact)",
+                     "bound": "tensor", "achieved": achieved, "peak": tf_burst,
+                     "unit": "TFLOP/s", "frac": achieved / tf_burst,
+                     "peak_source": f"{peak_kind} burst bf16", "traffic": None},
+        "batch_stats": stats, "fit_s": fit_s, "plan_s": plan_s,
+        "e2e": {"value": total_q / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "cpu_baseline": {"value": total_q / est_cpu_s, "unit": "queries/s", "cores": threads,
+                         "kind": "reference" if ref else "port",
+                         "sample": f"first {per} queries of every problem, time scaled by "
+                                   "each problem's query count"},
+        "parity_vs_cpu_reference": {"queries": sample_q, "bit_exact": exact},
+        "clocks": clk.summary(),
+    }
+    batch.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def _ref_knn_threads(ref, X, Q, k, dist, idx, threads):
     """The reference's exact native kNN scan over query blocks in threads."""
     from concurrent.futures import ThreadPoolExecutor
@@ -499,7 +612,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="knn", choices=["knn", "pixels", "radius", "small"])
+    ap.add_argument("--workload", default="knn",
+                    choices=["knn", "pixels", "radius", "small", "batch"])
     ap.add_argument("--profile", action="store_true",
                     help="profiling driver: only the bf16 device-resident steps of the "
                          "headline workload (no fp32 leg, e2e or CPU baseline)")
@@ -510,6 +624,8 @@ def main():
         return run_reference_arm(args)
     if args.profile:
         return run_profile(args)
+    if args.workload == "batch":
+        return run_batch(args)
     if args.workload != "knn":
         return run_secondary(args)
     return run_ours(args)

@@ -162,6 +162,61 @@ B2K_API int b2k_class_votes(const int64_t *d_idx, const double *d_dist, int64_t 
                             const int32_t *d_codes, int32_t n_classes, int32_t weighted,
                             double *d_votes, int64_t *d_pred, void *stream);
 
+/* ---------------------------------------------------------------- batches */
+
+/* One independent kNN problem of a batch: a fitted index and a device query
+ * block answered into device outputs (same meaning as b2k_knn_device). */
+typedef struct b2k_problem {
+  b2k_index *index;
+  const float *queries; /* device float32[m, d] of the index's d          */
+  int64_t m;
+  int32_t k;
+  int32_t exclude_self;
+  int64_t q_offset;
+  double *dist;         /* device float64[m, k] or NULL                   */
+  int64_t *idx;         /* device int64[m, k]                             */
+} b2k_problem;
+
+typedef struct b2k_batch b2k_batch;
+
+typedef struct b2k_batch_stats {
+  int32_t problems;        /* problems in the batch                           */
+  int32_t graph_problems;  /* problems inside the captured graph              */
+  int32_t screen_launches; /* persistent screen launches per run              */
+  int32_t work_items;      /* (problem, query tile, reference range) units    */
+  int64_t candidates;      /* re-ranked candidates (last finished run)        */
+  int64_t fallback_rows;   /* rows answered by the exhaustive scan            */
+  int64_t exact_compares;  /* exact comparator calls                          */
+  float tune_ms;           /* time spent autotuning at create                 */
+  float run_ms;            /* device time of the last finished run's graph    */
+} b2k_batch_stats;
+
+#define B2K_BATCH_AUTOTUNE 1 /* time the tuning candidates at create (cached per process) */
+
+/* Plan a batch of independent problems (uneven n, d, k, m) and capture it as
+ * one CUDA graph: a batched query preparation, one persistent tcgen05 screen
+ * launch per (heap width, epilogue width) over a device work queue of
+ * (problem, query tile, reference range) items balanced across the SMs, one
+ * batched certify launch and one batched exhaustive-scan launch for the rows
+ * that need it.  Problems the bf16 screen cannot certify (d < 16, k > 64,
+ * coordinates outside its range) are answered by b2k_knn_device inside
+ * b2k_batch_finish.  All indices must live on one device; queries and
+ * outputs are read and written in place on every run, so refilling the
+ * query buffers and running again answers the new queries.  No counterpart
+ * in the reference (mlxlearn answers one problem per call); results are
+ * identical to calling b2k_knn_device per problem. */
+B2K_API int b2k_batch_create(const b2k_problem *problems, int32_t count, int32_t flags,
+                             void *stream, b2k_batch **out);
+/* Launch one run of the batch's graph on `stream` (asynchronous). */
+B2K_API int b2k_batch_run(b2k_batch *batch, void *stream);
+/* Wait for the last run on `stream`, check the device status, answer the
+ * problems outside the graph (and any whose queries left the screen's range)
+ * and fill `stats` (may be NULL). */
+B2K_API int b2k_batch_finish(b2k_batch *batch, void *stream, b2k_batch_stats *stats);
+B2K_API int b2k_batch_destroy(b2k_batch *batch);
+/* create + run + finish + destroy. */
+B2K_API int b2k_batch_submit(const b2k_problem *problems, int32_t count, void *stream);
+
 /* ----------------------------------------------------------------- radius */
 
 typedef struct b2k_radius_result b2k_radius_result;

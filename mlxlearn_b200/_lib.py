@@ -48,6 +48,40 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Problem(ctypes.Structure):
+    """b2k_problem: one kNN problem of a batch (device pointers)."""
+
+    _fields_ = [
+        ("index", ctypes.c_void_p),
+        ("queries", ctypes.c_void_p),
+        ("m", ctypes.c_int64),
+        ("k", ctypes.c_int32),
+        ("exclude_self", ctypes.c_int32),
+        ("q_offset", ctypes.c_int64),
+        ("dist", ctypes.c_void_p),
+        ("idx", ctypes.c_void_p),
+    ]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("problems", ctypes.c_int32),
+        ("graph_problems", ctypes.c_int32),
+        ("screen_launches", ctypes.c_int32),
+        ("work_items", ctypes.c_int32),
+        ("candidates", ctypes.c_int64),
+        ("fallback_rows", ctypes.c_int64),
+        ("exact_compares", ctypes.c_int64),
+        ("tune_ms", ctypes.c_float),
+        ("run_ms", ctypes.c_float),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+BATCH_AUTOTUNE = 1
+
 # Every exported symbol of the C ABI, with (restype, argtypes).
 _vp, _i32, _i64, _dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 SIGNATURES = {
@@ -73,6 +107,12 @@ SIGNATURES = {
     "b2k_radius_result_nnz": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
     "b2k_radius_result_fetch": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "b2k_radius_result_release": (ctypes.c_int, [_vp]),
+    "b2k_batch_create": (ctypes.c_int, [ctypes.POINTER(Problem), _i32, _i32, _vp,
+                                        ctypes.POINTER(_vp)]),
+    "b2k_batch_run": (ctypes.c_int, [_vp, _vp]),
+    "b2k_batch_finish": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(BatchStats)]),
+    "b2k_batch_destroy": (ctypes.c_int, [_vp]),
+    "b2k_batch_submit": (ctypes.c_int, [ctypes.POINTER(Problem), _i32, _vp]),
 }
 
 _lib = None

@@ -186,8 +186,7 @@ static int ensure_bf16(Index& ix) {
   ix.dp = (int32_t)round_up(ix.d, kTcBK);
   ix.n_pad_tc = round_up(ix.n, kTcBN);
   B2K_CUDA(cudaMalloc(&ix.Xh, (size_t)ix.n_pad_tc * ix.dp * sizeof(uint16_t)));
-  B2K_CUDA(cudaMalloc(&ix.nxh, (size_t)ix.n_pad_tc * sizeof(float)));
-  launch_prep_index_bf16(&ix, st);
+  launch_prep_index_bf16(&ix, ix.Xh, st);
   B2K_CUDA(cudaGetLastError());
   float stats[8];
   B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
@@ -199,7 +198,7 @@ static int ensure_bf16(Index& ix) {
   // norm columns of the reference rows and the matching query-side ones
   B2K_CUDA(cudaMalloc(&ix.Xaug, (size_t)ix.n_pad_tc * kTcAug * sizeof(uint16_t)));
   B2K_CUDA(cudaMalloc(&ix.aug_ones, (size_t)kTcBM * kTcAug * sizeof(uint16_t)));
-  launch_prep_aug(&ix, st);
+  launch_prep_aug(&ix, ix.Xaug, ix.aug_ones, st);
   B2K_CUDA(cudaGetLastError());
   B2K_CUDA(cudaStreamSynchronize(st));
   if (!tensor_map_2d_bf16(&ix.tmap_baug, ix.Xaug, kTcAug, (uint64_t)ix.n_pad_tc, kTcAug, kTcBN,
@@ -476,6 +475,25 @@ int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
   return validate_knn(ix, m, k, exclude_self, q_offset, B2K_MODE_AUTO);
 }
 Index* index_of(b2k_index* h) { return h ? &h->ix : nullptr; }
+int knn_device_run(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
+                   int64_t q_offset, int mode, double* d_dist, int64_t* d_idx, cudaStream_t st) {
+  return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, mode, d_dist, d_idx, st, nullptr);
+}
+int injected_fault() { return fault_mode(); }
+int index_prepare_bf16_stats(Index& ix, uint16_t* Xh, uint16_t* Xaug, uint16_t* ones,
+                             cudaStream_t st, float* xh_max, float* ex_max) {
+  std::lock_guard<std::mutex> lock(ix.mu);
+  launch_prep_index_bf16(&ix, Xh, st);
+  B2K_CUDA(cudaGetLastError());
+  launch_prep_aug(&ix, Xaug, ones, st);
+  B2K_CUDA(cudaGetLastError());
+  float stats[8];
+  B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  *xh_max = stats[3];
+  *ex_max = stats[4];
+  return B2K_OK;
+}
 
 static bool host_finite(const float* v, size_t count) {
   for (size_t i = 0; i < count; ++i) {
@@ -595,7 +613,6 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.nx64);
   cudaFree(ix.stats_dev);
   cudaFree(ix.Xh);
-  cudaFree(ix.nxh);
   cudaFree(ix.pivots);
   cudaFree(ix.pivot_norms);
   cudaFree(ix.Xaug);

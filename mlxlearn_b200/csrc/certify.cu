@@ -251,12 +251,9 @@ __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
   }
 }
 
-__global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyArgs a) {
-  extern __shared__ uint8_t smem[];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * kCertWarps + w;
-  if (row >= a.m) return;
-  uint8_t* wbase = smem + (size_t)w * kCertWarpBytes;
+// One query row of one problem, by one warp; `wbase` is the warp's shared
+// memory (kCertWarpBytes).
+__device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, uint8_t* wbase, int lane) {
   int* ci = reinterpret_cast<int*>(wbase);                          // [kCertifyCap]
   float* cv = reinterpret_cast<float*>(ci + kCertifyCap);           // [kCertifyCap]
   double* cs = reinterpret_cast<double*>(cv + kCertifyCap);         // [kSurvivorCap]
@@ -275,7 +272,7 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
   }
   overflow = __any_sync(0xffffffffu, overflow);
   if (overflow) {
-    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)(a.row_base + row);
     return;
   }
   entries = __reduce_add_sync(0xffffffffu, entries);
@@ -329,7 +326,7 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
     }
   }
   if (too_many || C < k) {
-    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)(a.row_base + row);
     return;
   }
   __syncwarp();
@@ -355,7 +352,7 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
     Cs += __popc(bal);
   }
   if (Cs > kSurvivorCap) {
-    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)row;
+    if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)(a.row_base + row);
     return;
   }
   __syncwarp();
@@ -375,6 +372,27 @@ __global__ void __launch_bounds__(kCertWarps * 32) certify_kernel(const CertifyA
   }
 }
 
+__global__ void __launch_bounds__(kCertWarps * 32, 2)
+    certify_kernel(const __grid_constant__ CertifyArgs a) {
+  extern __shared__ uint8_t smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kCertWarps + w;
+  if (row >= a.m) return;
+  certify_row(a, row, smem + (size_t)w * kCertWarpBytes, lane);
+}
+
+// Batched form: problem p owns global rows [row_start[p], row_start[p + 1]).
+__global__ void __launch_bounds__(kCertWarps * 32, 2)
+    certify_batch_kernel(const CertifyArgs* __restrict__ tab, const int64_t* __restrict__ row_start,
+                         int P, int64_t total) {
+  extern __shared__ uint8_t smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = (int64_t)blockIdx.x * kCertWarps + w;
+  if (r >= total) return;
+  const int p = problem_of(row_start, P, r);
+  certify_row(tab[p], r - row_start[p], smem + (size_t)w * kCertWarpBytes, lane);
+}
+
 // ---------------------------------------------------------------------------
 // Exhaustive exact scan: one CTA per query.  Canonical float64 values of all
 // rows, an exact radix select of the k-th smallest value, every row whose
@@ -390,88 +408,130 @@ __device__ __forceinline__ double exact_value(const ExactArgs& a, const float* q
   return canonical_d2(q, a.X + (size_t)j * a.d, a.d);
 }
 
-__global__ void __launch_bounds__(kExactThreads) exact_kernel(const ExactArgs a) {
-  extern __shared__ uint8_t smem[];
-  double* cs = reinterpret_cast<double*>(smem);            // [kExactCap]
-  int* ci = reinterpret_cast<int*>(cs + kExactCap);         // [kExactCap]
-  __shared__ unsigned hist[256];
-  __shared__ unsigned long long s_prefix;
-  __shared__ int s_rank, s_count;
+struct ExactShared {
+  double* cs;  // [kExactCap]
+  int* ci;     // [kExactCap]
+  unsigned* hist;
+  unsigned long long* prefix;
+  int* rank;
+  int* count;
+};
+
+// One query row of one problem, by the whole CTA.  `sc` is the CTA's scratch
+// of a.n canonical values (or null: recompute per pass).
+__device__ __forceinline__ void exact_row(const ExactArgs& a, int64_t row, double* sc, const ExactShared& sh) {
   const int tid = threadIdx.x;
-  const int count = a.rows ? *a.row_count : (int)a.m;
-  double* sc = a.scratch ? a.scratch + (size_t)blockIdx.x * a.n : nullptr;
-  for (int it = blockIdx.x; it < count; it += gridDim.x) {
-    const int64_t row = a.rows ? a.rows[it] : it;
-    const int64_t orow = a.perm ? a.perm[row] : row;
-    const float* q = a.Q + (size_t)row * a.d;
-    if (sc) {
-      for (int64_t j = tid; j < a.n; j += kExactThreads) {
-        sc[j] = (a.exclude_self && j == a.q_offset + orow)
-                    ? INFINITY
-                    : canonical_d2(q, a.X + (size_t)j * a.d, a.d);
-      }
-      __syncthreads();
-    }
-    // radix select over the bit patterns of non-negative doubles (monotone)
-    unsigned long long prefix = 0, mask = 0;
-    if (tid == 0) s_rank = a.k;
-    __syncthreads();
-    for (int shift = 56; shift >= 0; shift -= 8) {
-      hist[tid] = 0;
-      __syncthreads();
-      for (int64_t j = tid; j < a.n; j += kExactThreads) {
-        const unsigned long long b = __double_as_longlong(exact_value(a, q, orow, j, sc));
-        if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
-      }
-      __syncthreads();
-      if (tid == 0) {
-        int r = s_rank;
-        unsigned acc = 0;
-        int dgt = 0;
-        for (; dgt < 256; ++dgt) {
-          if (acc + hist[dgt] >= (unsigned)r) break;
-          acc += hist[dgt];
-        }
-        s_rank = r - (int)acc;
-        s_prefix = prefix | ((unsigned long long)dgt << shift);
-      }
-      __syncthreads();
-      prefix = s_prefix;
-      mask |= 255ull << shift;
-    }
-    const double Vk = __longlong_as_double((long long)prefix);
-    const double g2 = interval_g2(a.d);
-    const double reach = __dmul_ru(Vk, 1.0 + g2);
-    if (tid == 0) s_count = 0;
-    __syncthreads();
+  double* cs = sh.cs;
+  int* ci = sh.ci;
+  unsigned* hist = sh.hist;
+  const int64_t orow = a.perm ? a.perm[row] : row;
+  const float* q = a.Q + (size_t)row * a.d;
+  if (sc) {
     for (int64_t j = tid; j < a.n; j += kExactThreads) {
-      const double v = exact_value(a, q, orow, j, sc);
-      if (v != INFINITY && __dmul_rd(v, 1.0 - g2) <= reach) {
-        const int pos = atomicAdd(&s_count, 1);
-        if (pos < kExactCap) {
-          cs[pos] = v;
-          ci[pos] = (int)j;
-        }
-      }
-    }
-    __syncthreads();
-    const int C = s_count;
-    if (C > kExactCap) {
-      if (tid == 0) atomicCAS(a.status, DEV_OK, DEV_TOO_MANY_TIES);
-    } else if (tid < 32) {
-      const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
-      for (int t = tid; t < a.k; t += 32) {
-        a.idx[orow * a.k + t] = ci[t];
-        if (a.dist) a.dist[orow * a.k + t] = sqrt(cs[t]);
-      }
-      if (tid == 0) {
-        atomicAdd(&a.counters[3], 1ull);
-        if (cmp) atomicAdd(&a.counters[2], (unsigned long long)cmp);
-      }
+      sc[j] = (a.exclude_self && j == a.q_offset + orow)
+                  ? INFINITY
+                  : canonical_d2(q, a.X + (size_t)j * a.d, a.d);
     }
     __syncthreads();
   }
+  // radix select over the bit patterns of non-negative doubles (monotone)
+  unsigned long long prefix = 0, mask = 0;
+  if (tid == 0) *sh.rank = a.k;
+  __syncthreads();
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    hist[tid] = 0;
+    __syncthreads();
+    for (int64_t j = tid; j < a.n; j += kExactThreads) {
+      const unsigned long long b = __double_as_longlong(exact_value(a, q, orow, j, sc));
+      if ((b & mask) == prefix) atomicAdd(&hist[(b >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int r = *sh.rank;
+      unsigned acc = 0;
+      int dgt = 0;
+      for (; dgt < 256; ++dgt) {
+        if (acc + hist[dgt] >= (unsigned)r) break;
+        acc += hist[dgt];
+      }
+      *sh.rank = r - (int)acc;
+      *sh.prefix = prefix | ((unsigned long long)dgt << shift);
+    }
+    __syncthreads();
+    prefix = *sh.prefix;
+    mask |= 255ull << shift;
+  }
+  const double Vk = __longlong_as_double((long long)prefix);
+  const double g2 = interval_g2(a.d);
+  const double reach = __dmul_ru(Vk, 1.0 + g2);
+  if (tid == 0) *sh.count = 0;
+  __syncthreads();
+  for (int64_t j = tid; j < a.n; j += kExactThreads) {
+    const double v = exact_value(a, q, orow, j, sc);
+    if (v != INFINITY && __dmul_rd(v, 1.0 - g2) <= reach) {
+      const int pos = atomicAdd(sh.count, 1);
+      if (pos < kExactCap) {
+        cs[pos] = v;
+        ci[pos] = (int)j;
+      }
+    }
+  }
+  __syncthreads();
+  const int C = *sh.count;
+  if (C > kExactCap) {
+    if (tid == 0) atomicCAS(a.status, DEV_OK, DEV_TOO_MANY_TIES);
+  } else if (tid < 32) {
+    const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
+    for (int t = tid; t < a.k; t += 32) {
+      a.idx[orow * a.k + t] = ci[t];
+      if (a.dist) a.dist[orow * a.k + t] = sqrt(cs[t]);
+    }
+    if (tid == 0) {
+      atomicAdd(&a.counters[3], 1ull);
+      if (cmp) atomicAdd(&a.counters[2], (unsigned long long)cmp);
+    }
+  }
+  __syncthreads();
 }
+
+#define B2K_EXACT_SHARED                                                   \
+  extern __shared__ uint8_t smem[];                                        \
+  __shared__ unsigned hist[256];                                           \
+  __shared__ unsigned long long s_prefix;                                  \
+  __shared__ int s_rank, s_count;                                          \
+  ExactShared sh;                                                          \
+  sh.cs = reinterpret_cast<double*>(smem);                                 \
+  sh.ci = reinterpret_cast<int*>(sh.cs + kExactCap);                       \
+  sh.hist = hist;                                                          \
+  sh.prefix = &s_prefix;                                                   \
+  sh.rank = &s_rank;                                                       \
+  sh.count = &s_count;
+
+__global__ void __launch_bounds__(kExactThreads)
+    exact_kernel(const __grid_constant__ ExactArgs a) {
+  B2K_EXACT_SHARED
+  const int count = a.rows ? *a.row_count : (int)a.m;
+  double* sc = a.scratch ? a.scratch + (size_t)blockIdx.x * a.n : nullptr;
+  for (int it = blockIdx.x; it < count; it += gridDim.x)
+    exact_row(a, a.rows ? a.rows[it] : it, sc, sh);
+}
+
+// Batched form over a list of global rows (problem p owns rows
+// [row_start[p], row_start[p + 1])); scratch holds n_max values per CTA.
+__global__ void __launch_bounds__(kExactThreads)
+    exact_batch_kernel(const ExactArgs* __restrict__ tab, const int64_t* __restrict__ row_start,
+                       int P, const int* __restrict__ rows, const int* __restrict__ row_count,
+                       double* scratch, int64_t n_max) {
+  B2K_EXACT_SHARED
+  const int count = *row_count;
+  double* sc = scratch ? scratch + (size_t)blockIdx.x * n_max : nullptr;
+  for (int it = blockIdx.x; it < count; it += gridDim.x) {
+    const int64_t r = rows[it];
+    const int p = problem_of(row_start, P, r);
+    exact_row(tab[p], r - row_start[p], sc, sh);
+  }
+}
+#undef B2K_EXACT_SHARED
 
 }  // namespace
 
@@ -481,6 +541,27 @@ void launch_certify(const CertifyArgs& a, cudaStream_t st) {
   cudaFuncSetAttribute(certify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const unsigned grid = (unsigned)((a.m + kCertWarps - 1) / kCertWarps);
   certify_kernel<<<grid, kCertWarps * 32, smem, st>>>(a);
+}
+
+void launch_certify_batch(const CertifyArgs* tab, const int64_t* row_start, int P,
+                          int64_t total_rows, cudaStream_t st) {
+  if (total_rows <= 0) return;
+  const size_t smem = (size_t)kCertWarps * kCertWarpBytes;
+  cudaFuncSetAttribute(certify_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const unsigned grid = (unsigned)((total_rows + kCertWarps - 1) / kCertWarps);
+  certify_batch_kernel<<<grid, kCertWarps * 32, smem, st>>>(tab, row_start, P, total_rows);
+}
+
+void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, const int* rows,
+                        const int* row_count, double* scratch, int64_t n_max, int grid,
+                        cudaStream_t st) {
+  if (grid <= 0) return;
+  const size_t smem = (size_t)kExactCap * (sizeof(double) + sizeof(int));
+  cudaFuncSetAttribute(exact_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  exact_batch_kernel<<<grid, kExactThreads, smem, st>>>(tab, row_start, P, rows, row_count,
+                                                        scratch, n_max);
 }
 
 void launch_exact(const ExactArgs& a, cudaStream_t st) {

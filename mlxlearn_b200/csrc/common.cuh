@@ -180,6 +180,20 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_bf16) {
 }
 
 // --------------------------------------------------------------- arithmetic
+// Batched kernels: the problem owning global row r, i.e. the largest p with
+// row_start[p] <= r (row_start ascending; problems with no rows are skipped).
+B2K_DEV int problem_of(const int64_t* __restrict__ row_start, int P, int64_t r) {
+  int lo = 0, hi = P - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (row_start[mid] <= r)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 B2K_DEV float min3f(float a, float b, float c) {
   float r;
   asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));

@@ -52,7 +52,6 @@ struct Index {
   int64_t n_pad_tc = 0;          // multiple of kTcBN
   int32_t dp = 0;                // d padded to a multiple of kTcBK
   uint16_t* Xh = nullptr;        // [n_pad_tc, dp]
-  float* nxh = nullptr;          // [n_pad_tc] fl32(||x||^2), NaN on padding rows
   float xh_max = 0, ex_max = 0;  // max ||bf16 operand||, max ||(x - center) - bf16 operand||
   CUtensorMap tmap_b;            // TMA map over Xh, box 64 x 256
   uint16_t* Xaug = nullptr;      // [n_pad_tc, 16] bf16 [n_hi, n_mid, n_lo, 0...] of ||x - c||^2
@@ -69,8 +68,12 @@ struct Index {
 
 // ------------------------------------------------------------ prep kernels
 void launch_prep_index(Index* ix, cudaStream_t st);
-void launch_prep_index_bf16(Index* ix, cudaStream_t st);
-void launch_prep_aug(Index* ix, cudaStream_t st);  // Xaug (norm split) and aug_ones
+// bf16 operand rows [n_pad, dp] (n_pad = n rounded up to 256) into Xh; the
+// operand statistics go to the index's stats_dev [3], [4].
+void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st);
+// norm columns [n_pad, 16] into Xaug; when `ones` is set, also the query-side
+// columns [128, 16].
+void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st);
 // Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
 struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
@@ -80,6 +83,22 @@ struct QueryPrep {
 };
 void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
                          QueryPrep qp, cudaStream_t st);
+// One problem of a query preparation (the batched form takes a table of them).
+struct PrepProblem {
+  const float* Q;
+  int64_t m, m_pad;
+  int d, dp, mode;
+  const float* center;
+  float xh_max, nx_max, ex_max;  // operand statistics of the index for `mode`
+  float* E;
+  uint16_t* Ah;                  // [m_pad, dp] (bf16 mode)
+  double* nq;
+  int* flags;
+};
+PrepProblem prep_problem(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
+                         const QueryPrep& qp);
+void launch_prep_queries_batch(const PrepProblem* tab, const int64_t* row_start, int P,
+                               int64_t total_rows, cudaStream_t st);
 
 // ---------------------------------------------------------- screen kernels
 constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
@@ -114,8 +133,12 @@ struct CertifyArgs {
   int* fallback_count; // [1]
   unsigned long long* counters;  // [4]: candidates, entries, exact compares, -
   const int* perm;     // row -> output row (or null)
+  int64_t row_base;    // added to the row in fallback_list entries (batched runs)
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
+// problem p owns global rows [row_start[p], row_start[p + 1]) of the batch
+void launch_certify_batch(const CertifyArgs* tab, const int64_t* row_start, int P,
+                          int64_t total_rows, cudaStream_t st);
 
 struct ExactArgs {
   const float* X;
@@ -135,6 +158,10 @@ struct ExactArgs {
   const int* perm;      // row -> original query row for output and self (or null)
 };
 void launch_exact(const ExactArgs& a, cudaStream_t st);
+// rows: global row ids of the batch; scratch: [grid][n_max] or null
+void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, const int* rows,
+                        const int* row_count, double* scratch, int64_t n_max, int grid,
+                        cudaStream_t st);
 
 // ------------------------------------------------------------------ radius
 struct RadiusPlanArgs {
@@ -182,6 +209,14 @@ int report_error(int code, const char* msg);  // sets b2k_last_error(), returns 
 int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
                    int64_t q_offset);
 Index* index_of(b2k_index* h);
+// knn on device pointers (b2k_knn_device without the stats), synchronises st
+int knn_device_run(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
+                   int64_t q_offset, int mode, double* d_dist, int64_t* d_idx, cudaStream_t st);
+int injected_fault();  // B2K_FAULT: 0 none, 1 alloc, 2 launch, 3 timeout
+// bf16 operand rows and norm columns of an index into caller buffers, and the
+// operand statistics the query bound needs (synchronises st)
+int index_prepare_bf16_stats(Index& ix, uint16_t* Xh, uint16_t* Xaug, uint16_t* ones,
+                             cudaStream_t st, float* xh_max, float* ex_max);
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
                         uint32_t box_inner, uint32_t box_outer, int swizzle_bytes = 128);
 int num_sms(int device);

@@ -104,16 +104,15 @@ __global__ void prep_index_kernel(const float* __restrict__ X, int64_t n, int d,
 
 __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, int d,
                                        int64_t n_pad, int dp, const float* __restrict__ center,
-                                       const float* __restrict__ nx32,
-                                       __nv_bfloat16* __restrict__ Xh, float* __restrict__ nxh,
+                                       __nv_bfloat16* __restrict__ Xh,
                                        float* __restrict__ stats) {
   int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   int lane = threadIdx.x & 31;
   if (row >= n_pad) return;
   __nv_bfloat16* xh = Xh + row * dp;
   if (row >= n) {
+    // padding rows: zero operands (their NaN norm column keeps them out)
     for (int i = lane; i < dp; i += 32) xh[i] = __float2bfloat16_rn(0.0f);
-    if (lane == 0) nxh[row] = __int_as_float(0x7fc00000);  // NaN: never admitted
     return;
   }
   const float* x = X + row * d;
@@ -134,7 +133,6 @@ __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, i
   en = warp_sum(en);
   yy = warp_sum(yy);
   if (lane == 0) {
-    nxh[row] = nx32[row];
     atomic_max_pos(stats + 3, __double2float_ru(sqrt(hn) * (1.0 + 1e-15)));
     atomic_max_pos(stats + 4, __double2float_ru(sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy)));
   }
@@ -147,7 +145,7 @@ __global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int6
                                 __nv_bfloat16* __restrict__ Xaug,
                                 __nv_bfloat16* __restrict__ ones) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row < kTcBM) {
+  if (ones && row < kTcBM) {
     for (int c = 0; c < kTcAug; ++c)
       ones[row * kTcAug + c] = __float2bfloat16_rn(c < 3 ? 1.0f : 0.0f);
   }
@@ -171,29 +169,25 @@ __global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int6
   a[2] = __float2bfloat16_rn((float)r2);
 }
 
-__global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int64_t m_pad,
-                                    int d, int dp, int mode, const float* __restrict__ center,
-                                    float xh_max, float nx_max, float ex_max,
-                                    float* __restrict__ E, __nv_bfloat16* __restrict__ Ah,
-                                    double* __restrict__ nq_out, int* __restrict__ flags) {
-  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  int lane = threadIdx.x & 31;
-  if (row >= m_pad) return;
+// One query row: error bound E, the bf16 operand row (bf16 mode), ||y||^2.
+__device__ __forceinline__ void prep_query_row(const PrepProblem& P, int64_t row, int lane) {
   const double u = 0x1p-24;
-  const bool bf16 = mode == B2K_MODE_BF16;
-  if (row >= m) {
+  const bool bf16 = P.mode == B2K_MODE_BF16;
+  const int d = P.d, dp = P.dp;
+  __nv_bfloat16* Ah = reinterpret_cast<__nv_bfloat16*>(P.Ah);
+  if (row >= P.m) {
     if (bf16)
       for (int i = lane; i < dp; i += 32) Ah[row * dp + i] = __float2bfloat16_rn(0.0f);
-    if (lane == 0) E[row] = 0.0f;
+    if (lane == 0) P.E[row] = 0.0f;
     return;
   }
-  const float* q = Q + row * d;
+  const float* q = P.Q + row * d;
   double yy = 0.0, hn = 0.0, en = 0.0;
   bool ok = true;
   const int width = bf16 ? dp : d;
   for (int i = lane; i < width; i += 32) {
     const float v = i < d ? q[i] : 0.0f;
-    const float c = i < d ? center[i] : 0.0f;
+    const float c = i < d ? P.center[i] : 0.0f;
     ok &= coord_in_range(v);
     const double y = (double)v - (double)c;
     const float h32 = v - c;
@@ -217,17 +211,34 @@ __global__ void prep_queries_kernel(const float* __restrict__ Q, int64_t m, int6
   if (lane == 0) {
     const double qh = sqrt(hn) * (1.0 + 1e-15);
     const double eq = sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy);
-    const double XH = xh_max, EX = ex_max, NX = nx_max;
+    const double XH = P.xh_max, EX = P.ex_max, NX = P.nx_max;
     // tensor cores: dp feature columns + 16 norm columns accumulated in fp32;
     // the accumulation also carries ||y_x||^2 itself (the g * NX term)
     const double g = bf16 ? (double)(dp + kTcAug + 16) * 0x1p-20 : (double)(d + 4) * u * 1.01;
     double bound = 2.0 * (qh * EX + eq * XH + eq * EX) + 2.0 * g * qh * XH + 2.0 * u * NX +
                    2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy + (bf16 ? g * NX * 1.01 : 0.0);
     bound = bound * (1.0 + 0x1p-16) + (double)width * 0x1p-120;
-    E[row] = __double2float_ru(bound);
-    if (nq_out) nq_out[row] = yy;
-    if (!ok) atomicOr(flags, 1);
+    P.E[row] = __double2float_ru(bound);
+    if (P.nq) P.nq[row] = yy;
+    if (!ok) atomicOr(P.flags, 1);
   }
+}
+
+__global__ void prep_queries_kernel(const __grid_constant__ PrepProblem P) {
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (row >= P.m_pad) return;
+  prep_query_row(P, row, threadIdx.x & 31);
+}
+
+// Batched form: rows of all problems back to back, problem p owning padded
+// rows [row_start[p], row_start[p + 1]).
+__global__ void prep_queries_batch_kernel(const PrepProblem* __restrict__ tab,
+                                          const int64_t* __restrict__ row_start, int P,
+                                          int64_t total) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (r >= total) return;
+  const int p = problem_of(row_start, P, r);
+  prep_query_row(tab[p], r - row_start[p], threadIdx.x & 31);
 }
 
 }  // namespace
@@ -244,19 +255,43 @@ void launch_prep_index(Index* ix, cudaStream_t st) {
       ix->X, ix->n, ix->d, ix->center, ix->nx32, ix->nx64, ix->stats_dev);
 }
 
-void launch_prep_index_bf16(Index* ix, cudaStream_t st) {
+void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st) {
   const int warps = 8;
-  const int64_t blocks = (ix->n_pad_tc + warps - 1) / warps;
+  const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
+  const int dp = (ix->d + kTcBK - 1) / kTcBK * kTcBK;
+  const int64_t blocks = (n_pad + warps - 1) / warps;
   prep_index_bf16_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
-      ix->X, ix->n, ix->d, ix->n_pad_tc, ix->dp, ix->center, ix->nx32,
-      reinterpret_cast<__nv_bfloat16*>(ix->Xh), ix->nxh, ix->stats_dev);
+      ix->X, ix->n, ix->d, n_pad, dp, ix->center, reinterpret_cast<__nv_bfloat16*>(Xh),
+      ix->stats_dev);
 }
 
-void launch_prep_aug(Index* ix, cudaStream_t st) {
-  const int64_t rows = ix->n_pad_tc > kTcBM ? ix->n_pad_tc : kTcBM;
+void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st) {
+  const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
+  const int64_t rows = n_pad > kTcBM ? n_pad : kTcBM;
   prep_aug_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
-      ix->nx64, ix->n, ix->n_pad_tc, reinterpret_cast<__nv_bfloat16*>(ix->Xaug),
-      reinterpret_cast<__nv_bfloat16*>(ix->aug_ones));
+      ix->nx64, ix->n, n_pad, reinterpret_cast<__nv_bfloat16*>(Xaug),
+      reinterpret_cast<__nv_bfloat16*>(ones));
+}
+
+PrepProblem prep_problem(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
+                         const QueryPrep& qp) {
+  const bool bf16 = mode == B2K_MODE_BF16;
+  PrepProblem P{};
+  P.Q = Q;
+  P.m = m;
+  P.m_pad = m_pad;
+  P.d = ix->d;
+  P.dp = (ix->d + kTcBK - 1) / kTcBK * kTcBK;
+  P.mode = mode;
+  P.center = ix->center;
+  P.xh_max = bf16 ? ix->xh_max : ix->xn_max;
+  P.nx_max = ix->nx_max;
+  P.ex_max = bf16 ? ix->ex_max : ix->ex32_max;
+  P.E = qp.E;
+  P.Ah = qp.Ah;
+  P.nq = qp.nq;
+  P.flags = qp.flags;
+  return P;
 }
 
 void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
@@ -264,11 +299,17 @@ void launch_prep_queries(const Index* ix, const float* Q, int64_t m, int64_t m_p
   const int warps = 8;
   const int64_t blocks = (m_pad + warps - 1) / warps;
   if (blocks == 0) return;
-  const bool bf16 = mode == B2K_MODE_BF16;
   prep_queries_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
-      Q, m, m_pad, ix->d, ix->dp, mode, ix->center, bf16 ? ix->xh_max : ix->xn_max, ix->nx_max,
-      bf16 ? ix->ex_max : ix->ex32_max, qp.E, reinterpret_cast<__nv_bfloat16*>(qp.Ah), qp.nq,
-      qp.flags);
+      prep_problem(ix, Q, m, m_pad, mode, qp));
+}
+
+void launch_prep_queries_batch(const PrepProblem* tab, const int64_t* row_start, int P,
+                               int64_t total_rows, cudaStream_t st) {
+  const int warps = 8;
+  const int64_t blocks = (total_rows + warps - 1) / warps;
+  if (blocks == 0) return;
+  prep_queries_batch_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(tab, row_start, P,
+                                                                       total_rows);
 }
 
 }  // namespace b2k

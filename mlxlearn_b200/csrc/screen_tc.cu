@@ -39,18 +39,72 @@
 #include "common.cuh"
 #include "internal.cuh"
 #include "sinks.cuh"
+#include "tc_batch.cuh"
 
 namespace b2k {
 
 namespace {
 
 struct TcParams {
-  int m, KB, n_tiles, S, tiles_per_split, m_tiles, exclude_self, stages;
-  long long q_offset;
-  const float* E;    // [m_pad]
-  const int* perm;   // tile row -> original query row (or null)
-  SinkArgs sink;
+  int stages;
+  int a_blocks;              // 64-column query blocks the resident A region holds
+  int m_tiles, S;            // single problem: m_tiles * S units, dealt round-robin
+  const TcProblem* probs;    // batched: problem table
+  const int4* items;         // batched: (problem, query tile, first tile, end tile)
+  const int* cta_begin;      // batched: CTA b runs items [cta_begin[b], cta_begin[b + 1])
   int* status;
+  TcProblem one;             // single problem
+};
+
+// Tensor maps of a launch: per operand group, the query tiles (A), reference
+// tiles (B) and reference norm columns; the query-side ones columns are common.
+template <int G>
+struct TcMapSet {
+  CUtensorMap a[G], b[G], baug[G];
+  CUtensorMap aaug;
+};
+
+struct TcUnit {
+  const TcProblem* pr;
+  int t, j0, j1, slot;
+};
+
+// The sequence of work units of this CTA; every warp role walks it in step.
+template <bool BATCH>
+struct UnitCursor {
+  int u, end, step;
+  B2K_DEV UnitCursor(const TcParams& p) {
+    if (BATCH) {
+      u = p.cta_begin[blockIdx.x];
+      end = p.cta_begin[blockIdx.x + 1];
+      step = 1;
+    } else {
+      u = blockIdx.x;
+      end = p.m_tiles * p.S;
+      step = gridDim.x;
+    }
+  }
+  B2K_DEV bool next(const TcParams& p, TcUnit& x) {
+    if (u >= end) return false;
+    if (BATCH) {
+      const int4 it = p.items[u];
+      x.pr = p.probs + it.x;
+      x.t = it.y;
+      x.j0 = it.z;
+      x.j1 = it.w;
+      x.slot = it.z / x.pr->tiles_per_split;
+    } else {
+      const int s = u / p.m_tiles;
+      x.pr = &p.one;
+      x.t = u % p.m_tiles;
+      x.j0 = s * p.one.tiles_per_split;
+      x.j1 = min(x.j0 + p.one.tiles_per_split, p.one.n_tiles);
+      x.slot = s;
+    }
+    u += step;
+    return true;
+  }
+  B2K_DEV bool more() const { return u < end; }
 };
 
 constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;     // 16 KB per 64-column block
@@ -58,6 +112,9 @@ constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;     // 32 KB per 64-column b
 constexpr uint32_t kAAugBytes = kTcBM * kTcAug * 2;     // 4 KB (query ones)
 constexpr uint32_t kBAugBytes = kTcBN * kTcAug * 2;     // 8 KB (reference norms)
 constexpr int kSpillStride = 9;  // 8 spilled values per thread, conflict-free stride
+// A CTA allocates all 512 TMEM columns, so no two may share an SM: ask for at
+// least this much shared memory (more than half of the SM's 228 KB).
+constexpr size_t kMinCtaSmem = 116 * 1024;
 
 __host__ __device__ inline uint32_t tc_stage_bytes(bool a_stream) {
   return (a_stream ? kATileBytes : 0) + kBTileBytes + kBAugBytes;
@@ -84,23 +141,21 @@ B2K_DEV uint64_t smem_desc_sw32(const void* smem_tile) {
   return desc;
 }
 
-template <class Sink, bool A_STREAM, int EW>
+template <class Sink, bool A_STREAM, int EW, bool BATCH>
 __global__ void __launch_bounds__(64 + 32 * EW, 1)
-    screen_tc_kernel(const __grid_constant__ CUtensorMap tmA,
-                     const __grid_constant__ CUtensorMap tmB,
-                     const __grid_constant__ CUtensorMap tmAaug,
-                     const __grid_constant__ CUtensorMap tmBaug, const TcParams p) {
+    screen_tc_kernel(const __grid_constant__ TcMapSet<BATCH ? kBatchGroups : 1> maps,
+                     const __grid_constant__ TcParams p) {
+  constexpr int G = BATCH ? kBatchGroups : 1;
   constexpr int kEpiThreads = 32 * EW;
   constexpr int kHalves = EW / 4;                 // column groups per tile
   constexpr int kChunks = kTcBN / 32 / kHalves;   // 32-column chunks per epilogue warp
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int KB = p.KB;
   const int nst = p.stages;
   uint8_t* aaug_smem = smem;                                   // 4 KB, 1024-aligned
   uint8_t* a_smem = smem + kAAugBytes;                         // KB x 16 KB (1024-aligned)
-  uint8_t* b_smem = a_smem + (A_STREAM ? 0 : KB * kATileBytes);
+  uint8_t* b_smem = a_smem + (A_STREAM ? 0 : p.a_blocks * kATileBytes);
   const uint32_t stage_bytes = tc_stage_bytes(A_STREAM);
   const uint32_t b_off = A_STREAM ? kATileBytes : 0;           // B tile inside a stage
   const uint32_t baug_off = b_off + kBTileBytes;               // norm columns inside a stage
@@ -142,40 +197,48 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  const int total_units = p.m_tiles * p.S;
-
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      prefetch_tmap(&tmA);
-      prefetch_tmap(&tmB);
-      prefetch_tmap(&tmAaug);
-      prefetch_tmap(&tmBaug);
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        prefetch_tmap(&maps.a[g]);
+        prefetch_tmap(&maps.b[g]);
+        prefetch_tmap(&maps.baug[g]);
+      }
+      prefetch_tmap(&maps.aaug);
       // the query-side norm columns are the same for every tile: load once
       mbar_arrive_expect_tx(aaug_full, kAAugBytes);
-      tma_load_2d(aaug_smem, &tmAaug, aaug_full, 0, 0);
+      tma_load_2d(aaug_smem, &maps.aaug, aaug_full, 0, 0);
       uint32_t stage = 0, phase = 0, a_phase = 0;
-      for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-        const int s = u / p.m_tiles, t = u % p.m_tiles;
-        const int j0 = s * p.tiles_per_split;
-        const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+      UnitCursor<BATCH> cur(p);
+      TcUnit x;
+      while (cur.next(p, x)) {
+        const int KB = x.pr->KB;
+        const int g = G == 1 ? 0 : x.pr->group;
+        const int a_row = x.pr->a_row0 + x.t * kTcBM;
+        const int b_row0 = x.pr->b_row0;
+        const CUtensorMap* tmA = &maps.a[g];
+        const CUtensorMap* tmB = &maps.b[g];
+        const CUtensorMap* tmBaug = &maps.baug[g];
         if (!A_STREAM) {
           if (!mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A)) goto prod_done;
           a_phase ^= 1;
           mbar_arrive_expect_tx(a_full, KB * kATileBytes);
           for (int kb = 0; kb < KB; ++kb)
-            tma_load_2d(a_smem + kb * kATileBytes, &tmA, a_full, kb * kTcBK, t * kTcBM);
+            tma_load_2d(a_smem + kb * kATileBytes, tmA, a_full, kb * kTcBK, a_row);
         }
-        for (int j = j0; j < j1; ++j) {
+        for (int j = x.j0; j < x.j1; ++j) {
+          const int b_row = b_row0 + j * kTcBN;
           for (int kb = 0; kb < KB; ++kb) {
             if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) goto prod_done;
             uint8_t* st = b_smem + (size_t)stage * stage_bytes;
             const bool last = kb == KB - 1;
             mbar_arrive_expect_tx(&full[stage], (A_STREAM ? kATileBytes : 0) + kBTileBytes +
                                                     (last ? kBAugBytes : 0));
-            if (A_STREAM) tma_load_2d(st, &tmA, &full[stage], kb * kTcBK, t * kTcBM);
-            tma_load_2d(st + b_off, &tmB, &full[stage], kb * kTcBK, j * kTcBN);
-            if (last) tma_load_2d(st + baug_off, &tmBaug, &full[stage], 0, j * kTcBN);
+            if (A_STREAM) tma_load_2d(st, tmA, &full[stage], kb * kTcBK, a_row);
+            tma_load_2d(st + b_off, tmB, &full[stage], kb * kTcBK, b_row);
+            if (last) tma_load_2d(st + baug_off, tmBaug, &full[stage], 0, b_row);
             if (++stage == (uint32_t)nst) {
               stage = 0;
               phase ^= 1;
@@ -203,16 +266,16 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto mma_done;
       {
         const uint64_t aaug_desc = smem_desc_sw32(aaug_smem);
-        for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-          const int s = u / p.m_tiles;
-          const int j0 = s * p.tiles_per_split;
-          const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
+        UnitCursor<BATCH> cur(p);
+        TcUnit x;
+        while (cur.next(p, x)) {
+          const int KB = x.pr->KB;
           if (!A_STREAM) {
             if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto mma_done;
             a_phase ^= 1;
             tc_fence_after();
           }
-          for (int j = j0; j < j1; ++j) {
+          for (int j = x.j0; j < x.j1; ++j) {
             const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
             if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto mma_done;
             tc_fence_after();
@@ -242,7 +305,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
           }
           // Release the query tile for the next unit (not after the last one, so
           // no arrival can land after the CTA has exited).
-          if (!A_STREAM && u + (int)gridDim.x < total_units) mma_commit(a_empty);
+          if (!A_STREAM && cur.more()) mma_commit(a_empty);
         }
       }
     mma_done:;
@@ -256,20 +319,20 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     const int et = threadIdx.x - 64;        // 0 .. kEpiThreads-1
     float* spill = spill_all + et * kSpillStride;
     uint32_t acc_it = 0;
-    for (int u = blockIdx.x; u < total_units; u += gridDim.x) {
-      const int s = u / p.m_tiles, t = u % p.m_tiles;
-      const int j0 = s * p.tiles_per_split;
-      const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
-      const int row = t * kTcBM + row_in_tile;
-      const bool valid = row < p.m;
+    UnitCursor<BATCH> cur(p);
+    TcUnit x;
+    while (cur.next(p, x)) {
+      const TcProblem& pr = *x.pr;
+      const int row = x.t * kTcBM + row_in_tile;
+      const bool valid = row < pr.m;
       const int c0 = half * kChunks;  // first 32-column chunk of this warp
       Sink sink;
       if (valid) {
-        const int orig = p.perm ? p.perm[row] : row;
-        sink.init(p.sink, row, s * kHalves + half, p.E[row],
-                  p.exclude_self ? (int)(p.q_offset + orig) : -1);
+        const int orig = pr.perm ? pr.perm[row] : row;
+        sink.init(pr.sink, row, x.slot * kHalves + half, pr.E[row],
+                  pr.exclude_self ? (int)(pr.q_offset + orig) : -1);
       }
-      for (int j = j0; j < j1; ++j) {
+      for (int j = x.j0; j < x.j1; ++j) {
         // the other warps' k-th values for this query: consumed after the tile
         const uint32_t shared_key = valid ? sink.tile_fetch() : 0u;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
@@ -307,7 +370,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       }
       if (valid) {
         sink.tile_sync();
-        sink.finish(p.sink);
+        sink.finish(pr.sink);
       }
     }
   epi_done:;
@@ -321,26 +384,36 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
   }
 }
 
-struct TcMaps {
-  const CUtensorMap* a;
-  const CUtensorMap* b;
-  const CUtensorMap* aaug;
-  const CUtensorMap* baug;
-};
-
-template <class Sink, bool A_STREAM, int EW>
-int launch_tc_variant(const TcMaps& maps, const TcParams& p, int grid, cudaStream_t st) {
+template <class Sink, bool A_STREAM, int EW, bool BATCH>
+size_t tc_variant_smem(int KB_max, int* stages_out) {
   const size_t budget = 227 * 1024;
   int stages = 8;
-  while (stages > 2 && tc_smem_bytes(p.KB, stages, A_STREAM, EW) > budget) --stages;
+  while (stages > 2 && tc_smem_bytes(KB_max, stages, A_STREAM, EW) > budget) --stages;
+  if (stages_out) *stages_out = stages;
+  size_t smem = tc_smem_bytes(KB_max, stages, A_STREAM, EW);
+  return smem < kMinCtaSmem ? kMinCtaSmem : smem;
+}
+
+template <class Sink, bool A_STREAM, int EW, bool BATCH>
+int prepare_tc_variant(int KB_max) {
+  const size_t smem = tc_variant_smem<Sink, A_STREAM, EW, BATCH>(KB_max, nullptr);
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH>;
+  return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <class Sink, bool A_STREAM, int EW, bool BATCH>
+int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcParams& p, int KB_max,
+                      int grid, cudaStream_t st) {
+  int stages = 0;
+  const size_t smem = tc_variant_smem<Sink, A_STREAM, EW, BATCH>(KB_max, &stages);
   TcParams q = p;
   q.stages = stages;
-  const size_t smem = tc_smem_bytes(p.KB, stages, A_STREAM, EW);
-  auto kern = screen_tc_kernel<Sink, A_STREAM, EW>;
+  q.a_blocks = KB_max;
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
-  kern<<<grid, 64 + 32 * EW, smem, st>>>(*maps.a, *maps.b, *maps.aaug, *maps.baug, q);
+  kern<<<grid, 64 + 32 * EW, smem, st>>>(maps, q);
   return (int)cudaGetLastError();
 }
 
@@ -354,26 +427,32 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st, const int* perm) {
   TcParams p{};
-  p.m = (int)m;
-  p.KB = ix->dp / kTcBK;
-  p.n_tiles = (int)(ix->n_pad_tc / kTcBN);
+  TcProblem& one = p.one;
+  one.m = (int)m;
+  one.KB = ix->dp / kTcBK;
+  one.n_tiles = (int)(ix->n_pad_tc / kTcBN);
+  one.tiles_per_split = (one.n_tiles + S - 1) / S;
+  one.exclude_self = exclude_self;
+  one.q_offset = q_offset;
+  one.E = E;
+  one.perm = perm;
+  one.sink = sa;
   p.S = S;
-  p.tiles_per_split = (p.n_tiles + S - 1) / S;
   p.m_tiles = (int)(m_pad / kTcBM);
-  p.exclude_self = exclude_self;
-  p.q_offset = q_offset;
-  p.E = E;
-  p.perm = perm;
-  p.sink = sa;
   p.status = status;
-  const bool a_stream = p.KB > 4;
+  const int KB = one.KB;
+  const bool a_stream = KB > 4;
   const int units = p.m_tiles * S;
   const int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
   if (grid <= 0) return 0;
-  const TcMaps maps{tmap_a, &ix->tmap_b, &ix->tmap_aaug, &ix->tmap_baug};
-#define B2K_TC_LAUNCH(SINK, EW)                                  \
-  (a_stream ? launch_tc_variant<SINK, true, EW>(maps, p, grid, st) \
-            : launch_tc_variant<SINK, false, EW>(maps, p, grid, st))
+  TcMapSet<1> maps;
+  maps.a[0] = *tmap_a;
+  maps.b[0] = ix->tmap_b;
+  maps.baug[0] = ix->tmap_baug;
+  maps.aaug = ix->tmap_aaug;
+#define B2K_TC_LAUNCH(SINK, EW)                                                \
+  (a_stream ? launch_tc_variant<SINK, true, EW, false>(maps, p, KB, grid, st) \
+            : launch_tc_variant<SINK, false, EW, false>(maps, p, KB, grid, st))
   if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, 4);
   if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
   if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 8);
@@ -383,5 +462,57 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   return B2K_TC_LAUNCH(KnnSink<64>, 4);
 #undef B2K_TC_LAUNCH
 }
+
+// Batched launches: kNN sinks only.  Heap widths 8/12/16 run with 4 or 8
+// epilogue warps, 32/64 with 4 (register budget).
+#define B2K_TC_BATCH_DISPATCH(CALL)                                         \
+  switch (kmax * 16 + ew) {                                                 \
+    case 8 * 16 + 8: return CALL(KnnSink<8>, 8);                            \
+    case 8 * 16 + 4: return CALL(KnnSink<8>, 4);                            \
+    case 12 * 16 + 8: return CALL(KnnSink<12>, 8);                          \
+    case 12 * 16 + 4: return CALL(KnnSink<12>, 4);                          \
+    case 16 * 16 + 8: return CALL(KnnSink<16>, 8);                          \
+    case 16 * 16 + 4: return CALL(KnnSink<16>, 4);                          \
+    case 32 * 16 + 4: return CALL(KnnSink<32>, 4);                          \
+    case 64 * 16 + 4: return CALL(KnnSink<64>, 4);                          \
+    default: return (int)cudaErrorInvalidValue;                             \
+  }
+
+int prepare_screen_tc_batch(int kmax, int ew, bool a_stream, int KB_max) {
+  if (!a_stream && KB_max > 4) return (int)cudaErrorInvalidValue;
+#define B2K_PREP(SINK, EW)                                         \
+  (a_stream ? prepare_tc_variant<SINK, true, EW, true>(KB_max) \
+            : prepare_tc_variant<SINK, false, EW, true>(KB_max))
+  B2K_TC_BATCH_DISPATCH(B2K_PREP)
+#undef B2K_PREP
+}
+
+int launch_screen_tc_batch(const TcBatchLaunch& L, cudaStream_t st) {
+  if (L.grid <= 0) return 0;
+  if (L.groups < 1 || L.groups > kBatchGroups) return (int)cudaErrorInvalidValue;
+  if (!L.a_stream && L.KB_max > 4) return (int)cudaErrorInvalidValue;
+  TcMapSet<kBatchGroups> maps;
+  for (int g = 0; g < kBatchGroups; ++g) {
+    // unused slots repeat group 0 (never addressed: every problem names a live group)
+    const int s = g < L.groups ? g : 0;
+    maps.a[g] = L.a[s];
+    maps.b[g] = L.b[s];
+    maps.baug[g] = L.baug[s];
+  }
+  maps.aaug = L.aaug;
+  TcParams p{};
+  p.probs = L.probs;
+  p.items = L.items;
+  p.cta_begin = L.cta_begin;
+  p.status = L.status;
+  const int kmax = L.kmax, ew = L.ew, KB = L.KB_max, grid = L.grid;
+  const bool a_stream = L.a_stream;
+#define B2K_LAUNCH(SINK, EW)                                                       \
+  (a_stream ? launch_tc_variant<SINK, true, EW, true>(maps, p, KB, grid, st) \
+            : launch_tc_variant<SINK, false, EW, true>(maps, p, KB, grid, st))
+  B2K_TC_BATCH_DISPATCH(B2K_LAUNCH)
+#undef B2K_LAUNCH
+}
+#undef B2K_TC_BATCH_DISPATCH
 
 }  // namespace b2k

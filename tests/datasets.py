@@ -53,3 +53,25 @@ def cfg3(n=200_000, m=50_000, d=32):
     X, y = mixture(rng, n, cen, 1.0)
     Q, _ = mixture(np.random.default_rng(40), m, cen, 1.0)
     return X, y, Q
+
+
+def cfg4(seed=5, problems=256, n_range=(1_000, 200_000), m_range=(100, 20_000),
+         dims=(16, 32, 64, 128, 256), ks=(1, 5, 10, 50)):
+    """Batched uneven problems: n_ref and n_query log-uniform over their
+    ranges, d and k drawn from their sets, rows i.i.d. N(0,1) float32, and 1%
+    of each problem's reference rows duplicated (ties).  Returns a list of
+    (X, Q, k) in draw order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(problems):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        m = int(round(np.exp(rng.uniform(np.log(m_range[0]), np.log(m_range[1])))))
+        d = int(rng.choice(dims))
+        k = int(rng.choice(ks))
+        X = rng.standard_normal((n, d)).astype(np.float32)
+        dup = max(1, n // 100)
+        dst = rng.choice(n, dup, replace=False)
+        X[dst] = X[rng.integers(0, n, dup)]
+        Q = rng.standard_normal((m, d)).astype(np.float32)
+        out.append((X, Q, min(k, n)))
+    return out
