@@ -94,8 +94,21 @@ struct RowTracker {
   }
   B2K_DEV void sync_shared() { apply_shared(fetch_shared()); }
 
+  // The list is full: drop the entries above the current threshold.  T only
+  // decreases, and (see above) every value above it is more than 2E above the
+  // final V_k, so the certify pass would discard those entries anyway.
+  B2K_DEV void compact() {
+    int w = 0;
+    for (int i = 0; i < cap; ++i) {
+      const int2 e = list[i];
+      if (__int_as_float(e.x) <= T) list[w++] = e;
+    }
+    cnt = w;
+  }
+
   // Caller guarantees v <= T and col is not the excluded self column.
   B2K_DEV void admit(float v, int col) {
+    if (cnt == cap) compact();
     if (cnt < cap) list[cnt] = make_int2(__float_as_int(v), col);
     ++cnt;
     if (v < kv[KMAX - 1]) {

@@ -220,3 +220,20 @@ def test_query_grouping_both_ways(mode, reorder, monkeypatch):
     dist, idx = index.query(X, 6, exclude_self=True, mode=mode)
     np.testing.assert_array_equal(idx, oi)
     np.testing.assert_array_equal(dist, od)
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_full_lists_are_compacted_not_rescanned(mode):
+    # k = 50 over 120k i.i.d. rows: a list admits ~k (1 + ln(n / k)) entries
+    # while its k-th value settles, more than one list holds; full lists drop
+    # what is above the running threshold instead of sending the row to the
+    # exhaustive scan.
+    rng = np.random.default_rng(17)
+    X = rng.standard_normal((120_000, 64)).astype(np.float32)
+    Q = rng.standard_normal((300, 64)).astype(np.float32)
+    od, oi = oracle.knn(X, Q, 50)
+    ix = make_index(X)
+    dist, idx = ix.query(Q, 50, mode=mode, stats=True)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+    assert ix.last_stats["fallback_rows"] == 0
