@@ -370,8 +370,10 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     fr.keep(so.lists);
     if ((rc = dalloc(&so.counts, (size_t)S_lists * m_pad, st))) return rc;
     fr.keep(so.counts);
-    if ((rc = dalloc(&so.kth, (size_t)S_lists * m_pad * k, st))) return rc;
-    fr.keep(so.kth);
+    if (!(tc && tc_lazy_sink(k))) {  // lazy screens leave V_k to the lists
+      if ((rc = dalloc(&so.kth, (size_t)S_lists * m_pad * k, st))) return rc;
+      fr.keep(so.kth);
+    }
     SinkArgs sa{};
     sa.out = so;
     sa.k = k;

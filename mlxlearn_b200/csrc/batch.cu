@@ -67,13 +67,12 @@ int bfail(int code, const char* fmt, ...) {
 
 int64_t rup(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-int kmax_class(int k) {
-  return k <= 8 ? 8 : k <= 12 ? 12 : k <= 16 ? 16 : k <= 32 ? 32 : 64;
-}
+// heap width of the screen's tracker; 64 = the lazy tracker (k > 16)
+int kmax_class(int k) { return k <= 8 ? 8 : k <= 12 ? 12 : k <= 16 ? 16 : 64; }
 
 // ---------------------------------------------------------------- tuning
 struct Tuning {
-  int ew8 = 1;  // 8 epilogue warps (heap widths <= 16), else 4
+  int ew8 = 1;  // 8 epilogue warps, else 4
 };
 struct TuneKey {
   int dp, kmax;
@@ -352,7 +351,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
   for (auto& p : b->probs) {
     if (!p.in_graph) continue;
     const Tuning t = tuning_for(p, tune);
-    p.ew = (p.kmax <= 16 && t.ew8) ? 8 : 4;
+    p.ew = t.ew8 ? 8 : 4;
     p.halves = p.ew / 4;
     total_cost += (double)p.m_tiles * p.n_tiles * (p.KB + 1);
     classes[std::make_tuple(p.kmax, p.ew, p.KB > 4)].push_back((int)(&p - b->probs.data()));
@@ -375,7 +374,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
     p.kth_off = kth;
     lists += (size_t)p.S_lists * p.m_pad * p.cap;
     counts += (size_t)p.S_lists * p.m_pad;
-    kth += (size_t)p.S_lists * p.m_pad * p.k;
+    if (p.kmax != 64) kth += (size_t)p.S_lists * p.m_pad * p.k;  // lazy: none
   }
   Owned& o = b->tuned;
   int rc;
@@ -410,7 +409,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
       ScreenOut so{};
       so.lists = d_lists + p.lists_off;
       so.counts = d_counts + p.counts_off;
-      so.kth = d_kth + p.kth_off;
+      so.kth = p.kmax == 64 ? nullptr : d_kth + p.kth_off;
       so.cap = p.cap;
       so.m_pad = p.m_pad;
       TcProblem& t = tc[p.gi];
@@ -652,7 +651,6 @@ int autotune(b2k_batch* b, std::map<TuneKey, Tuning>& tune, int& gran) {
   gran = best_gran;
   // epilogue width per (dp, heap width) bucket
   for (const TuneKey& k : keys) {
-    if (k.kmax > 16) continue;
     Tuning cur = tune.count(k) ? tune[k] : Tuning{};
     Tuning alt = cur;
     alt.ew8 = !cur.ew8;
@@ -753,7 +751,7 @@ int b2k_batch_create(const b2k_problem* problems, int32_t count, int32_t flags, 
   if ((flags & B2K_BATCH_AUTOTUNE) && b->n_graph > 0) {
     bool cached = g_gran != 0;
     for (auto& p : b->probs)
-      if (p.in_graph && p.kmax <= 16 && !tune.count(TuneKey{p.dp, p.kmax})) cached = false;
+      if (p.in_graph && !tune.count(TuneKey{p.dp, p.kmax})) cached = false;
     if (!cached) {
       cudaEvent_t t0, t1;
       cudaEventCreate(&t0);

@@ -121,17 +121,17 @@ __device__ unsigned warp_sort_resolve(double* s, int* id, int C, int k, const fl
 
 // k-th smallest (1-based) of `count` unsigned keys, by one warp: four 8-bit
 // radix passes with a 256-bin shared-memory histogram (`hist`).
-template <class KeyFn>
-__device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* hist, int lane) {
+// `visit(f)` calls f(key) for every key this lane owns.
+template <class Visit>
+__device__ uint32_t warp_radix_select(Visit visit, int k, unsigned* hist, int lane) {
   uint32_t prefix = 0, mask = 0;
   unsigned rank = (unsigned)k;
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int b = lane; b < 256; b += 32) hist[b] = 0;
     __syncwarp();
-    for (int i = lane; i < count; i += 32) {
-      const uint32_t key = key_of(i);
+    visit([&](uint32_t key) {
       if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
-    }
+    });
     __syncwarp();
     unsigned local[8], s = 0;
 #pragma unroll
@@ -170,6 +170,15 @@ __device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* his
     __syncwarp();
   }
   return prefix;
+}
+
+template <class KeyFn>
+__device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* hist, int lane) {
+  return warp_radix_select(
+      [&](auto f) {
+        for (int i = lane; i < count; i += 32) f(key_of(i));
+      },
+      k, hist, lane);
 }
 
 // fp32 direct squared distance of candidate rows, 8 lanes per row (coalesced
@@ -277,10 +286,23 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   }
   entries = __reduce_add_sync(0xffffffffu, entries);
 
-  // 2. V_k = k-th smallest of the lists' k smallest values (radix select)
+  // 2. V_k = k-th smallest of the lists' k smallest values (radix select);
+  // screens without per-slot k-th values list every value up to their own
+  // threshold, which covers the k smallest overall: select over the lists.
   const int total = S * k;
   float Vk;
-  if (total <= kCertifyCap) {
+  if (!so.kth) {
+    Vk = key_float(warp_radix_select(
+        [&](auto f) {
+          for (int s = 0; s < S; ++s) {
+            const size_t slot = (size_t)s * so.m_pad + row;
+            const int cnt = so.counts[slot];
+            const int2* lst = so.lists + slot * so.cap;
+            for (int i = lane; i < cnt; i += 32) f(float_key(__int_as_float(lst[i].x)));
+          }
+        },
+        k, hist, lane));
+  } else if (total <= kCertifyCap) {
     uint32_t* keys = reinterpret_cast<uint32_t*>(ci);  // ci is free until step 3
     for (int i = lane; i < total; i += 32) {
       const int s = i / k, t = i % k;

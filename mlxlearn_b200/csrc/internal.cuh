@@ -27,7 +27,7 @@ constexpr int kMaxK = 64;          // largest k the screens track in registers
 struct ScreenOut {
   int2* lists;     // [S][m_pad][cap]
   int* counts;     // [S][m_pad]
-  float* kth;      // [S][m_pad][k]
+  float* kth;      // [S][m_pad][k], or null: the lists alone give V_k (lazy screens)
   int cap;
   int m_pad;
 };
@@ -108,6 +108,7 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
                      const SinkArgs& sa, int* status, cudaStream_t st,
                      const int* perm = nullptr);
 int tc_column_groups(int k);
+bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
                         int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                         const SinkArgs& sa, cudaStream_t st, const int* perm = nullptr);

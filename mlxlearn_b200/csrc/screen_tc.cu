@@ -326,24 +326,33 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       const int row = x.t * kTcBM + row_in_tile;
       const bool valid = row < pr.m;
       const int c0 = half * kChunks;  // first 32-column chunk of this warp
+      // warp-collective sinks run on every lane (inactive past the block's end)
+      const bool live = Sink::kWarpWide || valid;
       Sink sink;
-      if (valid) {
+      if constexpr (Sink::kWarpWide) {
+        const int orig = valid ? (pr.perm ? pr.perm[row] : row) : 0;
+        sink.init_warp(pr.sink, row, x.slot * kHalves + half, valid ? pr.E[row] : 0.0f,
+                       (valid && pr.exclude_self) ? (int)(pr.q_offset + orig) : -1, valid,
+                       reinterpret_cast<unsigned*>(spill_all + (size_t)ew * 32 * kSpillStride));
+      } else if (valid) {
         const int orig = pr.perm ? pr.perm[row] : row;
         sink.init(pr.sink, row, x.slot * kHalves + half, pr.E[row],
                   pr.exclude_self ? (int)(pr.q_offset + orig) : -1);
       }
       for (int j = x.j0; j < x.j1; ++j) {
         // the other warps' k-th values for this query: consumed after the tile
-        const uint32_t shared_key = valid ? sink.tile_fetch() : 0u;
+        const uint32_t shared_key = live ? sink.tile_fetch() : 0u;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
-        if (!mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)) goto epi_done;
+        // warp-uniform outcome, so collective sinks never run on a partial warp
+        if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)))
+          goto epi_done;
         tc_fence_after();
         const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN + c0 * 32;
         auto process = [&](const uint32_t(&r)[32], int c) {
           float v[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-          if (valid) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
+          if (live) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
         };
         // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
         uint32_t ra[32], rb[32];
@@ -366,9 +375,12 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
           }
         }
         ++acc_it;
-        if (valid) sink.tile_apply(shared_key);
+        if (live) sink.tile_apply(shared_key);
       }
-      if (valid) {
+      if constexpr (Sink::kWarpWide) {
+        sink.tile_sync();
+        sink.finish_warp(pr.sink);
+      } else if (valid) {
         sink.tile_sync();
         sink.finish(pr.sink);
       }
@@ -421,7 +433,8 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
 
 // Column groups (epilogue warps per TMEM lane group) of the kNN screen for k:
 // each group keeps its own candidate lists.
-int tc_column_groups(int k) { return k <= 16 ? 2 : 1; }
+int tc_column_groups(int k) { return k > 0 ? 2 : 1; }
+bool tc_lazy_sink(int k) { return k > 16; }
 
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
@@ -457,14 +470,13 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
   if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 8);
   if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 8);
-  if (sa.k <= 16) return B2K_TC_LAUNCH(KnnSink<16>, 8);
-  if (sa.k <= 32) return B2K_TC_LAUNCH(KnnSink<32>, 4);
-  return B2K_TC_LAUNCH(KnnSink<64>, 4);
+  if (!tc_lazy_sink(sa.k)) return B2K_TC_LAUNCH(KnnSink<16>, 8);
+  return B2K_TC_LAUNCH(LazyKnnSink, 8);
 #undef B2K_TC_LAUNCH
 }
 
-// Batched launches: kNN sinks only.  Heap widths 8/12/16 run with 4 or 8
-// epilogue warps, 32/64 with 4 (register budget).
+// Batched launches: kNN sinks only, with 4 or 8 epilogue warps.  Heap width
+// class 64 stands for the lazy tracker (every k > 16).
 #define B2K_TC_BATCH_DISPATCH(CALL)                                         \
   switch (kmax * 16 + ew) {                                                 \
     case 8 * 16 + 8: return CALL(KnnSink<8>, 8);                            \
@@ -473,8 +485,8 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
     case 12 * 16 + 4: return CALL(KnnSink<12>, 4);                          \
     case 16 * 16 + 8: return CALL(KnnSink<16>, 8);                          \
     case 16 * 16 + 4: return CALL(KnnSink<16>, 4);                          \
-    case 32 * 16 + 4: return CALL(KnnSink<32>, 4);                          \
-    case 64 * 16 + 4: return CALL(KnnSink<64>, 4);                          \
+    case 64 * 16 + 8: return CALL(LazyKnnSink, 8);                          \
+    case 64 * 16 + 4: return CALL(LazyKnnSink, 4);                          \
     default: return (int)cudaErrorInvalidValue;                             \
   }
 

@@ -38,6 +38,7 @@ __device__ __forceinline__ float min32(const float (&v)[32]) {
 
 template <int KMAX>
 struct KnnSink {
+  static constexpr bool kWarpWide = false;
   RowTracker<KMAX> tr;
   size_t slot;
   B2K_DEV void init(const SinkArgs& a, int row, int split, float E, int self) {
@@ -59,6 +60,7 @@ struct KnnSink {
 };
 
 struct RadiusCountSink {
+  static constexpr bool kWarpWide = false;
   float T;
   int self, cnt;
   size_t slot;
@@ -82,6 +84,7 @@ struct RadiusCountSink {
 };
 
 struct RadiusFillSink {
+  static constexpr bool kWarpWide = false;
   float T;
   int self;
   int* out;
@@ -105,6 +108,34 @@ struct RadiusFillSink {
   B2K_DEV uint32_t tile_fetch() const { return 0; }
   B2K_DEV void tile_apply(uint32_t) {}
   B2K_DEV void finish(const SinkArgs&) {}
+};
+
+// kNN sink for large k on the lazy tracker (tracker.cuh).  Warp-collective:
+// every lane of the warp calls every method, `active` false for rows past the
+// end of the query block; `hist` is the warp's 256-word shared scratch.
+static_assert(kListCap <= 512, "the lazy tracker's warp select holds 16 entries per lane");
+struct LazyKnnSink {
+  static constexpr bool kWarpWide = true;
+  LazyTracker tr;
+  size_t slot;
+  unsigned* hist;
+  int lane;
+  B2K_DEV void init_warp(const SinkArgs& a, int row, int split, float E, int self, bool active,
+                         unsigned* warp_hist) {
+    slot = (size_t)split * a.out.m_pad + row;
+    hist = warp_hist;
+    lane = threadIdx.x & 31;
+    tr.init(a.k, E, self, a.out.lists + slot * a.out.cap, a.out.cap,
+            a.shared_kth ? a.shared_kth + row : nullptr, active);
+  }
+  B2K_DEV void tile_sync() { tr.sync_shared(); }
+  B2K_DEV uint32_t tile_fetch() const { return tr.fetch_shared(); }
+  B2K_DEV void tile_apply(uint32_t key) { tr.apply_shared(key); }
+  B2K_DEV void offer32(const float (&v)[32], int col0, float*) { tr.offer32(v, col0, hist, lane); }
+  // Only the list length: the certify pass selects V_k from the lists.
+  B2K_DEV void finish_warp(const SinkArgs& a) {
+    if (tr.active) a.out.counts[slot] = tr.cnt;
+  }
 };
 
 }  // namespace b2k

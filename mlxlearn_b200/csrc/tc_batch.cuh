@@ -42,8 +42,8 @@ struct TcBatchLaunch {
   const int* cta_begin;
   int grid;
   int KB_max;
-  int kmax;       // heap width class: 8, 12, 16, 32 or 64
-  int ew;         // epilogue warps: 4, or 8 (kmax <= 16)
+  int kmax;       // heap width class: 8, 12, 16, or 64 (lazy tracker, k > 16)
+  int ew;         // epilogue warps: 4 or 8
   bool a_stream;  // stream the query tile with every block (KB_max > 4)
   int* status;
 };

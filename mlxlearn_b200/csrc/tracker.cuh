@@ -165,4 +165,199 @@ struct RowTracker {
   }
 };
 
+// Lazy form for large k (the insertion network above costs O(KMAX) per
+// admission, and while the k-th value settles a row admits about
+// k (1 + ln(n / k)) values).  No per-row heap: every v <= T is appended, and
+// T is refreshed from the list itself when the list nears capacity: the
+// whole warp selects the row's k-th smallest listed value V (radix select in
+// shared memory), sets T = min(V, shared) + 2E and drops the entries above
+// T.  The list always holds every value seen that is <= the current T, in
+// particular the k smallest seen so far, so V is the k-th smallest value seen
+// and the certificate argument above applies unchanged.
+//
+// Every method is warp-collective: all 32 lanes call it, rows past the end
+// of the query block included (inactive: they admit nothing).
+struct LazyTracker {
+  float T, E2, shared_kth, own_kth;
+  int cnt, self, cap, k;
+  int trig;  // compact once cnt exceeds this (cap - 32)
+  int2* list;
+  uint32_t* shared;
+  bool active, dirty;
+
+  B2K_DEV void init(int k_, float E, int self_col, int2* lst, int cap_, uint32_t* shared_word,
+                    bool active_) {
+    active = active_;
+    T = active_ ? INFINITY : -INFINITY;
+    E2 = __fmul_ru(2.0f, E);
+    shared_kth = INFINITY;
+    own_kth = INFINITY;
+    cnt = 0;
+    self = self_col;
+    k = k_;
+    list = lst;
+    cap = cap_;
+    trig = cap_ - 32;
+    shared = active_ ? shared_word : nullptr;
+    dirty = false;
+  }
+
+  B2K_DEV uint32_t fetch_shared() const {
+    uint32_t key = kNoKey;
+    if (shared) asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(key) : "l"(shared));
+    return key;
+  }
+  B2K_DEV void apply_shared(uint32_t key) {
+    if (!shared) return;
+    if (dirty) {
+      atomicMin(shared, float_key(own_kth));
+      dirty = false;
+    }
+    if (key != kNoKey) {
+      const float g = key_float(key);
+      if (g < shared_kth) {
+        shared_kth = g;
+        T = fminf(T, __fadd_ru(g, E2));
+      }
+    }
+  }
+  B2K_DEV void sync_shared() { apply_shared(fetch_shared()); }
+
+  // k-th smallest value of lane `src`'s list (c entries, c >= kk), by the
+  // whole warp: keys in registers, 4 radix passes over a 256-bin histogram in
+  // `hist` (this warp's shared memory).  Also returns how many are smaller.
+  B2K_DEV static uint32_t warp_kth(const int2* lst, int c, int kk, unsigned* hist, int lane,
+                                   int* n_less) {
+    constexpr int kPer = 16;  // up to 512 entries
+    uint32_t key[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = lane + 32 * j;
+      key[j] = i < c ? float_key(__int_as_float(lst[i].x)) : 0xffffffffu;
+    }
+    uint32_t prefix = 0, mask = 0;
+    int rank = kk, less = 0;
+#pragma unroll 1
+    for (int shift = 24; shift >= 0; shift -= 8) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < kPer; ++j)
+        if (lane + 32 * j < c && (key[j] & mask) == prefix)
+          atomicAdd(&hist[(key[j] >> shift) & 255u], 1u);
+      __syncwarp();
+      unsigned local[8], sum = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        local[b] = hist[lane * 8 + b];
+        sum += local[b];
+      }
+      unsigned incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const unsigned excl = incl - sum;
+      // the lane whose bins cross `rank` finds the digit
+      int digit = -1;
+      unsigned below = 0;
+      if (excl < (unsigned)rank && incl >= (unsigned)rank) {
+        unsigned acc = excl;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          if (digit < 0 && acc + local[b] >= (unsigned)rank) {
+            digit = lane * 8 + b;
+            below = acc;
+          }
+          acc += local[b];
+        }
+      }
+      const unsigned owner = __ballot_sync(0xffffffffu, digit >= 0);
+      const int src_lane = __ffs(owner) - 1;
+      digit = __shfl_sync(0xffffffffu, digit, src_lane);
+      below = __shfl_sync(0xffffffffu, below, src_lane);
+      rank -= (int)below;
+      less += (int)below;
+      prefix |= (uint32_t)digit << shift;
+      mask |= 255u << shift;
+      __syncwarp();
+    }
+    *n_less = less;
+    return prefix;
+  }
+
+  // Compact the lists that are within 32 entries of capacity (a chunk admits
+  // at most 32 values per row).  Each compaction costs the warp ~200
+  // instructions; a row scanning n columns needs about
+  // k (1 + ln(n / k)) / (cap - k) of them.
+  B2K_DEV void maintain(unsigned* hist, int lane) {
+    unsigned todo = __ballot_sync(0xffffffffu, active && cnt > trig && cnt >= k && cnt <= cap);
+    if (todo) __syncwarp();  // the lanes' appends are visible to the whole warp
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      int2* lst = reinterpret_cast<int2*>(__shfl_sync(0xffffffffu, (unsigned long long)list, src));
+      const int c = __shfl_sync(0xffffffffu, cnt, src);
+      const int kk = __shfl_sync(0xffffffffu, k, src);
+      const float e2 = __shfl_sync(0xffffffffu, E2, src);
+      const float sh = __shfl_sync(0xffffffffu, shared_kth, src);
+      int n_less;
+      const float V = key_float(warp_kth(lst, c, kk, hist, lane, &n_less));
+      const float Tn = __fadd_ru(fminf(V, sh), e2);
+      // in-place stream compaction: writes never pass the reads of the same
+      // or a later round
+      int w = 0;
+      for (int base = 0; base < c; base += 32) {
+        const int i = base + lane;
+        int2 e = make_int2(0, 0);
+        bool keep = false;
+        if (i < c) {
+          e = lst[i];
+          keep = __int_as_float(e.x) <= Tn;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) lst[w + __popc(bal & ((1u << lane) - 1))] = e;
+        w += __popc(bal);
+      }
+      __syncwarp();
+      if (lane == src) {
+        cnt = w;
+        own_kth = V;
+        T = fminf(T, Tn);
+        dirty = true;
+      }
+    }
+  }
+
+  B2K_DEV void offer32(const float (&v)[32], int col0, unsigned* hist, int lane) {
+    float g[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float a = min3f(v[8 * q], v[8 * q + 1], v[8 * q + 2]);
+      const float b = min3f(v[8 * q + 3], v[8 * q + 4], v[8 * q + 5]);
+      g[q] = min3f(a, b, fminf(v[8 * q + 6], v[8 * q + 7]));
+    }
+    if (fminf(min3f(g[0], g[1], g[2]), g[3]) <= T) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (g[q] <= T) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const float x = v[8 * q + e];
+            const int col = col0 + 8 * q + e;
+            if (x <= T && col != self) {
+              if (cnt < cap) list[cnt] = make_int2(__float_as_int(x), col);
+              ++cnt;
+            }
+          }
+        }
+      }
+    }
+    maintain(hist, lane);
+  }
+
+};
+
 }  // namespace b2k
