@@ -592,6 +592,65 @@ def run_batch(args):
     return 0
 
 
+def run_chamfer(args):
+    """Differentiable kNN losses: 64 symmetric k=1 Chamfer terms on 8192 x 3
+    clouds plus a self k=8 mean-distance term on 4096 x 64, forward + backward."""
+    import torch
+
+    from datasets import cfg5
+    from mlxlearn_b200.autograd import chamfer_loss, knn_distances
+
+    import oracle
+
+    torch.cuda.set_device(0)
+    threads = os.cpu_count() or 1
+    clouds, S = cfg5()
+    A = [torch.from_numpy(a).cuda().requires_grad_() for a, _ in clouds]
+    B = [torch.from_numpy(b).cuda().requires_grad_() for _, b in clouds]
+    Sd = torch.from_numpy(S).cuda().requires_grad_()
+    pairs = sum(2 * a.shape[0] * b.shape[0] for a, b in clouds) + S.shape[0] * S.shape[0]
+
+    def step():
+        loss = sum(chamfer_loss(a, b) for a, b in zip(A, B))
+        d8, _ = knn_distances(Sd, None, 8)
+        loss = loss + d8.mean()
+        loss.backward()
+        return loss
+
+    s, loss = _timed_wall(step, args.steps, args.warmup)
+    # CPU baseline: the reference's exact scan for the forward of two pairs
+    # (both directions) and torch float64 autograd on the CPU for their backward
+    ref = oracle.ref_native()
+    t0 = time.perf_counter()
+    cpu_pairs = 0
+    for a, b in clouds[:2]:
+        for P, Qr in ((a, b), (b, a)):
+            dist = np.empty((len(P), 1)); idx = np.empty((len(P), 1), np.int64)
+            _ref_knn_threads(ref, Qr, P, 1, dist, idx, threads)
+            Pt = torch.from_numpy(P).double().requires_grad_()
+            Qt = torch.from_numpy(Qr).double().requires_grad_()
+            ((Pt - Qt[torch.from_numpy(idx[:, 0])]) ** 2).sum().backward()
+            cpu_pairs += len(P) * len(Qr)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "differentiable kNN: (query, reference) pairs/s, forward + backward "
+                  "(64 Chamfer k=1 pairs of 8192x3 + self k=8 on 4096x64)",
+        "value": pairs / s, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * s, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: cfg5 recipe (seed 6)", "workload_kind": "secondary",
+        "config": {"workload": "knn_chamfer_64x8192x3_self4096x64", "pairs_per_step": pairs,
+                   "api": "mlxlearn_b200.autograd (public), wall clock with device sync"},
+        "loss": float(loss.item()),
+        "cpu_baseline": {"value": cpu_pairs / cpu_s, "unit": "pairs/s", "cores": threads,
+                         "kind": "reference" if ref else "port",
+                         "sample": "2 Chamfer pairs both ways: reference exact scan forward, "
+                                   "torch float64 CPU autograd backward"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def _ref_knn_threads(ref, X, Q, k, dist, idx, threads):
     """The reference's exact native kNN scan over query blocks in threads."""
     from concurrent.futures import ThreadPoolExecutor
@@ -622,10 +681,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="knn",
-                    choices=["knn", "pixels", "radius", "small", "batch"])
+                    choices=["knn", "pixels", "radius", "small", "batch", "chamfer"])
     ap.add_argument("--profile", action="store_true",
                     help="profiling driver: only the bf16 device-resident steps of the "
                          "headline workload (no fp32 leg, e2e or CPU baseline)")
+    ap.add_argument("--mode", default="bf16", choices=["bf16", "fp32", "exact", "auto"],
+                    help="screen form for --profile")
+    ap.add_argument("--k", type=int, default=K, help="neighbours for --profile")
     ap.add_argument("--problems", type=int, default=256,
                     help="problem count of the batch workload (the benchmark uses 256)")
     ap.add_argument("--queries", type=int, default=N_QUERY,
@@ -635,6 +697,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "chamfer":
+        return run_chamfer(args)
     if args.profile:
         return run_profile(args)
     if args.workload != "knn":
@@ -643,7 +707,7 @@ def main():
 
 
 def run_profile(args):
-    """bf16 screen + certify on the headline index, `--queries` queries."""
+    """Screen + certify on the headline index, `--queries` queries, `--mode`."""
     import torch
 
     from datasets import cfg2a
@@ -654,12 +718,13 @@ def run_profile(args):
     index = build_index(X)
     Qd = torch.from_numpy(Q).cuda()
     for _ in range(args.warmup):
-        index.query_device(Qd, K, mode="bf16")
+        index.query_device(Qd, args.k, mode=args.mode)
     torch.cuda.synchronize()
     for _ in range(args.steps):
-        index.query_device(Qd, K, mode="bf16", stats=True)
+        index.query_device(Qd, args.k, mode=args.mode, stats=True)
     torch.cuda.synchronize()
-    print(json.dumps({"profile": True, "queries": args.queries, "stats": index.last_stats}))
+    print(json.dumps({"profile": True, "queries": args.queries, "mode": args.mode, "k": args.k,
+                      "stats": index.last_stats}))
     return 0
 
 

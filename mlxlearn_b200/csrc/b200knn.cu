@@ -328,7 +328,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     const int sms = num_sms(ix.device);
     S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
     // lists per query: one per (split, column group of the screen)
-    const int S_lists = S * (tc ? tc_column_groups(k) : 1);
+    const int S_lists = S * (tc ? tc_column_groups(k) : simt_column_groups(kSinkKnn));
     // Group nearby queries (reorder.cu); results go back to the original rows.
     const int* perm = nullptr;
     const float* Qs = dQ;

@@ -15,7 +15,7 @@ constexpr int kTcBN = 256;   // reference rows per tcgen05 tile (TMEM columns)
 constexpr int kTcBK = 64;    // 16-bit elements per 128-byte swizzle row
 constexpr int kTcAug = 16;   // norm columns appended to every operand row (one K=16 step)
 constexpr int kSimtBM = 128; // query rows per CUDA-core tile
-constexpr int kSimtBN = 128; // reference rows per CUDA-core tile
+constexpr int kSimtBN = 64;  // reference rows per CUDA-core tile
 constexpr int kListCap = 512;      // screen list entries per (split, query)
 constexpr int kCertifyCap = 1024;  // re-rank candidates per query held in shared memory
 constexpr int kExactCap = 4096;    // exhaustive-scan candidates per query
@@ -109,9 +109,13 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
                      const int* perm = nullptr);
 int tc_column_groups(int k);
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
+// noalloc: one scanner per row (half the list memory of the default two)
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
                         int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                        const SinkArgs& sa, cudaStream_t st, const int* perm = nullptr);
+                        const SinkArgs& sa, cudaStream_t st, const int* perm = nullptr,
+                        bool noalloc = false);
+// candidate lists per (split, query) of the CUDA-core screen
+int simt_column_groups(int sink_kind, bool noalloc = false);
 
 // ----------------------------------------------------------- query order
 int pivot_count(int64_t n);

@@ -152,7 +152,8 @@ extern "C" B2K_API int b2k_knn_device_noalloc(b2k_index* h, const float* dQ, int
     SinkArgs sa{};
     sa.out = so;
     sa.k = k;
-    launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, 1, E, kSinkKnn, sa, st);
+    launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, 1, E, kSinkKnn, sa, st,
+                       nullptr, /*noalloc=*/true);
     CertifyArgs ca{};
     ca.X = ix.X;
     ca.Q = dQ;

@@ -10,10 +10,14 @@
 //
 // Error bound: prep.cu, with g = (d+4) u (1.01) for the fp32 FMA chains.
 //
-// Tile: 128 queries x 128 reference rows per CTA step, 16-wide k chunks staged
-// through shared memory, an 8x8 register micro-tile per thread; the finished
-// v tile is transposed through shared memory so that each of 128 threads scans
-// one query row with its own tracker.
+// Tile: 128 queries x 64 reference rows per CTA step, 16-wide k chunks staged
+// through shared memory, an 8x4 register micro-tile per thread (256 threads).
+// The finished v tile is transposed through shared memory and scanned by all
+// 256 threads: for the kNN sink two threads per query row, each with its own
+// tracker over one 32-column half of every tile (its own candidate list);
+// radius sinks keep one scanner per row so each row's columns arrive in
+// ascending order.  Trackers live in shared memory between tiles, so the
+// GEMM phase holds only the accumulators and two CTAs fit on an SM.
 #include "common.cuh"
 #include "internal.cuh"
 #include "sinks.cuh"
@@ -22,8 +26,10 @@ namespace b2k {
 
 namespace {
 
-constexpr int BM = kSimtBM, BN = kSimtBN, BK = 16, LDA = BM + 4, LDV = BN + 1;
+constexpr int BM = kSimtBM, BN = kSimtBN, BK = 16;
+constexpr int LDA = BM + 4, LDB = BN + 4, LDV = BN + 1;
 constexpr int kThreads = 256;
+static_assert(BM == 128 && BN == 64, "thread mapping below assumes a 128 x 64 tile");
 
 struct SimtParams {
   const float* Q;
@@ -37,59 +43,75 @@ struct SimtParams {
   SinkArgs sink;
 };
 
-template <class Sink>
-__global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams p) {
+template <class Sink, int HALVES>
+__host__ __device__ constexpr size_t simt_smem_bytes() {
+  return (size_t)(2 * BK * LDA + 2 * BK * LDB + BM * LDV) * sizeof(float) +
+         (size_t)BM * HALVES * sizeof(Sink);
+}
+
+// HALVES = scanners per row (2: kNN, each scans 32 columns of a tile; 1: radius).
+template <class Sink, int HALVES>
+__global__ void __launch_bounds__(kThreads, (sizeof(Sink) <= 160 ? 2 : 1))
+    screen_simt_kernel(const __grid_constant__ SimtParams p) {
   extern __shared__ float sm[];
-  float* As = sm;                    // [2][BK][LDA]
-  float* Bs = As + 2 * BK * LDA;     // [2][BK][LDA]
-  float* Vs = Bs + 2 * BK * LDA;     // [BM][LDV]
+  float* As = sm;                        // [2][BK][LDA]
+  float* Bs = As + 2 * BK * LDA;         // [2][BK][LDB]
+  float* Vs = Bs + 2 * BK * LDB;         // [BM][LDV]
+  Sink* sinks = reinterpret_cast<Sink*>(Vs + BM * LDV);  // [BM * HALVES]
 
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
+  const int tx = tid & 15, ty = tid >> 4;  // micro-tile: rows ty*8.., columns tx*4..
   const int t = blockIdx.x / p.S, s = blockIdx.x % p.S;
   const int row0 = t * BM;
   const int j0 = s * p.tiles_per_split;
   const int j1 = min(j0 + p.tiles_per_split, p.n_tiles);
 
-  Sink sink;
-  const int my_row = row0 + tid;
-  const bool scanner = tid < BM && my_row < p.m;
-  if (scanner)
-    sink.init(p.sink, my_row, s, p.E[my_row],
+  // scanner role: row r, half h
+  const int r = tid & (BM - 1), h = tid >> 7;
+  const int my_row = row0 + r;
+  const bool scanner = h < HALVES && my_row < p.m;
+  constexpr int kScanCols = BN / HALVES;
+  if (scanner) {
+    Sink sink;
+    sink.init(p.sink, my_row, s * HALVES + h, p.E[my_row],
               p.exclude_self ? (int)(p.q_offset + (p.perm ? p.perm[my_row] : my_row)) : -1);
+    sinks[tid] = sink;
+  }
 
-  // global -> register staging: thread loads 8 elements of each tile,
-  // column c = tid % 16, rows r = tid / 16 + 16 i.
+  // global -> register staging: column c = tid % 16 of the k chunk;
+  // A rows tid / 16 + 16 i (8 of them), B rows tid / 16 + 16 i (4 of them)
   const int lc = tid & 15, lr = tid >> 4;
-  float ra[8], rb[8];
-
+  float ra[8], rb[4];
   auto load_regs = [&](int k0, int col_base) {
+    const int kq = k0 + lc;
+    const bool kin = kq < p.d;
+    const float c = kin ? __ldg(p.center + kq) : 0.0f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      int r = lr + 16 * i;
-      int kq = k0 + lc;
-      int qi = row0 + r, xi = col_base + r;
-      const float c = kq < p.d ? __ldg(p.center + kq) : 0.0f;
-      ra[i] = (qi < p.m && kq < p.d) ? __ldg(p.Q + (size_t)qi * p.d + kq) - c : 0.0f;
-      rb[i] = (xi < p.n && kq < p.d) ? __ldg(p.X + (size_t)xi * p.d + kq) - c : 0.0f;
+      const int qi = row0 + lr + 16 * i;
+      ra[i] = (qi < p.m && kin) ? __ldg(p.Q + (size_t)qi * p.d + kq) - c : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int xi = col_base + lr + 16 * i;
+      rb[i] = (xi < p.n && kin) ? __ldg(p.X + (size_t)xi * p.d + kq) - c : 0.0f;
     }
   };
   auto store_regs = [&](int buf) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      As[(buf * BK + lc) * LDA + lr + 16 * i] = ra[i];
-      Bs[(buf * BK + lc) * LDA + lr + 16 * i] = rb[i];
-    }
+    for (int i = 0; i < 8; ++i) As[(buf * BK + lc) * LDA + lr + 16 * i] = ra[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) Bs[(buf * BK + lc) * LDB + lr + 16 * i] = rb[i];
   };
 
   const int nk = (p.d + BK - 1) / BK;
   for (int j = j0; j < j1; ++j) {
     const int col_base = j * BN;
-    float acc[8][8];
+    float acc[8][4];
 #pragma unroll
     for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int b = 0; b < 8; ++b) acc[a][b] = 0.0f;
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0f;
 
     load_regs(0, col_base);
     store_regs(0);
@@ -100,52 +122,67 @@ __global__ void __launch_bounds__(kThreads) screen_simt_kernel(const SimtParams 
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
         const float4* ap = reinterpret_cast<const float4*>(As + (buf * BK + kk) * LDA + ty * 8);
-        const float4* bp = reinterpret_cast<const float4*>(Bs + (buf * BK + kk) * LDA + tx * 8);
-        float4 a0 = ap[0], a1 = ap[1], b0 = bp[0], b1 = bp[1];
-        float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-        float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        const float4 b0 = *reinterpret_cast<const float4*>(Bs + (buf * BK + kk) * LDB + tx * 4);
+        const float4 a0 = ap[0], a1 = ap[1];
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+        const float bv[4] = {b0.x, b0.y, b0.z, b0.w};
 #pragma unroll
         for (int a = 0; a < 8; ++a)
 #pragma unroll
-          for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+          for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
       }
       if (kc + 1 < nk) store_regs(buf ^ 1);
       __syncthreads();
     }
     // v tile to shared memory (NaN marks columns past n: never admitted)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int col = col_base + tx * 8 + b;
+    for (int b = 0; b < 4; ++b) {
+      const int col = col_base + tx * 4 + b;
       const float nxv = col < p.n ? __ldg(p.nx + col) : __int_as_float(0x7fc00000);
 #pragma unroll
-      for (int a = 0; a < 8; ++a) Vs[(ty * 8 + a) * LDV + tx * 8 + b] = fmaf(-2.0f, acc[a][b], nxv);
+      for (int a = 0; a < 8; ++a) Vs[(ty * 8 + a) * LDV + tx * 4 + b] = fmaf(-2.0f, acc[a][b], nxv);
     }
     __syncthreads();
     if (scanner) {
+      Sink sink = sinks[tid];
       sink.tile_sync();
-      const float* vr = Vs + tid * LDV;
-#pragma unroll 4
-      for (int c = 0; c < BN; ++c) {
-        sink.offer1(vr[c], col_base + c);
+      float* vr = Vs + r * LDV + h * kScanCols;
+#pragma unroll
+      for (int c0 = 0; c0 < kScanCols; c0 += 32) {
+        float v[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = vr[c0 + i];
+        // the slow path may overwrite vr[c0 .. c0+8): those values are in v[]
+        sink.offer32(v, col_base + h * kScanCols + c0, vr + c0);
       }
+      sinks[tid] = sink;
     }
     __syncthreads();
   }
-  if (scanner) sink.finish(p.sink);
+  if (scanner) {
+    Sink sink = sinks[tid];
+    sink.tile_sync();
+    sink.finish(p.sink);
+  }
 }
 
-template <class Sink>
-void launch_simt_variant(const SimtParams& p, int grid, size_t smem, cudaStream_t st) {
-  cudaFuncSetAttribute(screen_simt_kernel<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
-  screen_simt_kernel<Sink><<<grid, kThreads, smem, st>>>(p);
+template <class Sink, int HALVES>
+void launch_simt_variant(const SimtParams& p, int grid, cudaStream_t st) {
+  constexpr size_t smem = simt_smem_bytes<Sink, HALVES>();
+  cudaFuncSetAttribute(screen_simt_kernel<Sink, HALVES>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  screen_simt_kernel<Sink, HALVES><<<grid, kThreads, smem, st>>>(p);
 }
 
 }  // namespace
 
+int simt_column_groups(int sink_kind, bool noalloc) {
+  return (sink_kind == kSinkKnn && !noalloc) ? 2 : 1;
+}
+
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,
                         int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                        const SinkArgs& sa, cudaStream_t st, const int* perm) {
+                        const SinkArgs& sa, cudaStream_t st, const int* perm, bool noalloc) {
   SimtParams p{};
   p.Q = Q;
   p.X = ix->X;
@@ -163,14 +200,18 @@ void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pa
   p.perm = perm;
   p.sink = sa;
   const int m_tiles = (int)(m_pad / BM);
-  const size_t smem = (size_t)(4 * BK * LDA + BM * LDV) * sizeof(float);
   const int grid = m_tiles * S;
   if (grid <= 0) return;
-  if (sink_kind == kSinkRadiusCount) return launch_simt_variant<RadiusCountSink>(p, grid, smem, st);
-  if (sink_kind == kSinkRadiusFill) return launch_simt_variant<RadiusFillSink>(p, grid, smem, st);
-  if (sa.k <= 16) return launch_simt_variant<KnnSink<16>>(p, grid, smem, st);
-  if (sa.k <= 32) return launch_simt_variant<KnnSink<32>>(p, grid, smem, st);
-  launch_simt_variant<KnnSink<64>>(p, grid, smem, st);
+  if (sink_kind == kSinkRadiusCount) return launch_simt_variant<RadiusCountSink, 1>(p, grid, st);
+  if (sink_kind == kSinkRadiusFill) return launch_simt_variant<RadiusFillSink, 1>(p, grid, st);
+  if (simt_column_groups(sink_kind, noalloc) == 1) {
+    if (sa.k <= 16) return launch_simt_variant<KnnSink<16>, 1>(p, grid, st);
+    if (sa.k <= 32) return launch_simt_variant<KnnSink<32>, 1>(p, grid, st);
+    return launch_simt_variant<KnnSink<64>, 1>(p, grid, st);
+  }
+  if (sa.k <= 16) return launch_simt_variant<KnnSink<16>, 2>(p, grid, st);
+  if (sa.k <= 32) return launch_simt_variant<KnnSink<32>, 2>(p, grid, st);
+  launch_simt_variant<KnnSink<64>, 2>(p, grid, st);
 }
 
 }  // namespace b2k

@@ -75,3 +75,19 @@ def cfg4(seed=5, problems=256, n_range=(1_000, 200_000), m_range=(100, 20_000),
         Q = rng.standard_normal((m, d)).astype(np.float32)
         out.append((X, Q, min(k, n)))
     return out
+
+
+def cfg5(seed=6, pairs=64, points=8192, self_n=4096, self_d=64):
+    """Point clouds for the differentiable kNN losses: `pairs` pairs of
+    `points` x 3 clouds uniform on the unit sphere plus N(0, 0.01^2) noise,
+    and one self_n x self_d N(0,1) matrix (self k-NN)."""
+    rng = np.random.default_rng(seed)
+
+    def cloud():
+        v = rng.standard_normal((points, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        return (v + 0.01 * rng.standard_normal((points, 3))).astype(np.float32)
+
+    clouds = [(cloud(), cloud()) for _ in range(pairs)]
+    S = rng.standard_normal((self_n, self_d)).astype(np.float32)
+    return clouds, S
