@@ -186,48 +186,67 @@ __device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* his
 // non-negative terms, each (fl(q_i - x_i))^2 accumulated with FMA: the result
 // is within (d + 5) u (1.01) S + d 2^-126 of the exact S, u = 2^-24, whatever
 // the order of the additions.
+// Vectorised form for d <= 32 NI (16-byte aligned rows): the query's pieces
+// stay in registers, and each 8-lane group loads UNR candidate rows before
+// using any of them, so a warp keeps 4 UNR rows of loads in flight.
+template <int NI, int UNR>
+__device__ __forceinline__ void refine_vec(const float* __restrict__ q,
+                                           const float* __restrict__ X, int d, const int* ci,
+                                           float* cv, int C, int lane) {
+  const int grp = lane >> 3, l8 = lane & 7;
+  const int d4 = d / 4;
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  float4 qr[NI];
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    const int f = l8 + 8 * i;
+    qr[i] = f < d4 ? __ldg(q4 + f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (int c0 = 0; c0 < C; c0 += 4 * UNR) {
+    float4 b[UNR][NI];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int c = c0 + 4 * u + grp;
+      const float4* x4 =
+          reinterpret_cast<const float4*>(X + (size_t)(c < C ? ci[c] : ci[0]) * d);
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        const int f = l8 + 8 * i;
+        b[u][i] = (c < C && f < d4) ? __ldg(x4 + f) : qr[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      float acc0 = 0.f, acc1 = 0.f;
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        const float e0 = qr[i].x - b[u][i].x, e1 = qr[i].y - b[u][i].y;
+        const float e2 = qr[i].z - b[u][i].z, e3 = qr[i].w - b[u][i].w;
+        acc0 = fmaf(e0, e0, acc0);
+        acc1 = fmaf(e1, e1, acc1);
+        acc0 = fmaf(e2, e2, acc0);
+        acc1 = fmaf(e3, e3, acc1);
+      }
+      float acc = acc0 + acc1;
+      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      const int c = c0 + 4 * u + grp;
+      if (l8 == 0 && c < C) cv[c] = acc;
+    }
+  }
+}
+
 __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
                                             const float* __restrict__ X, int d, const int* ci,
                                             float* cv, int C, int lane) {
   const int grp = lane >> 3, l8 = lane & 7;
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(q) & 15) == 0 &&
                    (reinterpret_cast<uintptr_t>(X) & 15) == 0;
-  if (vec && d <= 256) {
-    // the query's 16-byte pieces this lane needs stay in registers
-    const int d4 = d / 4;
-    const float4* q4 = reinterpret_cast<const float4*>(q);
-    float4 qr[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int f = l8 + 8 * i;
-      qr[i] = f < d4 ? __ldg(q4 + f) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for (int c0 = 0; c0 < C; c0 += 4) {
-      const int c = c0 + grp;
-      float acc0 = 0.f, acc1 = 0.f;
-      if (c < C) {
-        const float4* x4 = reinterpret_cast<const float4*>(X + (size_t)ci[c] * d);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int f = l8 + 8 * i;
-          if (f < d4) {
-            const float4 b = __ldg(x4 + f);
-            const float e0 = qr[i].x - b.x, e1 = qr[i].y - b.y;
-            const float e2 = qr[i].z - b.z, e3 = qr[i].w - b.w;
-            acc0 = fmaf(e0, e0, acc0);
-            acc1 = fmaf(e1, e1, acc1);
-            acc0 = fmaf(e2, e2, acc0);
-            acc1 = fmaf(e3, e3, acc1);
-          }
-        }
-      }
-      float acc = acc0 + acc1;
-      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-      if (l8 == 0 && c < C) cv[c] = acc;
-    }
-    return;
+  if (vec && C > 0) {
+    if (d <= 64) return refine_vec<2, 4>(q, X, d, ci, cv, C, lane);
+    if (d <= 128) return refine_vec<4, 2>(q, X, d, ci, cv, C, lane);
+    if (d <= 256) return refine_vec<8, 1>(q, X, d, ci, cv, C, lane);
   }
   for (int c0 = 0; c0 < C; c0 += 4) {
     const int c = c0 + grp;
