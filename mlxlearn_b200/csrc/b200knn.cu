@@ -383,8 +383,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
       CUtensorMap tmap_a;
       if (!tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
         return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
+      // status[6] (zeroed above) counts the claimed work units
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
-                                kSinkKnn, sa, status, st, perm);
+                                kSinkKnn, sa, status, st, perm, status + 6);
       if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
                           cudaGetErrorString((cudaError_t)lr));
     } else {

@@ -106,7 +106,7 @@ struct SinkArgs;
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st,
-                     const int* perm = nullptr);
+                     const int* perm = nullptr, int* unit_counter = nullptr);
 int tc_column_groups(int k);
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
 // noalloc: one scanner per row (half the list memory of the default two)

@@ -18,23 +18,28 @@
 //   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16, fp32
 //               accumulators in TMEM, double-buffered (2 x 256 columns).
 //   warps 2..   EW epilogue warps.  Warp w reads TMEM lane group w % 4 (the
-//               hardware's rule); with EW = 8 the two warps of a lane group
-//               take the two 128-column halves of each tile.  Per 32-column
+//               hardware's rule); the EW / 4 warps of a lane group take
+//               equal column ranges of each tile (16 warps for k <= 16, 8 for
+//               the lazy tracker).  Per 32-column
 //               chunk: tcgen05.ld (two loads in flight), 3-input min over
 //               8-column groups, and only when a group passes the row's
 //               threshold, admit its columns (sinks.cuh).  The accumulator is
 //               handed back to the MMA warp as soon as its last chunk is in
 //               registers.  The distance tile never reaches HBM.
 // A work unit is (query tile of 128 rows, split s of the reference tiles);
-// units are dealt round-robin over the persistent CTAs in split-major order,
-// so the CTAs of a wave stream the same reference range (it stays in L2) and
-// later splits start from the k-th values the earlier ones published.
-// Candidate lists are kept per (split, column half, row).
+// units are numbered split-major and claimed in order by the persistent CTAs
+// (an atomic counter, broadcast to the CTA's warps through a shared-memory
+// ring), so the CTAs of a wave stream the same reference range (it stays in
+// L2), later splits start from the k-th values the earlier ones published,
+// and CTAs whose tiles run slow take fewer units.  Candidate lists are kept
+// per (split, column group, row).
 //
 // Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
 // B = bf16(x - c)); the certified error bound of v is derived in prep.cu with
 // g = (dp + 32) 2^-20 for the tensor-core fp32 accumulation.
 #include <cuda_bf16.h>
+
+#include <cstdlib>
 
 #include "common.cuh"
 #include "internal.cuh"
@@ -53,6 +58,7 @@ struct TcParams {
   const int4* items;         // batched: (problem, query tile, first tile, end tile)
   const int* cta_begin;      // batched: CTA b runs items [cta_begin[b], cta_begin[b + 1])
   int* status;
+  int* unit_counter;         // single problem: units claimed dynamically (or null: round-robin)
   TcProblem one;             // single problem
 };
 
@@ -69,11 +75,31 @@ struct TcUnit {
   int t, j0, j1, slot;
 };
 
+// Dynamically claimed units are broadcast by the producer thread through a
+// small ring in shared memory (index -1: no units left).
+constexpr int kUnitRing = 4;
+struct UnitRing {
+  int* idx;          // [kUnitRing]
+  uint64_t* full;    // [kUnitRing] producer -> consumers
+  uint64_t* empty;   // [kUnitRing] consumers (MMA thread + epilogue threads) -> producer
+};
+
 // The sequence of work units of this CTA; every warp role walks it in step.
+// Batched launches read host-balanced per-CTA lists; a single problem either
+// deals units round-robin or, with a unit counter, lets the producer claim
+// the next unit when it starts one, so CTAs whose tiles run slow take fewer.
 template <bool BATCH>
 struct UnitCursor {
   int u, end, step;
-  B2K_DEV UnitCursor(const TcParams& p) {
+  bool dyn, producer;
+  UnitRing ring;
+  uint32_t rs, rph;
+  B2K_DEV UnitCursor(const TcParams& p, const UnitRing& r, bool is_producer) {
+    dyn = !BATCH && p.unit_counter != nullptr;
+    producer = is_producer;
+    ring = r;
+    rs = 0;
+    rph = 0;
     if (BATCH) {
       u = p.cta_begin[blockIdx.x];
       end = p.cta_begin[blockIdx.x + 1];
@@ -84,27 +110,59 @@ struct UnitCursor {
       step = gridDim.x;
     }
   }
+  // Next unit index, -1 when done; false also when a bounded wait gave up.
+  B2K_DEV bool claim(const TcParams& p, int* v) {
+    if (!dyn) {
+      if (u >= end) return false;
+      *v = u;
+      u += step;
+      return true;
+    }
+    bool ok;
+    if (producer) {
+      int w = atomicAdd(p.unit_counter, 1);
+      if (w >= end) w = -1;
+      ok = mbar_wait(&ring.empty[rs], rph ^ 1, p.status, DEV_TIMEOUT_A);
+      if (ok) {
+        ring.idx[rs] = w;
+        mbar_arrive(&ring.full[rs]);
+      }
+      *v = w;
+    } else {
+      ok = mbar_wait(&ring.full[rs], rph, p.status, DEV_TIMEOUT_A);
+      if (ok) {
+        *v = *reinterpret_cast<volatile int*>(&ring.idx[rs]);
+        mbar_arrive(&ring.empty[rs]);
+      }
+    }
+    if (++rs == (uint32_t)kUnitRing) {
+      rs = 0;
+      rph ^= 1;
+    }
+    return ok && *v >= 0;
+  }
   B2K_DEV bool next(const TcParams& p, TcUnit& x) {
-    if (u >= end) return false;
+    int w;
+    if (!claim(p, &w)) return false;
     if (BATCH) {
-      const int4 it = p.items[u];
+      const int4 it = p.items[w];
       x.pr = p.probs + it.x;
       x.t = it.y;
       x.j0 = it.z;
       x.j1 = it.w;
       x.slot = it.z / x.pr->tiles_per_split;
     } else {
-      const int s = u / p.m_tiles;
+      const int s = w / p.m_tiles;
       x.pr = &p.one;
-      x.t = u % p.m_tiles;
+      x.t = w % p.m_tiles;
       x.j0 = s * p.one.tiles_per_split;
       x.j1 = min(x.j0 + p.one.tiles_per_split, p.one.n_tiles);
       x.slot = s;
     }
-    u += step;
     return true;
   }
-  B2K_DEV bool more() const { return u < end; }
+  // Whether another unit follows (always assumed when units are claimed).
+  B2K_DEV bool more() const { return dyn || u < end; }
 };
 
 constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;     // 16 KB per 64-column block
@@ -123,7 +181,8 @@ __host__ __device__ inline uint32_t tc_stage_bytes(bool a_stream) {
 __host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream, int ew) {
   size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
   size_t spill = (size_t)ew * 32 * kSpillStride * sizeof(float);
-  size_t bars = (2 * (size_t)stages + 7) * sizeof(uint64_t) + 16;
+  size_t bars = (2 * (size_t)stages + 7 + 2 * kUnitRing) * sizeof(uint64_t) + 16 +
+                kUnitRing * sizeof(int);
   return 1024 /*alignment slack*/ + kAAugBytes + a + (size_t)tc_stage_bytes(a_stream) * stages +
          spill + bars;
 }
@@ -168,7 +227,11 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
   uint64_t* acc_full = a_empty + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2; // [2]
   uint64_t* aaug_full = acc_empty + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(aaug_full + 1);
+  UnitRing ring;
+  ring.full = aaug_full + 1;           // [kUnitRing]
+  ring.empty = ring.full + kUnitRing;  // [kUnitRing]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ring.empty + kUnitRing);
+  ring.idx = reinterpret_cast<int*>(tmem_slot + 4);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -186,6 +249,10 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     mbar_init(&acc_empty[0], kEpiThreads);
     mbar_init(&acc_empty[1], kEpiThreads);
     mbar_init(aaug_full, 1);
+    for (int r = 0; r < kUnitRing; ++r) {
+      mbar_init(&ring.full[r], 1);
+      mbar_init(&ring.empty[r], 1 + kEpiThreads);
+    }
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -211,7 +278,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       mbar_arrive_expect_tx(aaug_full, kAAugBytes);
       tma_load_2d(aaug_smem, &maps.aaug, aaug_full, 0, 0);
       uint32_t stage = 0, phase = 0, a_phase = 0;
-      UnitCursor<BATCH> cur(p);
+      UnitCursor<BATCH> cur(p, ring, true);
       TcUnit x;
       while (cur.next(p, x)) {
         const int KB = x.pr->KB;
@@ -256,6 +323,9 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
         }
       }
       mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A);
+      // with claimed units the MMA warp releases the query tile after every
+      // unit: take the last release so no arrival lands after the CTA exits
+      if (!A_STREAM && cur.dyn) mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A);
     prod_done:;
     }
   } else if (warp == 1) {
@@ -266,7 +336,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto mma_done;
       {
         const uint64_t aaug_desc = smem_desc_sw32(aaug_smem);
-        UnitCursor<BATCH> cur(p);
+        UnitCursor<BATCH> cur(p, ring, false);
         TcUnit x;
         while (cur.next(p, x)) {
           const int KB = x.pr->KB;
@@ -319,9 +389,11 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     const int et = threadIdx.x - 64;        // 0 .. kEpiThreads-1
     float* spill = spill_all + et * kSpillStride;
     uint32_t acc_it = 0;
-    UnitCursor<BATCH> cur(p);
+    UnitCursor<BATCH> cur(p, ring, false);
     TcUnit x;
-    while (cur.next(p, x)) {
+    for (;;) {
+      // warp-uniform: a bounded wait that gave up in one lane ends the warp
+      if (!__all_sync(0xffffffffu, cur.next(p, x))) break;
       const TcProblem& pr = *x.pr;
       const int row = x.t * kTcBM + row_in_tile;
       const bool valid = row < pr.m;
@@ -339,9 +411,12 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
         sink.init(pr.sink, row, x.slot * kHalves + half, pr.E[row],
                   pr.exclude_self ? (int)(pr.q_offset + orig) : -1);
       }
+      uint32_t pending_key = kNoKey;
       for (int j = x.j0; j < x.j1; ++j) {
         // the other warps' k-th values for this query: consumed after the tile
-        const uint32_t shared_key = live ? sink.tile_fetch() : 0u;
+        // the load issued one tile earlier is consumed at the end of this one
+        const uint32_t shared_key = pending_key;
+        pending_key = live ? sink.tile_fetch() : 0u;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
         // warp-uniform outcome, so collective sinks never run on a partial warp
         if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)))
@@ -354,6 +429,21 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
           for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
           if (live) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
         };
+        if constexpr (EW == 16) {
+          // four warps per lane group: one 32-column buffer each (register budget);
+          // the other warps of the SM cover the load latency
+#pragma unroll 1
+          for (int c = 0; c < kChunks; ++c) {
+            uint32_t ra[32];
+            tmem_ld_32x32b_x32(tbase + c * 32, ra);
+            tmem_ld_wait_regs(ra);
+            if (c == kChunks - 1) {
+              tc_fence_before();
+              mbar_arrive(&acc_empty[buf]);
+            }
+            process(ra, c);
+          }
+        } else {
         // Two 32-column TMEM loads in flight: load chunk c+1 while chunk c is scanned.
         uint32_t ra[32], rb[32];
         tmem_ld_32x32b_x32(tbase, ra);
@@ -373,6 +463,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
             mbar_arrive(&acc_empty[buf]);
             process(rb, c + 1);
           }
+        }
         }
         ++acc_it;
         if (live) sink.tile_apply(shared_key);
@@ -433,13 +524,27 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
 
 // Column groups (epilogue warps per TMEM lane group) of the kNN screen for k:
 // each group keeps its own candidate lists.
-int tc_column_groups(int k) { return k > 0 ? 2 : 1; }
+// Epilogue warps of the single-problem kNN screen: four per TMEM lane group
+// for the register-heap trackers (k <= 16), which shortens each warp's
+// per-tile chain and cuts the MMA warp's waits for a free accumulator
+// (B2K_TC_EW=8 selects two); two for the lazy tracker.
+static int tc_knn_ew(int k) {
+  if (k > 16) return 8;
+  static const int ew = [] {
+    const char* e = getenv("B2K_TC_EW");
+    return (e && atoi(e) == 8) ? 8 : 16;
+  }();
+  return ew;
+}
+int tc_column_groups(int k) { return tc_knn_ew(k) / 4; }
 bool tc_lazy_sink(int k) { return k > 16; }
 
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
-                     const SinkArgs& sa, int* status, cudaStream_t st, const int* perm) {
+                     const SinkArgs& sa, int* status, cudaStream_t st, const int* perm,
+                     int* unit_counter) {
   TcParams p{};
+  p.unit_counter = unit_counter;
   TcProblem& one = p.one;
   one.m = (int)m;
   one.KB = ix->dp / kTcBK;
@@ -468,6 +573,11 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
             : launch_tc_variant<SINK, false, EW, false>(maps, p, KB, grid, st))
   if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, 4);
   if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
+  if (tc_knn_ew(sa.k) == 16) {
+    if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 16);
+    if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 16);
+    return B2K_TC_LAUNCH(KnnSink<16>, 16);
+  }
   if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 8);
   if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 8);
   if (!tc_lazy_sink(sa.k)) return B2K_TC_LAUNCH(KnnSink<16>, 8);
