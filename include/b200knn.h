@@ -149,6 +149,22 @@ B2K_API int b2k_knn_backward(const float *dQ, int64_t m, const float *dX, int64_
                              const float *d_dist, int32_t squared, float *d_grad_q,
                              float *d_grad_x, void *stream);
 
+/* Exact kNN for many small problems given as segments of two device
+ * arrays, in one call: problem p asks, for every query row in
+ * [q_offsets[p], q_offsets[p+1]) of dQ float32[rows, d], for its k nearest
+ * reference rows in [x_offsets[p], x_offsets[p+1]) of dX float32[*, d].
+ * Offsets are HOST int64[segments + 1] starting at 0.  Writes d_idx
+ * int64[rows, k] (indices within the reference segment) and d_dist
+ * float64[rows, k] (or NULL), same order and tie rule as b2k_knn_device.
+ * exclude_self: every query segment is its reference segment and row i skips
+ * itself.  1 <= d <= 16, k <= 29.  Enqueued on `stream`; the call
+ * synchronises it.  No counterpart in the reference (one problem per
+ * NeighborIndex.query call, src/mlxlearn/_kernels/distance.py:242-270); it
+ * backs the batched Chamfer loss of mlxlearn_b200/autograd.py. */
+B2K_API int b2k_knn_segments(const float *dQ, const float *dX, int32_t d, const int64_t *q_offsets,
+                             const int64_t *x_offsets, int32_t segments, int32_t k,
+                             int32_t exclude_self, double *d_dist, int64_t *d_idx, void *stream);
+
 /* Class votes of kNN results on the device (all pointers device, on
  * `stream`; the call synchronises).  codes int32[n_train] are class codes
  * 0..n_classes-1; votes float64[m, n_classes] receives per-class totals (1 or

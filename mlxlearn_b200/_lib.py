@@ -101,6 +101,8 @@ SIGNATURES = {
                                               _vp]),
     "b2k_knn_backward": (ctypes.c_int, [_vp, _i64, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _i32,
                                         _vp, _vp, _vp]),
+    "b2k_knn_segments": (ctypes.c_int, [_vp, _vp, _i32, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
+                                        _vp]),
     "b2k_class_votes": (ctypes.c_int, [_vp, _vp, _i64, _i32, _vp, _i32, _i32, _vp, _vp, _vp]),
     "b2k_radius": (ctypes.c_int, [_vp, _vp, _i64, _dbl, _i32, _i64, _i32, _i32,
                                   ctypes.POINTER(_vp)]),

@@ -244,9 +244,9 @@ __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(q) & 15) == 0 &&
                    (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   if (vec && C > 0) {
-    if (d <= 64) return refine_vec<2, 4>(q, X, d, ci, cv, C, lane);
-    if (d <= 128) return refine_vec<4, 2>(q, X, d, ci, cv, C, lane);
-    if (d <= 256) return refine_vec<8, 1>(q, X, d, ci, cv, C, lane);
+    if (d <= 64) return refine_vec<2, 8>(q, X, d, ci, cv, C, lane);
+    if (d <= 128) return refine_vec<4, 4>(q, X, d, ci, cv, C, lane);
+    if (d <= 256) return refine_vec<8, 2>(q, X, d, ci, cv, C, lane);
   }
   for (int c0 = 0; c0 < C; c0 += 4) {
     const int c = c0 + grp;
