@@ -498,14 +498,21 @@ int index_prepare_bf16_stats(Index& ix, uint16_t* Xh, uint16_t* Xaug, uint16_t* 
   return B2K_OK;
 }
 
-static bool host_finite(const float* v, size_t count) {
-  for (size_t i = 0; i < count; ++i) {
-    uint32_t b;
-    memcpy(&b, v + i, 4);
-    if ((b & 0x7f800000u) == 0x7f800000u) return false;
-  }
-  return true;
+// Whether count device floats are all finite (one pass on the device).
+static int device_finite(const float* dv, size_t count, cudaStream_t st, bool* ok) {
+  int* flag = nullptr;
+  int rc = dalloc(&flag, 1, st);
+  if (rc) return rc;
+  int h = 0;
+  cudaMemsetAsync(flag, 0, sizeof(int), st);
+  launch_nonfinite_check(dv, (int64_t)count, flag, st);
+  cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(flag, st);
+  B2K_CUDA(cudaStreamSynchronize(st));
+  *ok = h == 0;
+  return B2K_OK;
 }
+
 
 }  // namespace b2k
 
@@ -567,13 +574,14 @@ int b2k_index_create(const float* X, int64_t n, int32_t d, int32_t device, b2k_i
   int rc = create_common(device, n, d, out);
   if (rc) return rc;
   if (!X) return fail(B2K_EINVAL, "X must not be NULL");
-  if (!host_finite(X, (size_t)n * d))
-    return fail(B2K_ENONFINITE, "training coordinates must be finite");
   auto* h = new b2k_index();
   h->ix.device = device;
   h->ix.n = n;
   h->ix.d = d;
   rc = build_from_device(h, X, cudaMemcpyHostToDevice, nullptr);
+  bool ok = true;
+  if (!rc) rc = device_finite(h->ix.X, (size_t)n * d, h->ix.stream, &ok);
+  if (!rc && !ok) rc = fail(B2K_ENONFINITE, "training coordinates must be finite");
   if (rc) {
     b2k_index_destroy(h);
     return rc;
@@ -596,6 +604,9 @@ int b2k_index_create_device(const float* dX, int64_t n, int32_t d, void* stream,
   h->ix.n = n;
   h->ix.d = d;
   rc = build_from_device(h, dX, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  bool ok = true;
+  if (!rc) rc = device_finite(h->ix.X, (size_t)n * d, h->ix.stream, &ok);
+  if (!rc && !ok) rc = fail(B2K_ENONFINITE, "training coordinates must be finite");
   if (rc) {
     b2k_index_destroy(h);
     return rc;
@@ -669,8 +680,6 @@ int b2k_knn(b2k_index* h, const float* Q, int64_t m, int32_t k, int32_t exclude_
     return B2K_OK;
   }
   if (!Q || !idx) return fail(B2K_EINVAL, "queries and indices must not be NULL");
-  if (!host_finite(Q, (size_t)m * ix.d))
-    return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
   cudaSetDevice(ix.device);
   cudaStream_t st = ix.stream;
   float* dQ = nullptr;
@@ -686,6 +695,10 @@ int b2k_knn(b2k_index* h, const float* Q, int64_t m, int32_t k, int32_t exclude_
     fr.keep(dd);
   }
   B2K_CUDA(cudaMemcpyAsync(dQ, Q, (size_t)m * ix.d * sizeof(float), cudaMemcpyHostToDevice, st));
+  // finiteness checked on the device after the upload (one pass over HBM)
+  bool finite = true;
+  if ((rc = device_finite(dQ, (size_t)m * ix.d, st, &finite))) return rc;
+  if (!finite) return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
   rc = knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, mode, dd, di, st, stats);
   if (rc) return rc;
   B2K_CUDA(cudaMemcpyAsync(idx, di, (size_t)m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -890,8 +903,6 @@ int b2k_radius(b2k_index* h, const float* Q, int64_t m, double radius, int32_t e
                 "query rows at offset %lld and %lld training rows.",
                 (long long)m, (long long)q_offset, (long long)ix.n);
   if (m > 0 && !Q) return fail(B2K_EINVAL, "queries must not be NULL");
-  if (!host_finite(Q, (size_t)m * ix.d))
-    return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
   if (fault_mode() == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
   const double R2 = radius * radius;
   cudaSetDevice(ix.device);
@@ -915,6 +926,14 @@ int b2k_radius(b2k_index* h, const float* Q, int64_t m, double radius, int32_t e
     return rc;
   }
   cudaMemcpyAsync(dQ, Q, (size_t)m * ix.d * sizeof(float), cudaMemcpyHostToDevice, st);
+  bool finite = true;
+  rc = device_finite(dQ, (size_t)m * ix.d, st, &finite);
+  if (!rc && !finite) rc = fail(B2K_ENONFINITE, "training and query coordinates must be finite");
+  if (rc) {
+    cudaFreeAsync(dQ, st);
+    delete res;
+    return rc;
+  }
   rc = radius_block(ix, dQ, m, R2, exclude_self, q_offset, need_distance != 0,
                     sort_results != 0, !ix.range_ok, st, res);
   cudaFreeAsync(dQ, st);

@@ -68,6 +68,8 @@ struct Index {
 
 // ------------------------------------------------------------ prep kernels
 void launch_prep_index(Index* ix, cudaStream_t st);
+// flag |= 1 when some value is NaN or infinite
+void launch_nonfinite_check(const float* v, int64_t count, int* flag, cudaStream_t st);
 // bf16 operand rows [n_pad, dp] (n_pad = n rounded up to 256) into Xh; the
 // operand statistics go to the index's stats_dev [3], [4].
 void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st);

@@ -23,6 +23,8 @@
 //   g = (dp + 16) 2^-20           tcgen05 fp32 accumulation (16 ulp per add).
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -241,7 +243,36 @@ __global__ void prep_queries_batch_kernel(const PrepProblem* __restrict__ tab,
   prep_query_row(tab[p], r - row_start[p], threadIdx.x & 31);
 }
 
+__global__ void nonfinite_kernel(const float* __restrict__ v, int64_t count, int* flag) {
+  bool bad = false;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((reinterpret_cast<uintptr_t>(v) & 15) == 0) {
+    const int64_t n4 = count / 4;
+    const float4* v4 = reinterpret_cast<const float4*>(v);
+    for (int64_t i = i0; i < n4; i += stride) {
+      const float4 x = __ldg(v4 + i);
+      bad |= ((__float_as_uint(x.x) & 0x7f800000u) == 0x7f800000u) |
+             ((__float_as_uint(x.y) & 0x7f800000u) == 0x7f800000u) |
+             ((__float_as_uint(x.z) & 0x7f800000u) == 0x7f800000u) |
+             ((__float_as_uint(x.w) & 0x7f800000u) == 0x7f800000u);
+    }
+    for (int64_t i = 4 * n4 + i0; i < count; i += stride)
+      bad |= (__float_as_uint(v[i]) & 0x7f800000u) == 0x7f800000u;
+  } else {
+    for (int64_t i = i0; i < count; i += stride)
+      bad |= (__float_as_uint(v[i]) & 0x7f800000u) == 0x7f800000u;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 }  // namespace
+
+void launch_nonfinite_check(const float* v, int64_t count, int* flag, cudaStream_t st) {
+  if (count <= 0) return;
+  const int64_t blocks = std::min<int64_t>((count / 4 + 255) / 256 + 1, 4096);
+  nonfinite_kernel<<<(unsigned)blocks, 256, 0, st>>>(v, count, flag);
+}
 
 void launch_prep_index(Index* ix, cudaStream_t st) {
   const int64_t rows_per_block = 2048;

@@ -237,3 +237,24 @@ def test_full_lists_are_compacted_not_rescanned(mode):
     np.testing.assert_array_equal(idx, oi)
     np.testing.assert_array_equal(dist, od)
     assert ix.last_stats["fallback_rows"] == 0
+
+
+def test_non_finite_inputs_are_rejected():
+    # checked on the device after the upload: NaN / inf in the training rows
+    # or the queries raise ValueError, and the index stays usable
+    rng = np.random.default_rng(23)
+    X = rng.standard_normal((3000, 32)).astype(np.float32)
+    bad = X.copy()
+    bad[1234, 5] = np.inf
+    with pytest.raises(ValueError, match="finite"):
+        make_index(bad).query(X[:4], 3)
+    ix = make_index(X)
+    Q = X[:50].copy()
+    Q[17, 3] = np.nan
+    with pytest.raises(ValueError, match="finite"):
+        ix.query(Q, 3)
+    with pytest.raises(ValueError, match="finite"):
+        ix.query_radius_csr(Q, 1.0)
+    od, oi = oracle.knn(X, X[:50], 3)
+    dist, idx = ix.query(X[:50], 3)
+    np.testing.assert_array_equal(idx, oi)
