@@ -605,8 +605,9 @@ def run_chamfer(args):
     torch.cuda.set_device(0)
     threads = os.cpu_count() or 1
     clouds, S = cfg5()
-    A = [torch.from_numpy(a).cuda().requires_grad_() for a, _ in clouds]
-    B = [torch.from_numpy(b).cuda().requires_grad_() for _, b in clouds]
+    # the 64 pairs as two [64, 8192, 3] tensors
+    A = torch.from_numpy(np.stack([a for a, _ in clouds])).cuda().requires_grad_()
+    B = torch.from_numpy(np.stack([b for _, b in clouds])).cuda().requires_grad_()
     Sd = torch.from_numpy(S).cuda().requires_grad_()
     pairs = sum(2 * a.shape[0] * b.shape[0] for a, b in clouds) + S.shape[0] * S.shape[0]
 

@@ -155,12 +155,24 @@ def knn_segments(Q, X, q_sizes, x_sizes, k=1, *, exclude_self=False, squared=Fal
 
 def chamfer_loss_batch(As, Bs):
     """Sum over pairs of the symmetric k=1 Chamfer term of ``chamfer_loss``,
-    with one search and one backward call for all pairs (clouds of d <= 16)."""
-    if len(As) != len(Bs):
-        raise ValueError("As and Bs must hold the same number of clouds")
-    Q = torch.cat([t for a, b in zip(As, Bs) for t in (a, b)])
-    X = torch.cat([t for a, b in zip(As, Bs) for t in (b, a)])
-    q_sizes = [t.shape[0] for a, b in zip(As, Bs) for t in (a, b)]
-    x_sizes = [t.shape[0] for a, b in zip(As, Bs) for t in (b, a)]
+    with one search and one backward call for all pairs (clouds of d <= 16).
+    ``As`` and ``Bs`` are lists of ``[n_i, d]`` tensors, or two ``[P, n, d]``
+    tensors of equally sized clouds (cheaper: no per-cloud gradient tensors)."""
+    if torch.is_tensor(As) and torch.is_tensor(Bs) and As.dim() == 3 and Bs.dim() == 3:
+        P, na, d = As.shape
+        nb = Bs.shape[1]
+        if Bs.shape[0] != P or Bs.shape[2] != d:
+            raise ValueError("As and Bs must hold the same number of clouds of one width")
+        Q = torch.cat([As, Bs], dim=1).reshape(-1, d)
+        X = torch.cat([Bs, As], dim=1).reshape(-1, d)
+        q_sizes = [na, nb] * P
+        x_sizes = [nb, na] * P
+    else:
+        if len(As) != len(Bs):
+            raise ValueError("As and Bs must hold the same number of clouds")
+        Q = torch.cat([t for a, b in zip(As, Bs) for t in (a, b)])
+        X = torch.cat([t for a, b in zip(As, Bs) for t in (b, a)])
+        q_sizes = [t.shape[0] for a, b in zip(As, Bs) for t in (a, b)]
+        x_sizes = [t.shape[0] for a, b in zip(As, Bs) for t in (b, a)]
     d2, _ = knn_segments(Q, X, q_sizes, x_sizes, 1, squared=True)
     return d2.sum()

@@ -275,7 +275,8 @@ void launch_nonfinite_check(const float* v, int64_t count, int* flag, cudaStream
 }
 
 void launch_prep_index(Index* ix, cudaStream_t st) {
-  const int64_t rows_per_block = 2048;
+  // about eight blocks per SM, at least 16 rows each
+  const int64_t rows_per_block = std::max<int64_t>(16, (ix->n + 1183) / 1184);
   const int64_t blocks = (ix->n + rows_per_block - 1) / rows_per_block;
   cudaMemsetAsync(ix->colsum, 0, (size_t)ix->d * sizeof(double), st);
   column_sum_kernel<<<(unsigned)blocks, 128, 0, st>>>(ix->X, ix->n, ix->d, rows_per_block,

@@ -62,7 +62,9 @@ __global__ void seg_range_kernel(const float* __restrict__ v, int64_t count, int
   if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicOr(flags + 1, 1);
 }
 
-template <int D, int KS>
+// D: padded width (4, 8 or 16) of the shared-memory rows; DC: coordinates
+// actually computed (D, or 3 for three-dimensional points).
+template <int D, int KS, int DC = D>
 __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_constant__ SegArgs a) {
   constexpr int D4 = D / 4;
   __shared__ float4 tile[kSegTile * D4];
@@ -97,17 +99,21 @@ __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_cons
     }
     __syncthreads();
     if (active) {
+#pragma unroll 4
       for (int r = 0; r < cnt; ++r) {
         float s = 0.0f;
 #pragma unroll
         for (int c4 = 0; c4 < D4; ++c4) {
           const float4 v = tile[r * D4 + c4];
           const float e0 = q[4 * c4] - v.x, e1 = q[4 * c4 + 1] - v.y;
-          const float e2 = q[4 * c4 + 2] - v.z, e3 = q[4 * c4 + 3] - v.w;
+          const float e2 = q[4 * c4 + 2] - v.z;
           s = fmaf(e0, e0, s);
           s = fmaf(e1, e1, s);
           s = fmaf(e2, e2, s);
-          s = fmaf(e3, e3, s);
+          if (4 * c4 + 3 < DC) {
+            const float e3 = q[4 * c4 + 3] - v.w;
+            s = fmaf(e3, e3, s);
+          }
         }
         const int j = t0 + r;
         if (s < kv[KS - 1] && j != self) {
@@ -200,12 +206,12 @@ __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_cons
   }
 }
 
-template <int D>
+template <int D, int DC = D>
 void launch_seg_scan(const SegArgs& a, int ks, int blocks, cudaStream_t st) {
-  if (ks <= 4) seg_scan_kernel<D, 4><<<blocks, kSegThreads, 0, st>>>(a);
-  else if (ks <= 8) seg_scan_kernel<D, 8><<<blocks, kSegThreads, 0, st>>>(a);
-  else if (ks <= 16) seg_scan_kernel<D, 16><<<blocks, kSegThreads, 0, st>>>(a);
-  else seg_scan_kernel<D, 32><<<blocks, kSegThreads, 0, st>>>(a);
+  if (ks <= 4) seg_scan_kernel<D, 4, DC><<<blocks, kSegThreads, 0, st>>>(a);
+  else if (ks <= 8) seg_scan_kernel<D, 8, DC><<<blocks, kSegThreads, 0, st>>>(a);
+  else if (ks <= 16) seg_scan_kernel<D, 16, DC><<<blocks, kSegThreads, 0, st>>>(a);
+  else seg_scan_kernel<D, 32, DC><<<blocks, kSegThreads, 0, st>>>(a);
 }
 
 int seg_fail(int code, const char* msg) { return report_error(code, msg); }
@@ -329,7 +335,8 @@ extern "C" B2K_API int b2k_knn_segments(const float* dQ, const float* dX, int32_
     a.flags = flags;
     const int ks = k + 3;
     const int nb = (int)blocks.size();
-    if (d <= 4) launch_seg_scan<4>(a, ks, nb, st);
+    if (d <= 3) launch_seg_scan<4, 3>(a, ks, nb, st);
+    else if (d <= 4) launch_seg_scan<4>(a, ks, nb, st);
     else if (d <= 8) launch_seg_scan<8>(a, ks, nb, st);
     else launch_seg_scan<16>(a, ks, nb, st);
     if ((e = cudaGetLastError())) {

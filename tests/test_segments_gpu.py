@@ -116,3 +116,24 @@ def test_chamfer_batch_equals_per_pair_loss():
         torch.testing.assert_close(a.grad, a2.grad, rtol=1e-6, atol=1e-7)
     for b, b2 in zip(B, B2):
         torch.testing.assert_close(b.grad, b2.grad, rtol=1e-6, atol=1e-7)
+
+
+def test_chamfer_batch_stacked_tensors():
+    import torch
+
+    from mlxlearn_b200.autograd import chamfer_loss, chamfer_loss_batch
+
+    rng = np.random.default_rng(9)
+    A = torch.tensor(rng.normal(size=(5, 1000, 3)).astype(np.float32), device="cuda",
+                     requires_grad=True)
+    B = torch.tensor(rng.normal(size=(5, 1300, 3)).astype(np.float32), device="cuda",
+                     requires_grad=True)
+    loss = chamfer_loss_batch(A, B)
+    loss.backward()
+    A2 = A.detach().clone().requires_grad_(True)
+    B2 = B.detach().clone().requires_grad_(True)
+    ref = sum(chamfer_loss(A2[i], B2[i]) for i in range(5))
+    ref.backward()
+    torch.testing.assert_close(loss, ref, rtol=1e-6, atol=1e-6)
+    torch.testing.assert_close(A.grad, A2.grad, rtol=1e-6, atol=1e-7)
+    torch.testing.assert_close(B.grad, B2.grad, rtol=1e-6, atol=1e-7)
