@@ -259,6 +259,26 @@ B2K_API int b2k_radius_result_nnz(const b2k_radius_result *res, int64_t *nnz);
 B2K_API int b2k_radius_result_fetch(const b2k_radius_result *res, int64_t *indptr, int64_t *indices,
                             double *dist);
 
+/* Class votes of a radius result on the device, without downloading it:
+ * codes int32[n_train] (device) are class codes 0..n_classes-1; votes
+ * float64[m, n_classes] and counts int64[m] (device) receive per-row totals of
+ * weight 1, or 1/d with a row's zero distances taking its 0/1 indicator
+ * (weighted != 0 needs a result with distances), summed in ascending
+ * training-index order.  Synchronises `stream`.  Replaces the host
+ * reductions of RadiusNeighborsClassifier
+ * (src/mlxlearn/_kernels/radius_reduce.py:19-60). */
+B2K_API int b2k_radius_result_class_votes(const b2k_radius_result *res, const int32_t *d_codes,
+                                          int32_t n_classes, int32_t weighted, double *d_votes,
+                                          int64_t *d_counts, void *stream);
+
+/* Means of float64 targets[n_train] (device) over each radius row, weight 1 or
+ * 1/d as above; NaN for empty rows.  means float64[m], counts int64[m]
+ * (device).  Replaces src/mlxlearn/_kernels/radius_reduce.py:62-94
+ * (RadiusNeighborsRegressor). */
+B2K_API int b2k_radius_result_means(const b2k_radius_result *res, const double *d_targets,
+                                    int32_t weighted, double *d_means, int64_t *d_counts,
+                                    void *stream);
+
 B2K_API int b2k_radius_result_release(b2k_radius_result *res);
 
 #ifdef __cplusplus

@@ -205,6 +205,13 @@ void launch_votes(const int64_t* idx, const double* dist, int64_t m, int k, cons
                   int n_classes, int weighted, double* votes, int64_t* pred, int* status,
                   cudaStream_t st);
 
+void launch_radius_votes(const int64_t* indptr, const int64_t* indices, const double* dist,
+                         int64_t m, const int* codes, int n_classes, int weighted, double* votes,
+                         int64_t* counts, cudaStream_t st);
+void launch_radius_means(const int64_t* indptr, const int64_t* indices, const double* dist,
+                         int64_t m, const double* targets, int weighted, double* means,
+                         int64_t* counts, cudaStream_t st);
+
 // ---------------------------------------------------------------- backward
 int knn_backward(const float* Q, int64_t m, const float* X, int64_t n, int d, int k,
                  const int64_t* idx, const float* G, const float* E, int squared, float* dQ,

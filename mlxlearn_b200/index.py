@@ -271,6 +271,58 @@ class NeighborIndex:
         self.last_query_backend = "cuda"
         return parts
 
+    def query_radius_reduce(self, Q, radius, *, codes=None, n_classes=0, targets=None,
+                            weighted=False, exclude_self=False, query_block_size=None):
+        """Per-query class votes (``codes``: CUDA int32 labels of the training
+        rows) or target means (``targets``: CUDA float64) over the radius
+        neighbourhoods, reduced on the device without downloading them.
+        Returns ``(votes [m, n_classes] or means [m], counts [m])`` as numpy
+        arrays, equal to the host reductions over :meth:`query_radius_csr`."""
+        import torch
+
+        radius = validate_radius(radius)
+        Q = _as_f32_c(Q)
+        if Q.ndim != 2 or Q.shape[1] != self.n_features:
+            raise ValueError(f"Q must have shape (n, {self.n_features})")
+        if (codes is None) == (targets is None):
+            raise ValueError("pass exactly one of codes and targets")
+        n_query = int(Q.shape[0])
+        if exclude_self and n_query != self.n_samples:
+            raise ValueError(
+                "exclude_self requires the query matrix to be the training matrix: "
+                f"got {n_query} query rows and {self.n_samples} training rows.")
+        dev = torch.device("cuda", self.device)
+        width = int(n_classes) if codes is not None else 1
+        out = torch.empty((n_query, width) if codes is not None else (n_query,),
+                          dtype=torch.float64, device=dev)
+        counts = torch.empty(n_query, dtype=torch.int64, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        step = n_query if not query_block_size else max(1, int(query_block_size))
+        lib = _lib.load()
+        h = self._ensure_device()
+        for start in range(0, n_query, max(step, 1)):
+            stop = min(n_query, start + step)
+            block = Q[start:stop]
+            res = ctypes.c_void_p()
+            rc = lib.b2k_radius(h, block.ctypes.data, stop - start, float(radius),
+                                int(bool(exclude_self)), start, int(bool(weighted)), 0,
+                                ctypes.byref(res))
+            _lib.check(rc, "b2k_radius")
+            try:
+                if codes is not None:
+                    rc = lib.b2k_radius_result_class_votes(
+                        res, codes.data_ptr(), width, int(bool(weighted)),
+                        out[start:stop].data_ptr(), counts[start:stop].data_ptr(), stream)
+                else:
+                    rc = lib.b2k_radius_result_means(
+                        res, targets.data_ptr(), int(bool(weighted)),
+                        out[start:stop].data_ptr(), counts[start:stop].data_ptr(), stream)
+                _lib.check(rc, "radius reduction")
+            finally:
+                lib.b2k_radius_result_release(res)
+        self.last_query_backend = "cuda"
+        return out.cpu().numpy(), counts.cpu().numpy()
+
     def query_radius(self, Q, radius, *, return_distance=True, exclude_self=False,
                      sort_results=False, query_block_size=None, train_block_size=None,
                      algorithm="auto"):

@@ -195,18 +195,21 @@ class NeighborsMixin:
 class RadiusMixin:
     """``radius_neighbors`` and ``radius_neighbors_graph`` (reference _base.py:541-696)."""
 
-    def _radius_parts(self, X, radius, *, need_distance, sort_results):
+    def _radius_query(self, X):
+        """The query rows of a radius call and whether they are the training rows."""
         check_is_fitted(self, "_index_")
-        value = self.radius if radius is None else radius
         query_is_train = X is None
         if query_is_train:
-            Q = self._index_.training_data
-        else:
-            from scipy import sparse
+            return self._index_.training_data, True
+        from scipy import sparse
 
-            if sparse.issparse(X):
-                X = X.toarray()
-            Q = self._validate_query(X, "radius_neighbors")
+        if sparse.issparse(X):
+            X = X.toarray()
+        return self._validate_query(X, "radius_neighbors"), False
+
+    def _radius_parts(self, X, radius, *, need_distance, sort_results):
+        value = self.radius if radius is None else radius
+        Q, query_is_train = self._radius_query(X)
         parts = self._index_.query_radius_csr(Q, value, need_distance=need_distance,
                                               exclude_self=query_is_train,
                                               sort_results=sort_results)

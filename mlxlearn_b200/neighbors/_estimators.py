@@ -199,16 +199,23 @@ class RadiusNeighborsClassifier(RadiusMixin, NeighborsMixin, ClassifierMixin, Ba
         return self
 
     def _proba(self, X):
-        from ..radius_result import concatenate
-        from ._votes import radius_votes
+        import torch
 
         if self.weights not in (None, "uniform", "distance"):
             raise ValueError("weights not recognized: should be 'uniform' or 'distance', "
                              f"got {self.weights!r}")
         weighted = self.weights == "distance"
-        parts = self._radius_parts(X, None, need_distance=weighted, sort_results=False)
-        votes, counts = radius_votes(concatenate(parts), self._y, len(self.classes_),
-                                     weighted=weighted)
+        codes = self.__dict__.get("_codes_dev")
+        if codes is None:
+            codes = torch.from_numpy(self._y.astype(np.int32)).to(
+                torch.device("cuda", self._index_.device))
+            self.__dict__["_codes_dev"] = codes
+        Q, query_is_train = self._radius_query(X)
+        # votes reduced on the device from the device neighbourhoods
+        votes, counts = self._index_.query_radius_reduce(
+            Q, self.radius, codes=codes, n_classes=len(self.classes_), weighted=weighted,
+            exclude_self=query_is_train)
+        self._last_query_backend = "cuda"
         outliers = np.flatnonzero(counts == 0)
         if outliers.size > 0 and self.outlier_label_ is None:
             raise ValueError("No neighbors found for test samples "
@@ -241,6 +248,11 @@ class RadiusNeighborsClassifier(RadiusMixin, NeighborsMixin, ClassifierMixin, Ba
         check_is_fitted(self, "_index_")
         return self._proba(X)
 
+    def __getstate__(self):
+        state = dict(self.__dict__)
+        state.pop("_codes_dev", None)  # device copy of the labels, rebuilt lazily
+        return state
+
 
 class RadiusNeighborsRegressor(RadiusMixin, NeighborsMixin, RegressorMixin, BaseEstimator):
     """Mean (or 1/d-weighted mean) of the targets within ``radius``; a query
@@ -267,17 +279,27 @@ class RadiusNeighborsRegressor(RadiusMixin, NeighborsMixin, RegressorMixin, Base
         return self
 
     def predict(self, X):
-        from ..radius_result import concatenate
-        from ._votes import radius_mean
+        import torch
 
         check_is_fitted(self, "_index_")
         if self.weights not in (None, "uniform", "distance"):
             raise ValueError("weights not recognized: should be 'uniform' or 'distance', "
                              f"got {self.weights!r}")
         weighted = self.weights == "distance"
-        parts = self._radius_parts(X, None, need_distance=weighted, sort_results=False)
-        pred, counts = radius_mean(concatenate(parts), self._y, weighted=weighted)
+        targets = self.__dict__.get("_targets_dev")
+        if targets is None:
+            targets = torch.from_numpy(self._y).to(torch.device("cuda", self._index_.device))
+            self.__dict__["_targets_dev"] = targets
+        Q, query_is_train = self._radius_query(X)
+        pred, counts = self._index_.query_radius_reduce(
+            Q, self.radius, targets=targets, weighted=weighted, exclude_self=query_is_train)
+        self._last_query_backend = "cuda"
         if np.any(counts == 0):
             warnings.warn("One or more samples have no neighbors within specified radius; "
                           "predicting NaN.", stacklevel=2)
         return pred.astype(self._y_out_dtype_, copy=False)
+
+    def __getstate__(self):
+        state = dict(self.__dict__)
+        state.pop("_targets_dev", None)  # device copy of the targets, rebuilt lazily
+        return state

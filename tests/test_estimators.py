@@ -163,3 +163,51 @@ def test_pickle_roundtrip(rng):
     before = clf.predict(X[:50])
     clone = pickle.loads(pickle.dumps(clf))
     np.testing.assert_array_equal(clone.predict(X[:50]), before)
+
+
+@gpu
+@pytest.mark.parametrize("weighted", [False, True])
+def test_device_radius_reductions_equal_host_bincount(weighted):
+    # the device reductions sum each row in the order numpy's bincount does,
+    # so they must equal the host reductions over the downloaded CSR exactly;
+    # queries that coincide with training rows exercise the zero-distance rule
+    import torch
+
+    from mlxlearn_b200.index import build_index
+    from mlxlearn_b200.neighbors._votes import radius_mean, radius_votes
+    from mlxlearn_b200.radius_result import concatenate
+
+    rng = np.random.default_rng(31)
+    X = rng.normal(size=(6000, 8)).astype(np.float32)
+    Q = np.concatenate([X[:40], rng.normal(size=(400, 8)).astype(np.float32)])
+    labels = rng.integers(0, 7, size=6000)
+    targets = rng.normal(size=6000)
+    ix = build_index(X)
+    r = 1.9
+    csr = concatenate(ix.query_radius_csr(Q, r, need_distance=True))
+    hv, hc = radius_votes(csr, labels, 7, weighted=weighted)
+    hm, _ = radius_mean(csr, targets, weighted=weighted)
+    dev = torch.device("cuda", 0)
+    dv, dc = ix.query_radius_reduce(Q, r, codes=torch.from_numpy(labels.astype(np.int32)).to(dev),
+                                    n_classes=7, weighted=weighted)
+    dm, _ = ix.query_radius_reduce(Q, r, targets=torch.from_numpy(targets).to(dev),
+                                   weighted=weighted, query_block_size=97)
+    np.testing.assert_array_equal(dv, hv)
+    np.testing.assert_array_equal(dc, hc)
+    np.testing.assert_array_equal(np.isnan(dm), np.isnan(hm))
+    np.testing.assert_array_equal(dm[~np.isnan(dm)], hm[~np.isnan(hm)])
+
+
+@gpu
+def test_radius_estimators_pickle(rng):
+    X, y, Q = radius_data()
+    clf = RadiusNeighborsClassifier(radius=6.25, outlier_label="most_frequent").fit(X, y)
+    before = clf.predict(Q[:200])
+    np.testing.assert_array_equal(pickle.loads(pickle.dumps(clf)).predict(Q[:200]), before)
+    reg = RadiusNeighborsRegressor(radius=6.25, weights="distance").fit(X, y.astype(np.float64))
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        p0 = reg.predict(Q[:200])
+        p1 = pickle.loads(pickle.dumps(reg)).predict(Q[:200])
+    np.testing.assert_array_equal(np.isnan(p0), np.isnan(p1))
+    np.testing.assert_array_equal(p0[~np.isnan(p0)], p1[~np.isnan(p1)])
