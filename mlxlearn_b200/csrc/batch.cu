@@ -19,12 +19,14 @@
 // launch addresses all of its problems through at most kBatchGroups sets of
 // three tensor maps passed as kernel parameters.
 //
-// Balance: items are costed (reference tiles x (64-column blocks + 1)),
-// sorted by cost and dealt greedily to the least-loaded CTA (longest
-// processing time first); items of one problem stay adjacent in that order,
-// so CTAs running at the same time read the same reference tiles from L2.
+// Balance: items are costed (reference tiles x (64-column blocks + 1)) and
+// sorted longest first; each CTA claims the next item of that list when it
+// finishes one (an online longest-processing-time-first schedule that also
+// absorbs per-tile costs the model misses); items of one problem stay
+// adjacent, so CTAs running at the same time read the same reference tiles
+// from L2.
 //
-// Autotuner: per (dp, heap width) bucket the epilogue width (4 or 8 warps),
+// Autotuner: per (dp, heap width) bucket the epilogue width (4, 8 or 16 warps),
 // and for the whole batch the split granularity (items per CTA), chosen by
 // timing graph runs of the batch itself; choices are cached per process.
 #include <cuda.h>
@@ -71,9 +73,12 @@ int64_t rup(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 int kmax_class(int k) { return k <= 8 ? 8 : k <= 12 ? 12 : k <= 16 ? 16 : 64; }
 
 // ---------------------------------------------------------------- tuning
+// Epilogue warps per (dp, heap width) bucket; 0 = the default (16 for the
+// register-heap trackers, 8 for the lazy tracker).
 struct Tuning {
-  int ew8 = 1;  // 8 epilogue warps, else 4
+  int ew = 0;
 };
+int default_ew(int kmax) { return kmax <= 16 ? 16 : 8; }
 struct TuneKey {
   int dp, kmax;
   bool operator<(const TuneKey& o) const { return dp != o.dp ? dp < o.dp : kmax < o.kmax; }
@@ -169,6 +174,7 @@ struct b2k_batch {
   std::vector<b2k::LaunchSpec> specs;
   std::vector<b2k::TcBatchLaunch> launches;
   b2k::CertifyArgs* cert_tab = nullptr;
+  int* item_counters = nullptr;  // [launches]
   int work_items = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -351,7 +357,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
   for (auto& p : b->probs) {
     if (!p.in_graph) continue;
     const Tuning t = tuning_for(p, tune);
-    p.ew = t.ew8 ? 8 : 4;
+    p.ew = t.ew ? t.ew : default_ew(p.kmax);
     p.halves = p.ew / 4;
     total_cost += (double)p.m_tiles * p.n_tiles * (p.KB + 1);
     classes[std::make_tuple(p.kmax, p.ew, p.KB > 4)].push_back((int)(&p - b->probs.data()));
@@ -455,7 +461,8 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
   BCUDA(cudaMemcpyAsync(d_tc, tc.data(), P * sizeof(TcProblem), cudaMemcpyHostToDevice, st));
   BCUDA(cudaMemcpyAsync(b->cert_tab, cert.data(), P * sizeof(CertifyArgs),
                         cudaMemcpyHostToDevice, st));
-  // 4. work items per launch, balanced over the CTAs (longest first)
+  // 4. work items per launch, longest first; the CTAs claim them in that
+  //    order as they finish their previous item (greedy LPT online)
   std::vector<const BProb*> by_gi(P);
   for (auto& q : b->probs)
     if (q.in_graph) by_gi[q.gi] = &q;
@@ -478,30 +485,12 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
     std::stable_sort(items.begin(), items.end(),
                      [](const Item& a, const Item& c) { return a.cost > c.cost; });
     const int grid = (int)std::min<size_t>((size_t)sms, items.size());
-    std::vector<std::vector<int4>> per(grid);
-    using Load = std::pair<double, int>;
-    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-    for (int c = 0; c < grid; ++c) heap.push(Load{0.0, c});
-    for (const Item& it : items) {
-      Load l = heap.top();
-      heap.pop();
-      per[l.second].push_back(it.v);
-      heap.push(Load{l.first + it.cost, l.second});
-    }
     std::vector<int4> flat;
-    std::vector<int> begin(grid + 1, 0);
-    for (int c = 0; c < grid; ++c) {
-      begin[c] = (int)flat.size();
-      flat.insert(flat.end(), per[c].begin(), per[c].end());
-    }
-    begin[grid] = (int)flat.size();
+    flat.reserve(items.size());
+    for (const Item& it : items) flat.push_back(it.v);
     int4* d_items = nullptr;
-    int* d_begin = nullptr;
     if ((rc = o.alloc(&d_items, flat.size()))) return rc;
-    if ((rc = o.alloc(&d_begin, begin.size()))) return rc;
     BCUDA(cudaMemcpyAsync(d_items, flat.data(), flat.size() * sizeof(int4),
-                          cudaMemcpyHostToDevice, st));
-    BCUDA(cudaMemcpyAsync(d_begin, begin.data(), begin.size() * sizeof(int),
                           cudaMemcpyHostToDevice, st));
     TcBatchLaunch L{};
     L.groups = (int)spec.dpgs.size();
@@ -516,7 +505,8 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
     L.aaug = b->m_ones;
     L.probs = d_tc;
     L.items = d_items;
-    L.cta_begin = d_begin;
+    L.cta_begin = nullptr;
+    L.n_items = (int)flat.size();
     L.grid = grid;
     L.kmax = spec.kmax;
     L.ew = spec.ew;
@@ -528,6 +518,10 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
     b->launches.push_back(L);
     b->work_items += (int)flat.size();
   }
+  // one item counter per launch, zeroed at the start of every run
+  if ((rc = o.alloc(&b->item_counters, b->launches.size()))) return rc;
+  for (size_t i = 0; i < b->launches.size(); ++i)
+    b->launches[i].item_counter = b->item_counters + i;
   BCUDA(cudaStreamSynchronize(st));
   return B2K_OK;
 }
@@ -538,6 +532,7 @@ int record(b2k_batch* b, cudaStream_t st) {
   if (P == 0) return B2K_OK;
   BCUDA(cudaMemsetAsync(b->zero_block, 0, (8 + (size_t)P) * sizeof(int), st));
   BCUDA(cudaMemsetAsync(b->counters, 0, 4 * sizeof(unsigned long long), st));
+  BCUDA(cudaMemsetAsync(b->item_counters, 0, b->launches.size() * sizeof(int), st));
   BCUDA(cudaMemsetAsync(b->skth, 0xff, (size_t)b->total_pad * sizeof(uint32_t), st));
   launch_prep_queries_batch(b->prep_tab, b->pad_start, P, b->total_pad, st);
   BCUDA(cudaGetLastError());
@@ -651,16 +646,22 @@ int autotune(b2k_batch* b, std::map<TuneKey, Tuning>& tune, int& gran) {
   gran = best_gran;
   // epilogue width per (dp, heap width) bucket
   for (const TuneKey& k : keys) {
-    Tuning cur = tune.count(k) ? tune[k] : Tuning{};
-    Tuning alt = cur;
-    alt.ew8 = !cur.ew8;
-    tune[k] = alt;
-    float ms;
-    if ((rc = trial(&ms))) return rc;
-    if (ms < best * 0.98f)
-      best = ms;
-    else
-      tune[k] = cur;
+    const Tuning cur = tune.count(k) ? tune[k] : Tuning{};
+    const int ew0 = cur.ew ? cur.ew : default_ew(k.kmax);
+    Tuning keep = cur;
+    for (int ew : {16, 8, 4}) {
+      if (ew == ew0 || (ew == 16 && k.kmax > 16)) continue;
+      Tuning alt;
+      alt.ew = ew;
+      tune[k] = alt;
+      float ms;
+      if ((rc = trial(&ms))) return rc;
+      if (ms < best * 0.98f) {
+        best = ms;
+        keep = alt;
+      }
+    }
+    tune[k] = keep;
   }
   return B2K_OK;
 }

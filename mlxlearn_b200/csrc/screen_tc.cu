@@ -58,7 +58,8 @@ struct TcParams {
   const int4* items;         // batched: (problem, query tile, first tile, end tile)
   const int* cta_begin;      // batched: CTA b runs items [cta_begin[b], cta_begin[b + 1])
   int* status;
-  int* unit_counter;         // single problem: units claimed dynamically (or null: round-robin)
+  int* unit_counter;         // units claimed dynamically (or null: round-robin / per-CTA lists)
+  int n_items;               // batched, claimed: items in the list
   TcProblem one;             // single problem
 };
 
@@ -95,12 +96,16 @@ struct UnitCursor {
   UnitRing ring;
   uint32_t rs, rph;
   B2K_DEV UnitCursor(const TcParams& p, const UnitRing& r, bool is_producer) {
-    dyn = !BATCH && p.unit_counter != nullptr;
+    dyn = p.unit_counter != nullptr;
     producer = is_producer;
     ring = r;
     rs = 0;
     rph = 0;
-    if (BATCH) {
+    if (BATCH && dyn) {
+      u = 0;
+      end = p.n_items;
+      step = 1;
+    } else if (BATCH) {
       u = p.cta_begin[blockIdx.x];
       end = p.cta_begin[blockIdx.x + 1];
       step = 1;
@@ -588,15 +593,18 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
 // Batched launches: kNN sinks only, with 4 or 8 epilogue warps.  Heap width
 // class 64 stands for the lazy tracker (every k > 16).
 #define B2K_TC_BATCH_DISPATCH(CALL)                                         \
-  switch (kmax * 16 + ew) {                                                 \
-    case 8 * 16 + 8: return CALL(KnnSink<8>, 8);                            \
-    case 8 * 16 + 4: return CALL(KnnSink<8>, 4);                            \
-    case 12 * 16 + 8: return CALL(KnnSink<12>, 8);                          \
-    case 12 * 16 + 4: return CALL(KnnSink<12>, 4);                          \
-    case 16 * 16 + 8: return CALL(KnnSink<16>, 8);                          \
-    case 16 * 16 + 4: return CALL(KnnSink<16>, 4);                          \
-    case 64 * 16 + 8: return CALL(LazyKnnSink, 8);                          \
-    case 64 * 16 + 4: return CALL(LazyKnnSink, 4);                          \
+  switch (kmax * 32 + ew) {                                                 \
+    case 8 * 32 + 16: return CALL(KnnSink<8>, 16);                          \
+    case 12 * 32 + 16: return CALL(KnnSink<12>, 16);                        \
+    case 16 * 32 + 16: return CALL(KnnSink<16>, 16);                        \
+    case 8 * 32 + 8: return CALL(KnnSink<8>, 8);                            \
+    case 8 * 32 + 4: return CALL(KnnSink<8>, 4);                            \
+    case 12 * 32 + 8: return CALL(KnnSink<12>, 8);                          \
+    case 12 * 32 + 4: return CALL(KnnSink<12>, 4);                          \
+    case 16 * 32 + 8: return CALL(KnnSink<16>, 8);                          \
+    case 16 * 32 + 4: return CALL(KnnSink<16>, 4);                          \
+    case 64 * 32 + 8: return CALL(LazyKnnSink, 8);                          \
+    case 64 * 32 + 4: return CALL(LazyKnnSink, 4);                          \
     default: return (int)cudaErrorInvalidValue;                             \
   }
 
@@ -626,6 +634,8 @@ int launch_screen_tc_batch(const TcBatchLaunch& L, cudaStream_t st) {
   p.probs = L.probs;
   p.items = L.items;
   p.cta_begin = L.cta_begin;
+  p.unit_counter = L.item_counter;
+  p.n_items = L.n_items;
   p.status = L.status;
   const int kmax = L.kmax, ew = L.ew, KB = L.KB_max, grid = L.grid;
   const bool a_stream = L.a_stream;

@@ -40,10 +40,12 @@ struct TcBatchLaunch {
   const TcProblem* probs;
   const int4* items;
   const int* cta_begin;
+  int* item_counter;  // claimed in order from `items` when set (then cta_begin is unused)
+  int n_items;
   int grid;
   int KB_max;
   int kmax;       // heap width class: 8, 12, 16, or 64 (lazy tracker, k > 16)
-  int ew;         // epilogue warps: 4 or 8
+  int ew;         // epilogue warps: 4, 8, or 16 (heap widths <= 16)
   bool a_stream;  // stream the query tile with every block (KB_max > 4)
   int* status;
 };
