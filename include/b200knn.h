@@ -157,7 +157,7 @@ B2K_API int b2k_knn_backward(const float *dQ, int64_t m, const float *dX, int64_
  * int64[rows, k] (indices within the reference segment) and d_dist
  * float64[rows, k] (or NULL), same order and tie rule as b2k_knn_device.
  * exclude_self: every query segment is its reference segment and row i skips
- * itself.  1 <= d <= 16, k <= 29.  Enqueued on `stream`; the call
+ * itself.  1 <= d <= 64, k <= 29.  Enqueued on `stream`; the call
  * synchronises it.  No counterpart in the reference (one problem per
  * NeighborIndex.query call, src/mlxlearn/_kernels/distance.py:242-270); it
  * backs the batched Chamfer loss of mlxlearn_b200/autograd.py. */

@@ -17,6 +17,32 @@ __all__ = ["knn_distances", "chamfer_loss", "KnnDistances", "knn_segments",
            "chamfer_loss_batch", "KnnSegmentDistances"]
 
 
+# Below this many (query, reference) pairs a direct scan (b2k_knn_segments)
+# costs less than building and querying a temporary index.
+_DIRECT_PAIRS = 1 << 27
+
+
+def _segments_forward(Qc, Xc, q_sizes, x_sizes, k, exclude_self):
+    """float64 distances and int64 indices (within each reference segment)."""
+    import numpy as np
+
+    qo = np.zeros(len(q_sizes) + 1, dtype=np.int64)
+    np.cumsum(np.asarray(q_sizes, dtype=np.int64), out=qo[1:])
+    xo = np.zeros(len(x_sizes) + 1, dtype=np.int64)
+    np.cumsum(np.asarray(x_sizes, dtype=np.int64), out=xo[1:])
+    if qo[-1] != Qc.shape[0] or xo[-1] != Xc.shape[0]:
+        raise ValueError("segment sizes must add up to the row counts")
+    rows, d = Qc.shape
+    idx = torch.empty((rows, k), dtype=torch.int64, device=Qc.device)
+    dist64 = torch.empty((rows, k), dtype=torch.float64, device=Qc.device)
+    stream = torch.cuda.current_stream(Qc.device).cuda_stream
+    _lib.check(_lib.load().b2k_knn_segments(
+        Qc.data_ptr(), Xc.data_ptr(), d, qo.ctypes.data, xo.ctypes.data, len(q_sizes), k,
+        int(bool(exclude_self)), dist64.data_ptr(), idx.data_ptr(), stream),
+        "b2k_knn_segments")
+    return dist64, idx
+
+
 def _device_index(X: torch.Tensor):
     """A temporary exact index over a CUDA float32 tensor (copied)."""
     from .index import NeighborIndex
@@ -33,11 +59,16 @@ class KnnDistances(torch.autograd.Function):
             raise TypeError("knn_distances expects CUDA tensors")
         Qc = Q.detach().to(torch.float32).contiguous()
         Xc = X.detach().to(torch.float32).contiguous()
-        index = _device_index(Xc)
-        try:
-            dist64, idx = index.query_device(Qc, int(k), exclude_self=bool(exclude_self))
-        finally:
-            index.close()
+        m, n, d = Qc.shape[0], Xc.shape[0], Qc.shape[1]
+        if d <= 64 and int(k) <= 29 and m * n <= _DIRECT_PAIRS:
+            # small problem: one direct exact scan, no temporary index
+            dist64, idx = _segments_forward(Qc, Xc, (m,), (n,), int(k), bool(exclude_self))
+        else:
+            index = _device_index(Xc)
+            try:
+                dist64, idx = index.query_device(Qc, int(k), exclude_self=bool(exclude_self))
+            finally:
+                index.close()
         e = dist64.to(torch.float32)
         out = dist64.square().to(torch.float32) if squared else e
         ctx.save_for_backward(Qc, Xc, idx, e)
@@ -100,17 +131,9 @@ class KnnSegmentDistances(torch.autograd.Function):
             raise TypeError("knn_segments expects CUDA tensors")
         Qc = Q.detach().to(torch.float32).contiguous()
         Xc = X.detach().to(torch.float32).contiguous()
-        qo, xo = _offsets(q_sizes), _offsets(x_sizes)
-        if qo[-1] != Qc.shape[0] or xo[-1] != Xc.shape[0]:
-            raise ValueError("segment sizes must add up to the row counts")
-        rows, d, k = Qc.shape[0], Qc.shape[1], int(k)
-        idx = torch.empty((rows, k), dtype=torch.int64, device=Qc.device)
-        dist64 = torch.empty((rows, k), dtype=torch.float64, device=Qc.device)
-        stream = torch.cuda.current_stream(Qc.device).cuda_stream
-        _lib.check(_lib.load().b2k_knn_segments(
-            Qc.data_ptr(), Xc.data_ptr(), d, qo.ctypes.data, xo.ctypes.data, len(q_sizes), k,
-            int(bool(exclude_self)), dist64.data_ptr(), idx.data_ptr(), stream),
-            "b2k_knn_segments")
+        k = int(k)
+        dist64, idx = _segments_forward(Qc, Xc, q_sizes, x_sizes, k, exclude_self)
+        xo = _offsets(x_sizes)
         # global reference rows for the backward
         starts = torch.as_tensor(xo[:-1], device=Qc.device)
         seg = torch.repeat_interleave(torch.arange(len(q_sizes), device=Qc.device),
@@ -148,14 +171,14 @@ def knn_segments(Q, X, q_sizes, x_sizes, k=1, *, exclude_self=False, squared=Fal
     """Distances ``[rows, k]`` and indices (within each reference segment) of
     many small problems at once: problem p is the p-th block of ``q_sizes[p]``
     rows of ``Q`` against the p-th block of ``x_sizes[p]`` rows of ``X``
-    (d <= 16, k <= 29)."""
+    (d <= 64, k <= 29)."""
     return KnnSegmentDistances.apply(Q, X, tuple(int(v) for v in q_sizes),
                                      tuple(int(v) for v in x_sizes), k, exclude_self, squared)
 
 
 def chamfer_loss_batch(As, Bs):
     """Sum over pairs of the symmetric k=1 Chamfer term of ``chamfer_loss``,
-    with one search and one backward call for all pairs (clouds of d <= 16).
+    with one search and one backward call for all pairs (clouds of d <= 64).
     ``As`` and ``Bs`` are lists of ``[n_i, d]`` tensors, or two ``[P, n, d]``
     tensors of equally sized clouds (cheaper: no per-cloud gradient tensors)."""
     if torch.is_tensor(As) and torch.is_tensor(Bs) and As.dim() == 3 and Bs.dim() == 3:

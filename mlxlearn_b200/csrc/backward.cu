@@ -204,33 +204,31 @@ __global__ void grad_x_narrow_kernel(const float* __restrict__ Q, const float* _
     if (f < d) dX[r * d + f] = acc[f];
 }
 
-// One warp per reference row: order its bucket (insertion sort by flat
-// position, buckets are short), then accumulate in that order.
+// One warp per reference row: put its bucket in ascending flat position
+// (each lane ranks some entries against the whole bucket and writes them to
+// `sorted`: linear per entry, so rows that many queries picked stay cheap),
+// then accumulate in that order.
 __global__ void grad_x_kernel(const float* __restrict__ Q, const float* __restrict__ X,
                               const float* __restrict__ G, const float* __restrict__ E,
-                              const int* __restrict__ offsets, int* __restrict__ order,
-                              int64_t n, int d, int k, int squared, float* __restrict__ dX) {
+                              const int* __restrict__ offsets, const int* __restrict__ order,
+                              int* __restrict__ sorted, int64_t n, int d, int k, int squared,
+                              float* __restrict__ dX) {
   const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (r >= n) return;
-  const int a = offsets[r], b = offsets[r + 1];
-  if (lane == 0) {
-    for (int p = a + 1; p < b; ++p) {
-      const int v = order[p];
-      int q = p;
-      while (q > a && order[q - 1] > v) {
-        order[q] = order[q - 1];
-        --q;
-      }
-      order[q] = v;
-    }
+  const int a = offsets[r], b = offsets[r + 1], cnt = b - a;
+  for (int e = lane; e < cnt; e += 32) {
+    const int v = order[a + e];
+    int rank = 0;
+    for (int f = 0; f < cnt; ++f) rank += order[a + f] < v;  // flat positions are distinct
+    sorted[a + rank] = v;
   }
   __syncwarp();
   for (int f = lane; f < d; f += 32) {
     const float x = X[r * d + f];
     float acc = 0.0f;
     for (int p = a; p < b; ++p) {
-      const int t = order[p];
+      const int t = sorted[p];
       const int64_t i = t / k;
       const float c = coef_of(G[t], E ? E[t] : 0.0f, squared);
       acc = fmaf(c, x - Q[i * d + f], acc);
@@ -261,11 +259,12 @@ int knn_backward(const float* Q, int64_t m, const float* X, int64_t n, int d, in
     int* cursor = offsets + n + 1;     // [n]
     int* order = cursor + n;           // [mk]
     int* sums = order + mk;            // [nb + 1] block sums of the scan
+    const int nb = (int)((n + kScanBlock - 1) / kScanBlock);
+    int* sorted = sums + nb + 1;       // [mk] buckets in ascending flat order
     cudaMemsetAsync(counts, 0, (size_t)n * sizeof(int), st);
     cudaMemsetAsync(cursor, 0, (size_t)n * sizeof(int), st);
     if (mk > 0)
       bucket_count_kernel<<<(unsigned)((mk + 255) / 256), 256, 0, st>>>(idx, mk, counts);
-    const int nb = (int)((n + kScanBlock - 1) / kScanBlock);
     scan_sums_kernel<<<nb, kScanThreads, 0, st>>>(counts, n, sums);
     scan_top_kernel<<<1, kScanThreads, 0, st>>>(sums, nb);
     scan_apply_kernel<<<nb, kScanThreads, 0, st>>>(counts, n, sums, nb, offsets);
@@ -277,13 +276,14 @@ int knn_backward(const float* Q, int64_t m, const float* X, int64_t n, int d, in
           Q, X, G, E, offsets, order, n, d, k, squared, dX);
     else
       grad_x_kernel<<<(unsigned)((n + warps - 1) / warps), warps * 32, 0, st>>>(
-          Q, X, G, E, offsets, order, n, d, k, squared, dX);
+          Q, X, G, E, offsets, order, sorted, n, d, k, squared, dX);
   }
   return (int)cudaGetLastError();
 }
 
 size_t knn_backward_workspace_ints(int64_t m, int64_t n, int k) {
-  return (size_t)(3 * n + 1) + (size_t)m * k + (size_t)((n + kScanBlock - 1) / kScanBlock) + 1;
+  return (size_t)(3 * n + 1) + 2 * (size_t)m * k + (size_t)((n + kScanBlock - 1) / kScanBlock) +
+         1;
 }
 
 }  // namespace b2k

@@ -3,9 +3,9 @@
 // where every pair of clouds is its own small problem.
 //
 // The tensor-core screen needs an index per problem and one call per
-// problem; for d <= 16 and a few thousand rows a direct scan is cheaper.
+// problem; for d <= 64 and a few thousand rows a direct scan is cheaper.
 // One block takes 128 queries of one segment; the segment's reference rows
-// pass through shared memory in tiles of 512, and every thread keeps the KS
+// pass through shared memory in 32 KB tiles, and every thread keeps the KS
 // smallest fp32 squared distances of its query (KS >= k + 3) in registers.
 // The fp32 value s of a pair is within g S + d 2^-126 of the exact S,
 // g = (d + 5) 2^-24 (1.01) (a sum of rounded squares of rounded differences,
@@ -33,7 +33,8 @@ namespace b2k {
 namespace {
 
 constexpr int kSegThreads = 128;  // queries per block
-constexpr int kSegTile = 512;     // reference rows per shared-memory tile
+// reference rows per shared-memory tile: 32 KB of padded rows, at most 512
+__host__ __device__ constexpr int seg_tile_rows(int D) { return D <= 16 ? 512 : 8192 / D; }
 
 struct SegArgs {
   const float* Q;
@@ -64,9 +65,52 @@ __global__ void seg_range_kernel(const float* __restrict__ v, int64_t count, int
 
 // D: padded width (4, 8 or 16) of the shared-memory rows; DC: coordinates
 // actually computed (D, or 3 for three-dimensional points).
+// Packed pairs of fp32 values (one 64-bit register), for the paired
+// sub / fma instructions: each half is rounded exactly as the scalar op.
+__device__ __forceinline__ uint64_t pk(float lo, float hi) {
+  uint64_t x;
+  asm("mov.b64 %0, {%1,%2};" : "=l"(x) : "f"(lo), "f"(hi));
+  return x;
+}
+__device__ __forceinline__ void upk(uint64_t x, float& lo, float& hi) {
+  asm("mov.b64 {%0,%1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x));
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+template <int KS>
+__device__ __forceinline__ void seg_offer(float s, int j, int self, float (&kv)[KS],
+                                          int (&ki)[KS]) {
+  if (s < kv[KS - 1] && j != self) {
+    // insertion after any equal value: equal values keep scan (index) order
+    float cv = s;
+    int cj = j;
+#pragma unroll
+    for (int i = 0; i < KS; ++i) {
+      if (cv < kv[i]) {
+        const float tv = kv[i];
+        const int tj = ki[i];
+        kv[i] = cv;
+        ki[i] = cj;
+        cv = tv;
+        cj = tj;
+      }
+    }
+  }
+}
+
 template <int D, int KS, int DC = D>
 __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_constant__ SegArgs a) {
   constexpr int D4 = D / 4;
+  constexpr int kSegTile = seg_tile_rows(D);
   __shared__ float4 tile[kSegTile * D4];
   const int2 blk = a.blocks[blockIdx.x];
   const int64_t q_lo = a.qseg[blk.x], q_hi = a.qseg[blk.x + 1];
@@ -98,7 +142,34 @@ __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_cons
                             c + 2 < d ? x[c + 2] : 0.0f, c + 3 < d ? x[c + 3] : 0.0f);
     }
     __syncthreads();
-    if (active) {
+    if (active && DC == 3) {
+      // three coordinates, two reference rows per paired instruction; the
+      // sums are formed in the scalar order e0^2, e1^2, e2^2
+      const uint64_t q0 = pk(q[0], q[0]), q1 = pk(q[1], q[1]), q2 = pk(q[2], q[2]);
+      int r = 0;
+#pragma unroll 2
+      for (; r + 1 < cnt; r += 2) {
+        const float4 v0 = tile[r], v1 = tile[r + 1];
+        const uint64_t e0 = sub2(q0, pk(v0.x, v1.x));
+        const uint64_t e1 = sub2(q1, pk(v0.y, v1.y));
+        const uint64_t e2 = sub2(q2, pk(v0.z, v1.z));
+        uint64_t s2 = fma2(e0, e0, pk(0.0f, 0.0f));
+        s2 = fma2(e1, e1, s2);
+        s2 = fma2(e2, e2, s2);
+        float s0, s1;
+        upk(s2, s0, s1);
+        seg_offer<KS>(s0, t0 + r, self, kv, ki);
+        seg_offer<KS>(s1, t0 + r + 1, self, kv, ki);
+      }
+      if (r < cnt) {
+        const float4 v = tile[r];
+        const float e0 = q[0] - v.x, e1 = q[1] - v.y, e2 = q[2] - v.z;
+        float s0 = fmaf(e0, e0, 0.0f);
+        s0 = fmaf(e1, e1, s0);
+        s0 = fmaf(e2, e2, s0);
+        seg_offer<KS>(s0, t0 + r, self, kv, ki);
+      }
+    } else if (active) {
 #pragma unroll 4
       for (int r = 0; r < cnt; ++r) {
         float s = 0.0f;
@@ -115,23 +186,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_scan_kernel(const __grid_cons
             s = fmaf(e3, e3, s);
           }
         }
-        const int j = t0 + r;
-        if (s < kv[KS - 1] && j != self) {
-          // insertion after any equal value: equal values keep scan (index) order
-          float cv = s;
-          int cj = j;
-#pragma unroll
-          for (int i = 0; i < KS; ++i) {
-            if (cv < kv[i]) {
-              const float tv = kv[i];
-              const int tj = ki[i];
-              kv[i] = cv;
-              ki[i] = cj;
-              cv = tv;
-              cj = tj;
-            }
-          }
-        }
+        seg_offer<KS>(s, t0 + r, self, kv, ki);
       }
     }
   }
@@ -227,8 +282,8 @@ extern "C" B2K_API int b2k_knn_segments(const float* dQ, const float* dX, int32_
                                         double* d_dist, int64_t* d_idx, void* stream) {
   if (segments < 0 || !q_offsets || !x_offsets)
     return seg_fail(B2K_EINVAL, "segment offsets must not be NULL");
-  if (d <= 0 || d > 16)
-    return seg_fail(B2K_EUNSUPPORTED, "b2k_knn_segments handles 1 <= d <= 16; use the index API");
+  if (d <= 0 || d > 64)
+    return seg_fail(B2K_EUNSUPPORTED, "b2k_knn_segments handles 1 <= d <= 64; use the index API");
   if (k <= 0) return seg_fail(B2K_EINVAL, "Expected n_neighbors > 0.");
   if (k > 29) return seg_fail(B2K_EUNSUPPORTED, "b2k_knn_segments handles k <= 29");
   if (q_offsets[0] != 0 || x_offsets[0] != 0)
@@ -338,7 +393,9 @@ extern "C" B2K_API int b2k_knn_segments(const float* dQ, const float* dX, int32_
     if (d <= 3) launch_seg_scan<4, 3>(a, ks, nb, st);
     else if (d <= 4) launch_seg_scan<4>(a, ks, nb, st);
     else if (d <= 8) launch_seg_scan<8>(a, ks, nb, st);
-    else launch_seg_scan<16>(a, ks, nb, st);
+    else if (d <= 16) launch_seg_scan<16>(a, ks, nb, st);
+    else if (d <= 32) launch_seg_scan<32>(a, ks, nb, st);
+    else launch_seg_scan<64>(a, ks, nb, st);
     if ((e = cudaGetLastError())) {
       rc = seg_fail(B2K_ECUDA, "b2k_knn_segments: scan launch failed");
       break;

@@ -40,7 +40,8 @@ def _check(Qs, Xs, k, dist, idx, exclude_self=False):
         r += m
 
 
-@pytest.mark.parametrize("d,k", [(3, 1), (3, 8), (8, 5), (16, 13), (5, 29)])
+@pytest.mark.parametrize("d,k", [(3, 1), (3, 8), (8, 5), (16, 13), (5, 29), (32, 4), (64, 8),
+                                 (50, 20)])
 def test_uneven_segments_match_oracle(d, k):
     rng = np.random.default_rng(100 + d + k)
     sizes = [(int(rng.integers(1, 700)), int(rng.integers(k, 2500))) for _ in range(9)]
@@ -85,8 +86,8 @@ def test_rejects_bad_segments():
         knn_segments(Q, X, [4, 5], [5, 5], 1)       # sizes do not add up
     from mlxlearn_b200.exceptions import BackendExecutionError
     with pytest.raises(BackendExecutionError):
-        knn_segments(torch.zeros((4, 20), device="cuda"), torch.zeros((4, 20), device="cuda"),
-                     [4], [4], 1)                   # d > 16
+        knn_segments(torch.zeros((4, 80), device="cuda"), torch.zeros((4, 80), device="cuda"),
+                     [4], [4], 1)                   # d > 64
 
 
 def test_chamfer_batch_equals_per_pair_loss():
@@ -137,3 +138,21 @@ def test_chamfer_batch_stacked_tensors():
     torch.testing.assert_close(loss, ref, rtol=1e-6, atol=1e-6)
     torch.testing.assert_close(A.grad, A2.grad, rtol=1e-6, atol=1e-7)
     torch.testing.assert_close(B.grad, B2.grad, rtol=1e-6, atol=1e-7)
+
+
+def test_small_knn_distances_take_the_direct_scan_and_match_the_index_path():
+    # a self-kNN of 3,000 x 64 is below the direct-scan limit; its answer must
+    # equal the oracle's, exactly as the index path's does
+    import torch
+
+    from mlxlearn_b200.autograd import knn_distances
+
+    rng = np.random.default_rng(12)
+    X = rng.standard_normal((3000, 64)).astype(np.float32)
+    Xt = torch.from_numpy(X).cuda().requires_grad_()
+    d, i = knn_distances(Xt, None, 8)
+    od, oi = oracle.knn(X, X, 8, exclude_self=True)
+    np.testing.assert_array_equal(i.cpu().numpy(), oi)
+    np.testing.assert_allclose(d.detach().double().cpu().numpy(), od, rtol=1e-6, atol=0)
+    d.mean().backward()
+    assert torch.isfinite(Xt.grad).all()
