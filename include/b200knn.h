@@ -59,6 +59,7 @@ typedef struct b2k_stats {
   int64_t candidates;       /* candidates re-ranked in float64                 */
   int64_t list_entries;     /* screen list appends                             */
   int64_t fallback_rows;    /* queries resolved by the exhaustive exact scan   */
+  int64_t second_pass_rows; /* queries the bf16 pass left to the fp32 pass     */
   int64_t exact_compares;   /* near-tie pairs resolved with exact integer keys */
   double screen_ms;         /* device time of the screen kernel (if timed)     */
   double total_ms;          /* device time of the whole call (if timed)        */

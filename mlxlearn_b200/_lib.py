@@ -39,6 +39,7 @@ class Stats(ctypes.Structure):
         ("candidates", ctypes.c_int64),
         ("list_entries", ctypes.c_int64),
         ("fallback_rows", ctypes.c_int64),
+        ("second_pass_rows", ctypes.c_int64),
         ("exact_compares", ctypes.c_int64),
         ("screen_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),

@@ -281,9 +281,12 @@ static int run_exact(Index& ix, const float* dQ, int64_t m, int k, int exclude_s
   return B2K_OK;
 }
 
+// ext_perm (optional): the rows of dQ are already in screen order, and row i
+// answers query ext_perm[i] (its output row and self index); used for the
+// second pass over rows a bf16 pass could not certify.
 static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
                            int64_t q_offset, int mode, double* d_dist, int64_t* d_idx,
-                           cudaStream_t st, b2k_stats* stats) {
+                           cudaStream_t st, b2k_stats* stats, const int* ext_perm = nullptr) {
   const int fm = fault_mode();
   if (fm == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
   if (mode == B2K_MODE_AUTO)
@@ -313,11 +316,15 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   fr.keep(counters);
   B2K_CUDA(cudaMemsetAsync(status, 0, 8 * sizeof(int), st));
   B2K_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+  // NaN / inf queries: flagged on the device, reported with the final status
+  // read (the search itself stays bounded on such inputs)
+  launch_nonfinite_check(dQ, m * (int64_t)ix.d, status + 5, st);
 
   int S = 1;
+  int64_t second_pass_rows = 0, second_exact_rows = 0;
   if (mode == B2K_MODE_EXACT) {
     rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, nullptr, nullptr,
-                   counters, status, st, fr, true);
+                   counters, status, st, fr, true, ext_perm);
     if (rc) return rc;
   } else {
     if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
@@ -330,9 +337,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     // lists per query: one per (split, column group of the screen)
     const int S_lists = S * (tc ? tc_column_groups(k) : simt_column_groups(kSinkKnn));
     // Group nearby queries (reorder.cu); results go back to the original rows.
-    const int* perm = nullptr;
+    const int* perm = ext_perm;
     const float* Qs = dQ;
-    if (m >= 2048 && reorder_enabled()) {
+    if (!ext_perm && m >= 2048 && reorder_enabled()) {
       if ((rc = ensure_pivots(ix))) return rc;
       int *key = nullptr, *hist = nullptr, *pm = nullptr;
       float* Qp = nullptr;
@@ -415,11 +422,38 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.perm = perm;
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
-    // Rows the screen could not certify (list overflow, or query coordinates
-    // outside the screen's safe range: see the flag check below).
-    rc = run_exact(ix, Qs, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
-                   counters, status, st, fr, false, perm);
-    if (rc) return rc;
+    // Rows the screen could not certify (a list past capacity, too many
+    // candidates or survivors).  After a bf16 pass they get a second pass with
+    // the fp32 screen, whose bound is ~50x tighter; otherwise (and for rows the
+    // fp32 pass cannot certify) the exhaustive exact scan.
+    bool second_pass = false;
+    if (tc) {
+      int nfb = 0;
+      B2K_CUDA(cudaMemcpyAsync(&nfb, status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+      B2K_CUDA(cudaStreamSynchronize(st));
+      if (nfb > 0) {
+        float* Qfb = nullptr;
+        int* pfb = nullptr;
+        if ((rc = dalloc(&Qfb, (size_t)nfb * ix.d, st))) return rc;
+        fr.keep(Qfb);
+        if ((rc = dalloc(&pfb, (size_t)nfb, st))) return rc;
+        fr.keep(pfb);
+        launch_gather_fallback(Qs, ix.d, fb_list, perm, nfb, Qfb, pfb, st);
+        B2K_CUDA(cudaGetLastError());
+        b2k_stats sub{};
+        rc = knn_device_impl(ix, Qfb, nfb, k, exclude_self, q_offset, B2K_MODE_FP32, d_dist,
+                             d_idx, st, &sub, pfb);
+        if (rc) return rc;
+        second_pass_rows = nfb;
+        second_exact_rows = sub.fallback_rows;
+      }
+      second_pass = true;
+    }
+    if (!second_pass) {
+      rc = run_exact(ix, Qs, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
+                     counters, status, st, fr, false, perm);
+      if (rc) return rc;
+    }
   }
   if (stats) cudaEventRecord(ev[3], st);
   int hstatus[8];
@@ -428,6 +462,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   B2K_CUDA(cudaMemcpyAsync(hcnt, counters, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
   if (fm == 3) hstatus[0] = DEV_TIMEOUT_FULL;
+  if (hstatus[5]) return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
   if (hstatus[0] == DEV_TOO_MANY_TIES)
     return fail(B2K_EUNSUPPORTED,
                 "more than %d training rows tie (within float64 error) with a query's k-th "
@@ -438,14 +473,15 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   if (hstatus[4] & 1) {
     // Some query coordinate is outside the screens' safe range: redo exactly.
     return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, B2K_MODE_EXACT, d_dist, d_idx,
-                           st, stats);
+                           st, stats, ext_perm);
   }
   if (stats) {
     stats->splits = S;
     stats->candidates = (int64_t)hcnt[0];
     stats->list_entries = (int64_t)hcnt[1];
     stats->exact_compares = (int64_t)hcnt[2];
-    stats->fallback_rows = (int64_t)hcnt[3];
+    stats->fallback_rows = (int64_t)hcnt[3] + second_exact_rows;
+    stats->second_pass_rows = second_pass_rows;
     float ms = 0;
     if (mode != B2K_MODE_EXACT && cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess)
       stats->screen_ms = ms;
@@ -695,10 +731,7 @@ int b2k_knn(b2k_index* h, const float* Q, int64_t m, int32_t k, int32_t exclude_
     fr.keep(dd);
   }
   B2K_CUDA(cudaMemcpyAsync(dQ, Q, (size_t)m * ix.d * sizeof(float), cudaMemcpyHostToDevice, st));
-  // finiteness checked on the device after the upload (one pass over HBM)
-  bool finite = true;
-  if ((rc = device_finite(dQ, (size_t)m * ix.d, st, &finite))) return rc;
-  if (!finite) return fail(B2K_ENONFINITE, "training and query coordinates must be finite");
+  // finiteness is checked on the device inside the search (one pass over HBM)
   rc = knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, mode, dd, di, st, stats);
   if (rc) return rc;
   B2K_CUDA(cudaMemcpyAsync(idx, di, (size_t)m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, st));

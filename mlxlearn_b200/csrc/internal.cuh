@@ -126,6 +126,10 @@ void launch_pivots(Index* ix, cudaStream_t st);
 void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,
                         int* perm, float* Qp, cudaStream_t st);
 
+// second pass over uncertified rows: Qout[i] = Qs[rows[i]], pout[i] = perm[rows[i]]
+void launch_gather_fallback(const float* Qs, int d, const int* rows, const int* perm, int count,
+                            float* Qout, int* pout, cudaStream_t st);
+
 // -------------------------------------------------- certify + re-rank + exact
 struct CertifyArgs {
   const float* X;

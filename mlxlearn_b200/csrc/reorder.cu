@@ -125,7 +125,29 @@ __global__ void gather_rows_kernel(const float* __restrict__ Q, const int* __res
   for (int i = threadIdx.x & 31; i < d; i += 32) dst[i] = src[i];
 }
 
+// Rows the certify pass could not finish, for a second pass: their query
+// rows (in the pass's row order) and their output rows.
+__global__ void gather_fallback_kernel(const float* __restrict__ Qs, int d,
+                                       const int* __restrict__ rows,
+                                       const int* __restrict__ perm, int count,
+                                       float* __restrict__ Qout, int* __restrict__ pout) {
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (i >= count) return;
+  const int r = rows[i];
+  const float* src = Qs + (size_t)r * d;
+  float* dst = Qout + (size_t)i * d;
+  for (int c = threadIdx.x & 31; c < d; c += 32) dst[c] = src[c];
+  if ((threadIdx.x & 31) == 0) pout[i] = perm ? perm[r] : r;
+}
+
 }  // namespace
+
+void launch_gather_fallback(const float* Qs, int d, const int* rows, const int* perm, int count,
+                            float* Qout, int* pout, cudaStream_t st) {
+  if (count <= 0) return;
+  gather_fallback_kernel<<<(unsigned)((count + 7) / 8), 256, 0, st>>>(Qs, d, rows, perm, count,
+                                                                      Qout, pout);
+}
 
 int pivot_count(int64_t n) {
   int P = 512;

@@ -255,6 +255,45 @@ def test_non_finite_inputs_are_rejected():
         ix.query(Q, 3)
     with pytest.raises(ValueError, match="finite"):
         ix.query_radius_csr(Q, 1.0)
+    import torch
+
+    for mode in ("bf16", "fp32", "exact"):
+        with pytest.raises(ValueError, match="finite"):
+            ix.query_device(torch.from_numpy(Q).cuda(), 3, mode=mode)
     od, oi = oracle.knn(X, X[:50], 3)
     dist, idx = ix.query(X[:50], 3)
     np.testing.assert_array_equal(idx, oi)
+
+
+def test_uncertified_bf16_rows_get_an_fp32_second_pass():
+    # reference rows on the unit sphere with 1e-5 radial jitter, queries next
+    # to its centre: the squared distances spread ~2e-5 around 1, well inside
+    # the bf16 bound (~1e-4: bf16 operands, fp32 tensor-core accumulation of
+    # the norm column), so every row lands in the bf16 certify band and no
+    # query can be certified there; the fp32 bound (~2e-7) leaves a few
+    # candidates per query, so the fp32 pass certifies them without the
+    # exhaustive scan
+    rng = np.random.default_rng(41)
+    v = rng.standard_normal((4000, 32))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    X = (v * (1.0 + 1e-5 * rng.standard_normal((4000, 1)))).astype(np.float32)
+    Q = (1e-7 * rng.standard_normal((96, 32))).astype(np.float32)
+    od, oi = oracle.knn(X, Q, 40)
+    ix = make_index(X)
+    dist, idx = ix.query(Q, 40, mode="bf16", stats=True)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+    st = ix.last_stats
+    assert st["second_pass_rows"] > 0, st
+    assert st["fallback_rows"] == 0, st
+    # self-query: the second pass keeps each row's own index excluded
+    import torch
+
+    # (k = 60 > the 49 other near-centre rows, so the k-th lies on the sphere)
+    Xs = np.concatenate([Q[:50], X]).astype(np.float32)
+    ixs = make_index(Xs)
+    d2, i2 = ixs.query_device(torch.from_numpy(Xs[:50]).cuda(), 60, mode="bf16",
+                              exclude_self=True, q_offset=0, stats=True)
+    assert ixs.last_stats["second_pass_rows"] > 0, ixs.last_stats
+    o2d, o2i = oracle.knn(Xs, Xs[:50], 60, exclude_self=True)
+    np.testing.assert_array_equal(i2.cpu().numpy(), o2i)
