@@ -17,6 +17,16 @@
 //               columns (256 rows x 16, 32-byte swizzle) with the last block.
 //   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=256 K=16, fp32
 //               accumulators in TMEM, double-buffered (2 x 256 columns).
+//               It polls one mbarrier (go) per chunk of C = min(KB, stages/2)
+//               64-column blocks, i.e. once per tile for d <= 128: the thread
+//               issuing MMAs runs only about one MMA ahead of the tensor pipe,
+//               so every poll it makes idles the pipe; a poll per block plus
+//               one for the accumulator cost up to 2x in measured MMA
+//               throughput.
+//   last warp   gate: per chunk, waits for its TMA stages (at a tile's first
+//               chunk also for the epilogue's release of the accumulator
+//               buffer; at a unit's start for the query tile), then arrives
+//               on go.  A chunk never needs more stages than the ring holds.
 //   warps 2..   EW epilogue warps.  Warp w reads TMEM lane group w % 4 (the
 //               hardware's rule); the EW / 4 warps of a lane group take
 //               equal column ranges of each tile (16 warps for k <= 16, 8 for
@@ -174,7 +184,12 @@ constexpr uint32_t kATileBytes = kTcBM * kTcBK * 2;     // 16 KB per 64-column b
 constexpr uint32_t kBTileBytes = kTcBN * kTcBK * 2;     // 32 KB per 64-column block
 constexpr uint32_t kAAugBytes = kTcBM * kTcAug * 2;     // 4 KB (query ones)
 constexpr uint32_t kBAugBytes = kTcBN * kTcAug * 2;     // 8 KB (reference norms)
-constexpr int kSpillStride = 9;  // 8 spilled values per thread, conflict-free stride
+constexpr int kSpillStride = 9;
+// go barriers (gate -> MMA issuer), used in turn by successive chunks: the gate
+// runs at most `stages` chunks (each at least one stage) ahead of the MMA
+// issuer, so with more barriers than the deepest ring a barrier's next phase
+// never starts before the issuer has consumed the previous one.
+constexpr int kGoRing = 16;  // 8 spilled values per thread, conflict-free stride
 // A CTA allocates all 512 TMEM columns, so no two may share an SM: ask for at
 // least this much shared memory (more than half of the SM's 228 KB).
 constexpr size_t kMinCtaSmem = 116 * 1024;
@@ -186,7 +201,7 @@ __host__ __device__ inline uint32_t tc_stage_bytes(bool a_stream) {
 __host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream, int ew) {
   size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
   size_t spill = (size_t)ew * 32 * kSpillStride * sizeof(float);
-  size_t bars = (2 * (size_t)stages + 7 + 2 * kUnitRing) * sizeof(uint64_t) + 16 +
+  size_t bars = (2 * (size_t)stages + 7 + kGoRing + 2 * kUnitRing) * sizeof(uint64_t) + 16 +
                 kUnitRing * sizeof(int);
   return 1024 /*alignment slack*/ + kAAugBytes + a + (size_t)tc_stage_bytes(a_stream) * stages +
          spill + bars;
@@ -205,8 +220,11 @@ B2K_DEV uint64_t smem_desc_sw32(const void* smem_tile) {
   return desc;
 }
 
+// Threads per CTA: producer warp, MMA warp, EW epilogue warps, gate warp.
+__host__ __device__ constexpr int tc_block_threads(int ew) { return 96 + 32 * ew; }
+
 template <class Sink, bool A_STREAM, int EW, bool BATCH>
-__global__ void __launch_bounds__(64 + 32 * EW, 1)
+__global__ void __launch_bounds__(tc_block_threads(EW), 1)
     screen_tc_kernel(const __grid_constant__ TcMapSet<BATCH ? kBatchGroups : 1> maps,
                      const __grid_constant__ TcParams p) {
   constexpr int G = BATCH ? kBatchGroups : 1;
@@ -232,8 +250,9 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
   uint64_t* acc_full = a_empty + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2; // [2]
   uint64_t* aaug_full = acc_empty + 2;
+  uint64_t* go = aaug_full + 1;       // [kGoRing] gate -> MMA issuer, one per chunk in turn
   UnitRing ring;
-  ring.full = aaug_full + 1;           // [kUnitRing]
+  ring.full = go + kGoRing;            // [kUnitRing]
   ring.empty = ring.full + kUnitRing;  // [kUnitRing]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ring.empty + kUnitRing);
   ring.idx = reinterpret_cast<int*>(tmem_slot + 4);
@@ -248,15 +267,18 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(a_full, 1);
-    mbar_init(a_empty, 1);
+    // the query tile is free once its unit's MMAs are done (MMA commit) and
+    // its load has landed (gate; a unit may have no tiles at all)
+    mbar_init(a_empty, 2);
     mbar_init(&acc_full[0], 1);
     mbar_init(&acc_full[1], 1);
     mbar_init(&acc_empty[0], kEpiThreads);
     mbar_init(&acc_empty[1], kEpiThreads);
     mbar_init(aaug_full, 1);
+    for (int g = 0; g < kGoRing; ++g) mbar_init(&go[g], 1);
     for (int r = 0; r < kUnitRing; ++r) {
       mbar_init(&ring.full[r], 1);
-      mbar_init(&ring.empty[r], 1 + kEpiThreads);
+      mbar_init(&ring.empty[r], 2 + kEpiThreads);  // MMA issuer, gate, epilogue threads
     }
     fence_mbar_init();
   }
@@ -337,27 +359,27 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
-      uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0;
-      if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto mma_done;
+      uint32_t stage = 0, acc_it = 0, chunk = 0;
       {
         const uint64_t aaug_desc = smem_desc_sw32(aaug_smem);
         UnitCursor<BATCH> cur(p, ring, false);
         TcUnit x;
         while (cur.next(p, x)) {
           const int KB = x.pr->KB;
-          if (!A_STREAM) {
-            if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto mma_done;
-            a_phase ^= 1;
-            tc_fence_after();
-          }
+          const int C = max(1, min(KB, nst / 2));  // blocks per gated chunk
           for (int j = x.j0; j < x.j1; ++j) {
-            const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
-            if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto mma_done;
-            tc_fence_after();
+            const uint32_t buf = acc_it & 1;
             const uint32_t d_tmem = tmem_base + buf * kTcBN;
             for (int kb = 0; kb < KB; ++kb) {
-              if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto mma_done;
-              tc_fence_after();
+              if (kb % C == 0) {
+                // the chunk's operands are in shared memory (and, at kb 0, the
+                // accumulator is free)
+                if (!mbar_wait(&go[chunk % kGoRing], (chunk / kGoRing) & 1, status,
+                               DEV_TIMEOUT_ACC))
+                  goto mma_done;
+                ++chunk;
+                tc_fence_after();
+              }
               uint8_t* st = b_smem + (size_t)stage * stage_bytes;
               const uint8_t* a_tile = A_STREAM ? st : a_smem + kb * kATileBytes;
               const uint64_t adesc = smem_desc_sw128(a_tile);
@@ -370,10 +392,7 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
               if (kb == KB - 1)  // + ||y_x||^2 through the norm columns
                 mma_f16(d_tmem, aaug_desc, smem_desc_sw32(st + baug_off), idesc, 1);
               mma_commit(&empty[stage]);
-              if (++stage == (uint32_t)nst) {
-                stage = 0;
-                phase ^= 1;
-              }
+              if (++stage == (uint32_t)nst) stage = 0;
             }
             mma_commit(&acc_full[buf]);
             ++acc_it;
@@ -384,6 +403,44 @@ __global__ void __launch_bounds__(64 + 32 * EW, 1)
         }
       }
     mma_done:;
+    }
+  } else if (warp == 2 + EW) {
+    // --------------------------------------------------------------- gate
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0, chunk = 0;
+      if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto gate_done;
+      {
+        UnitCursor<BATCH> cur(p, ring, false);
+        TcUnit x;
+        while (cur.next(p, x)) {
+          const int KB = x.pr->KB;
+          const int C = max(1, min(KB, nst / 2));  // as the MMA issuer
+          if (!A_STREAM) {
+            if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto gate_done;
+            a_phase ^= 1;
+          }
+          for (int j = x.j0; j < x.j1; ++j) {
+            const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
+            // the epilogue has read this buffer's previous tile
+            if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto gate_done;
+            for (int kb = 0; kb < KB; ++kb) {
+              if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto gate_done;
+              if (++stage == (uint32_t)nst) {
+                stage = 0;
+                phase ^= 1;
+              }
+              if ((kb + 1) % C == 0 || kb + 1 == KB) {
+                mbar_arrive(&go[chunk % kGoRing]);
+                ++chunk;
+              }
+            }
+            ++acc_it;
+          }
+          // (not after the last unit, as with the MMA issuer's release)
+          if (!A_STREAM && cur.more()) mbar_arrive(a_empty);
+        }
+      }
+    gate_done:;
     }
   } else {
     // ----------------------------------------------------------- epilogue
@@ -521,7 +578,7 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
-  kern<<<grid, 64 + 32 * EW, smem, st>>>(maps, q);
+  kern<<<grid, tc_block_threads(EW), smem, st>>>(maps, q);
   return (int)cudaGetLastError();
 }
 
