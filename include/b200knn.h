@@ -179,6 +179,41 @@ B2K_API int b2k_class_votes(const int64_t *d_idx, const double *d_dist, int64_t 
                             const int32_t *d_codes, int32_t n_classes, int32_t weighted,
                             double *d_votes, int64_t *d_pred, void *stream);
 
+/* ------------------------------------------------------ reference-row shards
+ * One rank per GPU holds a contiguous range of the fitted rows (its own
+ * index) and answers the same query batch with its exact top-k_in, indices
+ * made global (row + offset; -1 where the shard has fewer rows).  After one
+ * exchange every rank holds d_dist / d_idx [n_shards, m, k_in] (shard
+ * order) and merges them into the answer over all rows; the reference has
+ * no multi-device path, so there is no counterpart to cite, and the merged
+ * answer follows the neighbour order of one index over all rows
+ * (src/mlxlearn/_kernels/_neighbors_cpu_native.cpp:170-190).
+ *
+ * b2k_shard_merge: out [m, k] from the float64 distances and global rows;
+ * self_offset >= 0 drops global row self_offset + r from query r's answer
+ * (the shards then search k_in = k + 1 without exclusion).  d_flags[r] = 1
+ * marks queries whose shards' candidates lie within each other's float64
+ * error interval: for those, every rank calls b2k_shard_keys (exact 640-bit
+ * keys of the candidates its own index holds, into a zeroed
+ * [n_flagged, n_shards * k_in, 10] buffer), the buffers are summed across
+ * ranks (each entry has one owner), and b2k_shard_resolve rewrites those
+ * rows in the exact order.  d_flagged lists the flagged queries ascending,
+ * the same on every rank.  1 <= n_shards <= 16, 1 <= k <= 256,
+ * k <= k_in <= k + 1.  Stream-ordered, no synchronisation. */
+B2K_API int b2k_shard_merge(const double *d_dist, const int64_t *d_idx, int32_t n_shards,
+                            int64_t m, int32_t k_in, int32_t k, int32_t d, int64_t self_offset,
+                            double *d_out_dist, int64_t *d_out_idx, int32_t *d_flags,
+                            void *stream);
+B2K_API int b2k_shard_keys(b2k_index *index, int64_t row_offset, const float *dQ,
+                           const int64_t *d_idx, int32_t n_shards, int64_t m, int32_t k_in,
+                           const int64_t *d_flagged, int64_t n_flagged, uint64_t *d_keys,
+                           void *stream);
+B2K_API int b2k_shard_resolve(const double *d_dist, const int64_t *d_idx, int32_t n_shards,
+                              int64_t m, int32_t k_in, int32_t k, int64_t self_offset,
+                              const int64_t *d_flagged, int64_t n_flagged,
+                              const uint64_t *d_keys, double *d_out_dist, int64_t *d_out_idx,
+                              void *stream);
+
 /* ---------------------------------------------------------------- batches */
 
 /* One independent kNN problem of a batch: a fitted index and a device query

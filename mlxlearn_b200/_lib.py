@@ -105,6 +105,12 @@ SIGNATURES = {
     "b2k_knn_segments": (ctypes.c_int, [_vp, _vp, _i32, _vp, _vp, _i32, _i32, _i32, _vp, _vp,
                                         _vp]),
     "b2k_class_votes": (ctypes.c_int, [_vp, _vp, _i64, _i32, _vp, _i32, _i32, _vp, _vp, _vp]),
+    "b2k_shard_merge": (ctypes.c_int, [_vp, _vp, _i32, _i64, _i32, _i32, _i32, _i64, _vp, _vp,
+                                       _vp, _vp]),
+    "b2k_shard_keys": (ctypes.c_int, [_vp, _i64, _vp, _vp, _i32, _i64, _i32, _vp, _i64, _vp,
+                                      _vp]),
+    "b2k_shard_resolve": (ctypes.c_int, [_vp, _vp, _i32, _i64, _i32, _i32, _i64, _vp, _i64, _vp,
+                                         _vp, _vp, _vp]),
     "b2k_radius": (ctypes.c_int, [_vp, _vp, _i64, _dbl, _i32, _i64, _i32, _i32,
                                   ctypes.POINTER(_vp)]),
     "b2k_radius_result_nnz": (ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),

@@ -1048,6 +1048,80 @@ int b2k_class_votes(const int64_t* d_idx, const double* d_dist, int64_t m, int32
   return B2K_OK;
 }
 
+// -------------------------------------------------------------- row shards
+// Relative bound on |canonical distance - exact distance|: the canonical
+// squared value is within g = (d+2)u/(1-(d+2)u) of the exact one (u = 2^-53),
+// its square root adds half of that plus one rounding; 2g + 4u is generous.
+static double shard_eps(int d) {
+  const double u = 0x1p-53;
+  const double g = (d + 2) * u / (1.0 - (d + 2) * u);
+  return 2 * g + 4 * u;
+}
+
+static int check_shard_shapes(int32_t n_shards, int64_t m, int32_t k_in, int32_t k) {
+  if (n_shards < 1 || n_shards > kMaxShards)
+    return fail(B2K_EINVAL, "shard count must be in [1, %d], got %d", kMaxShards, n_shards);
+  if (m < 0) return fail(B2K_EINVAL, "query count must be non-negative");
+  if (k < 1 || k > kMaxShardK || k_in < k || k_in > kMaxShardK + 1)
+    return fail(B2K_EINVAL, "shard merge needs 1 <= k <= %d and k <= k_in <= k + 1, got k=%d k_in=%d",
+                kMaxShardK, k, k_in);
+  return B2K_OK;
+}
+
+int b2k_shard_merge(const double* d_dist, const int64_t* d_idx, int32_t n_shards, int64_t m,
+                    int32_t k_in, int32_t k, int32_t d, int64_t self_offset, double* d_out_dist,
+                    int64_t* d_out_idx, int32_t* d_flags, void* stream) {
+  int rc = check_shard_shapes(n_shards, m, k_in, k);
+  if (rc) return rc;
+  if (d < 1) return fail(B2K_EINVAL, "feature count must be positive");
+  if (m == 0) return B2K_OK;
+  if (!d_dist || !d_idx || !d_out_dist || !d_out_idx || !d_flags)
+    return fail(B2K_EINVAL, "device pointers must not be NULL");
+  launch_shard_merge(d_dist, d_idx, n_shards, m, k_in, k, self_offset, shard_eps(d), d_out_dist,
+                     d_out_idx, d_flags, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(B2K_ECUDA, "shard merge launch failed: %s", cudaGetErrorString(e));
+  return B2K_OK;
+}
+
+int b2k_shard_keys(b2k_index* h, int64_t row_lo, const float* dQ, const int64_t* d_idx,
+                   int32_t n_shards, int64_t m, int32_t k_in, const int64_t* d_flagged,
+                   int64_t n_flagged, uint64_t* d_keys, void* stream) {
+  if (!h) return fail(B2K_EINVAL, "index must not be NULL");
+  int rc = check_shard_shapes(n_shards, m, k_in, k_in > 1 ? k_in - 1 : 1);
+  if (rc) return rc;
+  if (row_lo < 0) return fail(B2K_EINVAL, "row offset must be non-negative");
+  if (n_flagged < 0 || n_flagged > m) return fail(B2K_EINVAL, "invalid flagged query count");
+  if (n_flagged == 0) return B2K_OK;
+  if (!dQ || !d_idx || !d_flagged || !d_keys)
+    return fail(B2K_EINVAL, "device pointers must not be NULL");
+  Index& ix = h->ix;
+  B2K_CUDA(cudaSetDevice(ix.device));
+  launch_shard_keys(nullptr, d_idx, n_shards, m, k_in, dQ, ix.X, ix.n, ix.d, row_lo, d_flagged,
+                    n_flagged, d_keys, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(B2K_ECUDA, "shard keys launch failed: %s", cudaGetErrorString(e));
+  return B2K_OK;
+}
+
+int b2k_shard_resolve(const double* d_dist, const int64_t* d_idx, int32_t n_shards, int64_t m,
+                      int32_t k_in, int32_t k, int64_t self_offset, const int64_t* d_flagged,
+                      int64_t n_flagged, const uint64_t* d_keys, double* d_out_dist,
+                      int64_t* d_out_idx, void* stream) {
+  int rc = check_shard_shapes(n_shards, m, k_in, k);
+  if (rc) return rc;
+  if (n_flagged < 0 || n_flagged > m) return fail(B2K_EINVAL, "invalid flagged query count");
+  if (n_flagged == 0) return B2K_OK;
+  if (!d_dist || !d_idx || !d_flagged || !d_keys || !d_out_dist || !d_out_idx)
+    return fail(B2K_EINVAL, "device pointers must not be NULL");
+  launch_shard_resolve(d_dist, d_idx, n_shards, m, k_in, k, self_offset, d_flagged, n_flagged,
+                       d_keys, d_out_dist, d_out_idx, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(B2K_ECUDA, "shard resolve launch failed: %s", cudaGetErrorString(e));
+  return B2K_OK;
+}
+
 int b2k_radius_result_class_votes(const b2k_radius_result* res, const int32_t* d_codes,
                                   int32_t n_classes, int32_t weighted, double* d_votes,
                                   int64_t* d_counts, void* stream) {

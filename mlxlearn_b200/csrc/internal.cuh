@@ -20,6 +20,8 @@ constexpr int kListCap = 512;      // screen list entries per (split, query)
 constexpr int kCertifyCap = 1024;  // re-rank candidates per query held in shared memory
 constexpr int kExactCap = 4096;    // exhaustive-scan candidates per query
 constexpr int kMaxK = 64;          // largest k the screens track in registers
+constexpr int kMaxShards = 16;     // reference-row shards one merge takes
+constexpr int kMaxShardK = 256;    // largest k of a shard merge
 
 // Outputs of a screen kernel: per (split, query) a list of (v, column)
 // candidates, the list length (may exceed cap = overflow), and the k smallest
@@ -227,6 +229,17 @@ int report_error(int code, const char* msg);  // sets b2k_last_error(), returns 
 int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
                    int64_t q_offset);
 Index* index_of(b2k_index* h);
+
+// ------------------------------------------------------------ row shards
+void launch_shard_merge(const double* D, const int64_t* I, int S, int64_t m, int kin, int kout,
+                        int64_t self_offset, double eps, double* out_d, int64_t* out_i,
+                        int32_t* flags, cudaStream_t st);
+void launch_shard_keys(const double* D, const int64_t* I, int S, int64_t m, int kin,
+                       const float* Q, const float* X, int64_t n_local, int d, int64_t row_lo,
+                       const int64_t* flagged, int64_t F, uint64_t* keys, cudaStream_t st);
+void launch_shard_resolve(const double* D, const int64_t* I, int S, int64_t m, int kin, int kout,
+                          int64_t self_offset, const int64_t* flagged, int64_t F,
+                          const uint64_t* keys, double* out_d, int64_t* out_i, cudaStream_t st);
 // knn on device pointers (b2k_knn_device without the stats), synchronises st
 int knn_device_run(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
                    int64_t q_offset, int mode, double* d_dist, int64_t* d_idx, cudaStream_t st);

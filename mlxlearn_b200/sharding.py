@@ -1,13 +1,18 @@
-"""Multi-GPU kneighbors: index replicas, query shards, max-over-ranks timing.
+"""Multi-GPU kneighbors: query shards over index replicas, or reference-row
+shards with an exact merge; max-over-ranks timing.
 
-One process per GPU (torchrun).  Every rank holds a full replica of the
-fitted rows; a query batch is cut into contiguous shards, one per rank, and
-each rank answers its shard with no collective on the data path.  The only
-exchanges are host plumbing around the search: the training rows are
-broadcast once from the rank that holds them, and the per-shard answers are
-gathered back in query order.  The reference has no multi-device path; this
-module only partitions the work the single-device entry points already do,
-so answers are identical to one ``kneighbors`` over the whole batch.
+One process per GPU (torchrun).  Query shards: every rank holds a full
+replica of the fitted rows; a query batch is cut into contiguous shards, one
+per rank, and each rank answers its shard with no collective on the data
+path (the training rows are broadcast once, the answers gathered back in
+query order).  Row shards (``kneighbors_row_sharded``): every rank holds a
+contiguous range of the fitted rows and answers the whole batch with its own
+exact top-k; one all-gather of those lists (16 bytes per candidate) and a
+device merge give the answer over all rows, with exact 640-bit keys
+exchanged only for the rare queries whose candidates from different shards
+sit within float64 rounding of each other.  The reference has no
+multi-device path; both forms return exactly what one ``kneighbors`` over
+the whole batch and all rows returns.
 
 All exchanges go through ``torch.distributed`` on whatever backend the
 caller initialised (NCCL on GPUs, gloo on CPU); tensors are moved to the
@@ -20,7 +25,7 @@ from typing import Callable, Optional, Tuple
 import numpy as np
 
 __all__ = ["shard_bounds", "broadcast_rows", "max_over_ranks", "kneighbors_sharded",
-           "ShardTimer"]
+           "kneighbors_row_sharded", "merge_row_shards", "RowShardOps", "ShardTimer"]
 
 _DTYPES = {0: np.float32, 1: np.float64, 2: np.int64, 3: np.int32}
 _CODES = {np.dtype(v): k for k, v in _DTYPES.items()}
@@ -139,6 +144,156 @@ def kneighbors_sharded(query: Callable[[np.ndarray, int, int], Tuple[np.ndarray,
     if not gather:
         return d, i, a
     return _gather_rows(d, m, world, k, np.float64), _gather_rows(i, m, world, k, np.int64)
+
+
+class RowShardOps:
+    """The device steps of a row-shard query, through the CUDA library.
+
+    Tensors are CUDA tensors on the current device; every step runs on the
+    current torch stream.  (Tests swap in a CPU restatement to check the
+    exchange protocol on gloo ranks.)"""
+
+    def search(self, index, Q, k):
+        """This shard's exact top-k of every query: float64 [m, k], int64 [m, k]."""
+        return index.query_device(Q, k)
+
+    def merge(self, D, I, k, d, self_offset):
+        import torch
+
+        from . import _lib
+
+        S, m, k_in = I.shape
+        out_d = torch.empty((m, k), dtype=torch.float64, device=I.device)
+        out_i = torch.empty((m, k), dtype=torch.int64, device=I.device)
+        flags = torch.empty((m,), dtype=torch.int32, device=I.device)
+        st = torch.cuda.current_stream(I.device).cuda_stream
+        _lib.check(_lib.load().b2k_shard_merge(D.data_ptr(), I.data_ptr(), S, m, k_in, k, d,
+                                               self_offset, out_d.data_ptr(), out_i.data_ptr(),
+                                               flags.data_ptr(), st), "b2k_shard_merge")
+        return out_d, out_i, flags
+
+    def keys(self, index, row_offset, Q, I, flagged, keys):
+        import torch
+
+        from . import _lib
+
+        S, m, k_in = I.shape
+        st = torch.cuda.current_stream(I.device).cuda_stream
+        _lib.check(_lib.load().b2k_shard_keys(index._ensure_device(), row_offset, Q.data_ptr(),
+                                              I.data_ptr(), S, m, k_in, flagged.data_ptr(),
+                                              flagged.numel(), keys.data_ptr(), st),
+                   "b2k_shard_keys")
+
+    def resolve(self, D, I, k, self_offset, flagged, keys, out_d, out_i):
+        import torch
+
+        from . import _lib
+
+        S, m, k_in = I.shape
+        st = torch.cuda.current_stream(I.device).cuda_stream
+        _lib.check(_lib.load().b2k_shard_resolve(D.data_ptr(), I.data_ptr(), S, m, k_in, k,
+                                                 self_offset, flagged.data_ptr(), flagged.numel(),
+                                                 keys.data_ptr(), out_d.data_ptr(),
+                                                 out_i.data_ptr(), st), "b2k_shard_resolve")
+
+
+_KEY_LIMBS = 10
+
+
+def _shard_lists(index, row_offset, Q, k_in, ops):
+    """One shard's answer padded to k_in columns, rows made global (-1 = none)."""
+    import torch
+
+    n = int(index.n_samples)
+    m = int(Q.shape[0])
+    D = torch.full((m, k_in), float("inf"), dtype=torch.float64, device=Q.device)
+    I = torch.full((m, k_in), -1, dtype=torch.int64, device=Q.device)
+    kl = min(k_in, n)
+    if kl > 0 and m > 0:
+        d, i = ops.search(index, Q, kl)
+        D[:, :kl] = d
+        I[:, :kl] = i + row_offset
+    return D, I
+
+
+def _check_row_shard_args(k, n_total, exclude_self, q_offset, m):
+    limit = n_total - (1 if exclude_self else 0)
+    if k < 1:
+        raise ValueError(f"Expected n_neighbors > 0. Got {k}")
+    if k > limit:
+        raise ValueError(f"n_neighbors must be <= {limit}, got {k}.")
+    if exclude_self and (q_offset < 0 or q_offset + m > n_total):
+        raise ValueError("exclude_self requires the query matrix to be the training matrix")
+
+
+def merge_row_shards(parts, Q, k: int, *, exclude_self: bool = False, q_offset: int = 0,
+                     ops: Optional[RowShardOps] = None):
+    """The row-shard answer with every shard in this process.
+
+    ``parts`` lists ``(index, row_offset)`` in row order: index ``s`` holds
+    global rows ``[row_offset, row_offset + index.n_samples)``.  Returns float64
+    distances and int64 global rows [m, k], identical to one search over all
+    rows.  The same merge as ``kneighbors_row_sharded``, with stacking in
+    place of the collectives."""
+    import torch
+
+    ops = ops or RowShardOps()
+    n_total = sum(int(ix.n_samples) for ix, _ in parts)
+    m, d = int(Q.shape[0]), int(Q.shape[1])
+    _check_row_shard_args(k, n_total, exclude_self, q_offset, m)
+    k_in = k + (1 if exclude_self else 0)
+    lists = [_shard_lists(ix, off, Q, k_in, ops) for ix, off in parts]
+    D = torch.stack([a for a, _ in lists])
+    I = torch.stack([b for _, b in lists])
+    self_offset = q_offset if exclude_self else -1
+    out_d, out_i, flags = ops.merge(D, I, k, d, self_offset)
+    flagged = torch.nonzero(flags).flatten().to(torch.int64)
+    if flagged.numel():
+        keys = torch.zeros((flagged.numel(), len(parts) * k_in, _KEY_LIMBS), dtype=torch.int64,
+                           device=I.device)
+        for ix, off in parts:
+            ops.keys(ix, off, Q, I, flagged, keys)
+        ops.resolve(D, I, k, self_offset, flagged, keys, out_d, out_i)
+    return out_d, out_i
+
+
+def kneighbors_row_sharded(index, row_offset: int, n_total: int, Q, k: int, *,
+                           exclude_self: bool = False, q_offset: int = 0,
+                           ops: Optional[RowShardOps] = None):
+    """Answer ``Q`` over rows spread across the ranks.
+
+    Rank ``r`` passes its own ``index`` over global rows
+    ``[row_offset, row_offset + index.n_samples)`` (ranks hold consecutive ranges in
+    rank order, together ``n_total`` rows) and the same query tensor ``Q``
+    as every other rank.  Every rank returns the float64 distances and int64
+    global rows [m, k] of one search over all rows.  Collectives: one
+    all-gather of each rank's [m, k] lists, plus one all-reduce of exact keys
+    when some query has candidates from different shards within float64
+    rounding of each other (every rank takes the same branch)."""
+    import torch
+    import torch.distributed as dist
+
+    ops = ops or RowShardOps()
+    world = dist.get_world_size()
+    m, d = int(Q.shape[0]), int(Q.shape[1])
+    _check_row_shard_args(k, n_total, exclude_self, q_offset, m)
+    k_in = k + (1 if exclude_self else 0)
+    D_s, I_s = _shard_lists(index, row_offset, Q, k_in, ops)
+    Ds = [torch.empty_like(D_s) for _ in range(world)]
+    Is = [torch.empty_like(I_s) for _ in range(world)]
+    dist.all_gather(Ds, D_s.contiguous())
+    dist.all_gather(Is, I_s.contiguous())
+    D, I = torch.stack(Ds), torch.stack(Is)
+    self_offset = q_offset if exclude_self else -1
+    out_d, out_i, flags = ops.merge(D, I, k, d, self_offset)
+    flagged = torch.nonzero(flags).flatten().to(torch.int64)
+    if flagged.numel():  # the same on every rank: the inputs are
+        keys = torch.zeros((flagged.numel(), world * k_in, _KEY_LIMBS), dtype=torch.int64,
+                           device=I.device)
+        ops.keys(index, row_offset, Q, I, flagged, keys)
+        dist.all_reduce(keys)  # each entry has exactly one owner
+        ops.resolve(D, I, k, self_offset, flagged, keys, out_d, out_i)
+    return out_d, out_i
 
 
 class ShardTimer:

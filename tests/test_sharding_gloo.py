@@ -114,7 +114,33 @@ def _case_timer(rank, world):
     assert ms >= 45.0, ms
 
 
-_CASES = {"knn": _case_knn, "self": _case_self, "tiny": _case_tiny, "timer": _case_timer}
+def _case_rows(rank, world):
+    # reference-row shards: each rank holds its own rows; one all-gather of the
+    # per-shard lists plus the exact-key all-reduce give the all-rows answer
+    import torch
+
+    import oracle
+    from _row_shards_cpu import CpuRowShardOps, CpuShard, planted_rows
+    from mlxlearn_b200.sharding import kneighbors_row_sharded
+
+    rng = np.random.default_rng(21)
+    X, bounds = planted_rows(rng, 900, 5, world)
+    Q = np.concatenate([rng.standard_normal((40, 5)), X[:8] + 1e-3, X[:4]]).astype(np.float32)
+    a, b = int(bounds[rank]), int(bounds[rank + 1])
+    d, i = kneighbors_row_sharded(CpuShard(X[a:b]), a, X.shape[0], torch.from_numpy(Q), 6,
+                                  ops=CpuRowShardOps())
+    od, oi = oracle.knn(X, Q, 6, nthreads=2)
+    assert np.array_equal(i.numpy(), oi)
+    assert np.array_equal(d.numpy(), od)
+    # self-query over the sharded rows
+    d, i = kneighbors_row_sharded(CpuShard(X[a:b]), a, X.shape[0], torch.from_numpy(X[:30]), 4,
+                                  exclude_self=True, q_offset=0, ops=CpuRowShardOps())
+    od, oi = oracle.knn(X, X[:30], 4, exclude_self=True, nthreads=2)
+    assert np.array_equal(i.numpy(), oi) and np.array_equal(d.numpy(), od)
+
+
+_CASES = {"knn": _case_knn, "self": _case_self, "tiny": _case_tiny, "timer": _case_timer,
+          "rows": _case_rows}
 
 
 def _run(case, world=2):
@@ -157,6 +183,6 @@ def test_shard_bounds_rejects_bad_rank():
         shard_bounds(-1, 2, 0)
 
 
-@pytest.mark.parametrize("case", ["knn", "self", "tiny", "timer"])
+@pytest.mark.parametrize("case", ["knn", "self", "tiny", "timer", "rows"])
 def test_gloo_two_ranks(case):
     _run(case)
