@@ -25,7 +25,8 @@ from typing import Callable, Optional, Tuple
 import numpy as np
 
 __all__ = ["shard_bounds", "broadcast_rows", "max_over_ranks", "kneighbors_sharded",
-           "kneighbors_row_sharded", "merge_row_shards", "RowShardOps", "ShardTimer"]
+           "kneighbors_row_sharded", "merge_row_shards", "radius_neighbors_row_sharded",
+           "merge_radius_row_shards", "RowShardOps", "ShardTimer"]
 
 _DTYPES = {0: np.float32, 1: np.float64, 2: np.int64, 3: np.int32}
 _CODES = {np.dtype(v): k for k, v in _DTYPES.items()}
@@ -294,6 +295,94 @@ def kneighbors_row_sharded(index, row_offset: int, n_total: int, Q, k: int, *,
         dist.all_reduce(keys)  # each entry has exactly one owner
         ops.resolve(D, I, k, self_offset, flagged, keys, out_d, out_i)
     return out_d, out_i
+
+
+def _local_radius(index, Q, radius, need_distance, sort_results):
+    from .radius_result import concatenate
+
+    return concatenate(index.query_radius_csr(Q, radius, need_distance=need_distance,
+                                              sort_results=sort_results))
+
+
+def _radius_part(index, row_offset, Q, radius, need, exclude_self, q_offset, local):
+    """One shard's entries as (query row, global row, distance) arrays."""
+    part = (local or _local_radius)(index, Q, radius, need, False)
+    rows = part.row_ids()
+    idx = np.asarray(part.indices, dtype=np.int64) + int(row_offset)
+    dd = (np.asarray(part.distances, dtype=np.float64) if need
+          else np.zeros(len(idx), np.float64))
+    if exclude_self:
+        keep = idx != rows + int(q_offset)
+        rows, idx, dd = rows[keep], idx[keep], dd[keep]
+    return rows, idx, dd
+
+
+def _assemble_radius(rows, idx, dd, m, sort_results, return_distance):
+    """Per query row: ascending global index, or (float64 distance, index) --
+    the single-index path's sort key, so the result is identical."""
+    from .radius_result import RadiusCSR
+
+    order = np.lexsort((idx, dd, rows)) if sort_results else np.lexsort((idx, rows))
+    indptr = np.zeros(m + 1, np.int64)
+    np.cumsum(np.bincount(rows, minlength=m), out=indptr[1:])
+    return RadiusCSR(indptr, idx[order], dd[order] if return_distance else None)
+
+
+def merge_radius_row_shards(parts, Q: np.ndarray, radius: float, *, return_distance: bool = True,
+                            sort_results: bool = False, exclude_self: bool = False,
+                            q_offset: int = 0, local: Optional[Callable] = None):
+    """``radius_neighbors_row_sharded`` with every shard in this process:
+    ``parts`` lists ``(index, row_offset)``."""
+    Q = np.ascontiguousarray(Q, dtype=np.float32)
+    need = bool(return_distance or sort_results)
+    got = [_radius_part(ix, off, Q, radius, need, exclude_self, q_offset, local)
+           for ix, off in parts]
+    return _assemble_radius(np.concatenate([g[0] for g in got]),
+                            np.concatenate([g[1] for g in got]),
+                            np.concatenate([g[2] for g in got]), int(Q.shape[0]), sort_results,
+                            return_distance)
+
+
+def radius_neighbors_row_sharded(index, row_offset: int, Q: np.ndarray, radius: float, *,
+                                 return_distance: bool = True, sort_results: bool = False,
+                                 exclude_self: bool = False, q_offset: int = 0,
+                                 local: Optional[Callable] = None):
+    """Radius neighbourhoods over rows spread across the ranks, as one CSR.
+
+    Rank ``r`` passes its own ``index`` over global rows
+    ``[row_offset, row_offset + index.n_samples)`` and the same host query
+    array ``Q``.  Every rank returns the ``RadiusCSR`` of one search over all
+    rows: each rank answers with its rows (global indices), the per-rank
+    entries are all-gathered (counts first, then padded arrays), and each
+    query row is reassembled in ascending global index, or in (float64
+    distance, index) order with ``sort_results``.  With ``exclude_self``
+    query row ``j`` drops global row ``q_offset + j``.
+    ``local(index, Q, radius, need_distance, sort_results)`` replaces the
+    local search (default: ``index.query_radius_csr``)."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size()
+    dev = _device_for(dist)
+    Q = np.ascontiguousarray(Q, dtype=np.float32)
+    need = bool(return_distance or sort_results)
+    rows, idx, dd = _radius_part(index, row_offset, Q, radius, need, exclude_self, q_offset,
+                                 local)
+    cnt = torch.tensor([len(idx)], dtype=torch.int64, device=dev)
+    cnts = [torch.empty_like(cnt) for _ in range(world)]
+    dist.all_gather(cnts, cnt)
+    sizes = [int(c.item()) for c in cnts]
+    width = max(max(sizes), 1)
+    payload = np.zeros((3, width), np.float64)  # rows and indices exact below 2^53
+    payload[0, :len(idx)] = rows
+    payload[1, :len(idx)] = idx
+    payload[2, :len(idx)] = dd
+    mine = torch.from_numpy(payload).to(dev)
+    bufs = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(bufs, mine)
+    allp = np.concatenate([b.cpu().numpy()[:, :sz] for b, sz in zip(bufs, sizes)], axis=1)
+    return _assemble_radius(allp[0].astype(np.int64), allp[1].astype(np.int64), allp[2],
+                            int(Q.shape[0]), sort_results, return_distance)
 
 
 class ShardTimer:

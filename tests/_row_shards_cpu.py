@@ -121,3 +121,11 @@ def planted_rows(rng, n, d, n_shards):
     last = bounds[-2]
     X[last:last + 20] = X[:20]
     return X, bounds
+
+
+def oracle_radius_local(shard, Q, radius, need_distance, sort_results):
+    """The oracle's radius search over a shard's rows, as a RadiusCSR."""
+    from mlxlearn_b200.radius_result import RadiusCSR
+
+    ip, ii, dd = oracle.radius(shard.X, Q, radius, sort_results=sort_results, nthreads=2)
+    return RadiusCSR(ip, ii, dd if need_distance else None)

@@ -61,3 +61,27 @@ def test_row_shards_reject_bad_k():
         merge_row_shards(parts, torch.zeros((1, 2)), 11, ops=CpuRowShardOps())
     with pytest.raises(ValueError, match="n_neighbors must be <= 9"):
         merge_row_shards(parts, torch.zeros((10, 2)), 10, exclude_self=True, ops=CpuRowShardOps())
+
+
+@pytest.mark.parametrize("sort_results", [False, True])
+def test_radius_row_shards_equal_one_search(sort_results):
+    from _row_shards_cpu import oracle_radius_local
+    from mlxlearn_b200.sharding import merge_radius_row_shards
+
+    rng = np.random.default_rng(70)
+    X, bounds = planted_rows(rng, 2000, 3, 3)
+    Q = np.concatenate([rng.standard_normal((50, 3)), X[:10]]).astype(np.float32)
+    parts = [(CpuShard(X[a:b]), int(a)) for a, b in zip(bounds[:-1], bounds[1:])]
+    res = merge_radius_row_shards(parts, Q, 0.6, sort_results=sort_results,
+                                  local=oracle_radius_local)
+    ip, ii, dd = oracle.radius(X, Q, 0.6, sort_results=sort_results)
+    np.testing.assert_array_equal(res.indptr, ip)
+    np.testing.assert_array_equal(res.indices, ii)
+    np.testing.assert_array_equal(res.distances, dd)
+    # self-query: every row drops its own global index
+    res = merge_radius_row_shards(parts, X[:100], 0.6, exclude_self=True, q_offset=0,
+                                  sort_results=sort_results, local=oracle_radius_local)
+    ip, ii, dd = oracle.radius(X, X[:100], 0.6, exclude_self=True, sort_results=sort_results)
+    np.testing.assert_array_equal(res.indptr, ip)
+    np.testing.assert_array_equal(res.indices, ii)
+    np.testing.assert_array_equal(res.distances, dd)

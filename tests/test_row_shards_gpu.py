@@ -89,3 +89,23 @@ def test_row_shards_self_query():
     np.testing.assert_array_equal(i.cpu().numpy(), oi)
     np.testing.assert_array_equal(d.cpu().numpy(), od)
     assert not np.any(i.cpu().numpy() == np.arange(600)[:, None])
+
+
+@pytest.mark.parametrize("sort_results", [False, True])
+def test_radius_row_shards_equal_one_search(sort_results):
+    from mlxlearn_b200.sharding import merge_radius_row_shards
+
+    rng = np.random.default_rng(80)
+    X, bounds = planted_rows(rng, 20000, 8, 3)
+    Q = np.concatenate([rng.standard_normal((300, 8)), X[:20]]).astype(np.float32)
+    res = merge_radius_row_shards(_parts(X, bounds), Q, 1.4, sort_results=sort_results)
+    ip, ii, dd = oracle.radius(X, Q, 1.4, sort_results=sort_results)
+    np.testing.assert_array_equal(res.indptr, ip)
+    np.testing.assert_array_equal(res.indices, ii)
+    np.testing.assert_array_equal(res.distances, dd)
+    res = merge_radius_row_shards(_parts(X, bounds), X[:500], 1.4, exclude_self=True,
+                                  q_offset=0, sort_results=sort_results)
+    ip, ii, dd = oracle.radius(X, X[:500], 1.4, exclude_self=True, sort_results=sort_results)
+    np.testing.assert_array_equal(res.indptr, ip)
+    np.testing.assert_array_equal(res.indices, ii)
+    np.testing.assert_array_equal(res.distances, dd)

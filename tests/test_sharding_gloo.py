@@ -139,8 +139,29 @@ def _case_rows(rank, world):
     assert np.array_equal(i.numpy(), oi) and np.array_equal(d.numpy(), od)
 
 
+def _case_radius_rows(rank, world):
+    import oracle
+    from _row_shards_cpu import CpuShard, oracle_radius_local, planted_rows
+    from mlxlearn_b200.sharding import radius_neighbors_row_sharded
+
+    rng = np.random.default_rng(22)
+    X, bounds = planted_rows(rng, 1500, 3, world)
+    Q = np.concatenate([rng.standard_normal((30, 3)), X[:6]]).astype(np.float32)
+    a, b = int(bounds[rank]), int(bounds[rank + 1])
+    for sort_results in (False, True):
+        res = radius_neighbors_row_sharded(CpuShard(X[a:b]), a, Q, 0.7,
+                                           sort_results=sort_results, local=oracle_radius_local)
+        ip, ii, dd = oracle.radius(X, Q, 0.7, sort_results=sort_results, nthreads=2)
+        assert np.array_equal(res.indptr, ip) and np.array_equal(res.indices, ii)
+        assert np.array_equal(res.distances, dd)
+    # a rank with no entries for any query still joins both gathers
+    res = radius_neighbors_row_sharded(CpuShard(X[a:b]), a, Q + 100.0, 0.1,
+                                       local=oracle_radius_local)
+    assert res.nnz == 0 and res.indptr.shape == (Q.shape[0] + 1,)
+
+
 _CASES = {"knn": _case_knn, "self": _case_self, "tiny": _case_tiny, "timer": _case_timer,
-          "rows": _case_rows}
+          "rows": _case_rows, "radius_rows": _case_radius_rows}
 
 
 def _run(case, world=2):
@@ -183,6 +204,6 @@ def test_shard_bounds_rejects_bad_rank():
         shard_bounds(-1, 2, 0)
 
 
-@pytest.mark.parametrize("case", ["knn", "self", "tiny", "timer", "rows"])
+@pytest.mark.parametrize("case", ["knn", "self", "tiny", "timer", "rows", "radius_rows"])
 def test_gloo_two_ranks(case):
     _run(case)
