@@ -66,6 +66,10 @@ struct RowTracker {
     cap = cap_;
     shared = shared_word;
     dirty = false;
+    // start from the k-th value other lists of this query already published
+    // (earlier reference splits run first): this list then skips most of its
+    // own fill phase, k (1 + ln(n / k)) admissions above the final band
+    sync_shared();
   }
 
   B2K_DEV void update_threshold() { T = __fadd_ru(fminf(kv[KMAX - 1], shared_kth), E2); }
@@ -200,6 +204,7 @@ struct LazyTracker {
     trig = cap_ - 32;
     shared = active_ ? shared_word : nullptr;
     dirty = false;
+    sync_shared();  // start from the k-th value other lists already published
   }
 
   B2K_DEV uint32_t fetch_shared() const {
