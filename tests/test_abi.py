@@ -59,6 +59,27 @@ def test_invalid_arguments_rejected_before_device_use(lib):
     assert rc == _lib.B2K_EINVAL
 
 
+def test_shard_merge_rejects_bad_shapes(lib):
+    # the row-shard merge checks its shapes before touching any device memory
+    from mlxlearn_b200 import _lib
+
+    assert lib.b2k_shard_merge(None, None, 17, 4, 3, 3, 8, -1, None, None, None,
+                               None) == _lib.B2K_EINVAL
+    assert b"shard count" in lib.b2k_last_error()
+    assert lib.b2k_shard_merge(None, None, 2, 4, 3, 5, 8, -1, None, None, None,
+                               None) == _lib.B2K_EINVAL  # k_in < k
+    assert lib.b2k_shard_merge(None, None, 2, 4, 258, 257, 8, -1, None, None, None,
+                               None) == _lib.B2K_EINVAL  # k above 256
+    assert lib.b2k_shard_merge(None, None, 2, 0, 3, 3, 8, -1, None, None, None,
+                               None) == _lib.B2K_OK      # no queries: nothing to do
+    assert lib.b2k_shard_merge(None, None, 2, 4, 3, 3, 8, -1, None, None, None,
+                               None) == _lib.B2K_EINVAL  # NULL buffers
+    assert lib.b2k_shard_resolve(None, None, 2, 4, 3, 3, -1, None, 5, None, None, None,
+                                 None) == _lib.B2K_EINVAL  # more flagged rows than queries
+    assert lib.b2k_shard_keys(None, 0, None, None, 2, 4, 3, None, 0, None,
+                              None) == _lib.B2K_EINVAL     # no index
+
+
 def test_injected_allocation_failure(lib, monkeypatch):
     from mlxlearn_b200 import _lib
 
