@@ -1063,7 +1063,8 @@ static int check_shard_shapes(int32_t n_shards, int64_t m, int32_t k_in, int32_t
     return fail(B2K_EINVAL, "shard count must be in [1, %d], got %d", kMaxShards, n_shards);
   if (m < 0) return fail(B2K_EINVAL, "query count must be non-negative");
   if (k < 1 || k > kMaxShardK || k_in < k || k_in > kMaxShardK + 1)
-    return fail(B2K_EINVAL, "shard merge needs 1 <= k <= %d and k <= k_in <= k + 1, got k=%d k_in=%d",
+    return fail(B2K_EINVAL,
+                "shard merge needs 1 <= k <= %d and k <= k_in <= k + 1, got k=%d k_in=%d",
                 kMaxShardK, k, k_in);
   return B2K_OK;
 }
@@ -1080,7 +1081,8 @@ int b2k_shard_merge(const double* d_dist, const int64_t* d_idx, int32_t n_shards
   launch_shard_merge(d_dist, d_idx, n_shards, m, k_in, k, self_offset, shard_eps(d), d_out_dist,
                      d_out_idx, d_flags, static_cast<cudaStream_t>(stream));
   const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(B2K_ECUDA, "shard merge launch failed: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return fail(B2K_ECUDA, "shard merge launch failed: %s", cudaGetErrorString(e));
   return B2K_OK;
 }
 
@@ -1100,7 +1102,8 @@ int b2k_shard_keys(b2k_index* h, int64_t row_lo, const float* dQ, const int64_t*
   launch_shard_keys(nullptr, d_idx, n_shards, m, k_in, dQ, ix.X, ix.n, ix.d, row_lo, d_flagged,
                     n_flagged, d_keys, static_cast<cudaStream_t>(stream));
   const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(B2K_ECUDA, "shard keys launch failed: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return fail(B2K_ECUDA, "shard keys launch failed: %s", cudaGetErrorString(e));
   return B2K_OK;
 }
 

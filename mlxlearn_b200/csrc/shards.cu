@@ -135,7 +135,8 @@ __global__ void shard_resolve_kernel(ShardLists L, int kout, int64_t self_offset
       if (taken[c >> 5] >> (c & 31) & 1u) continue;
       const int64_t g = L.I[L.at(c / L.kin, q, c % L.kin)];
       if (g < 0 || g == self) continue;
-      if (best < 0 || key_row_less(kq + (size_t)c * kKeyLimbs, g, kq + (size_t)best * kKeyLimbs, bg)) {
+      if (best < 0 ||
+          key_row_less(kq + (size_t)c * kKeyLimbs, g, kq + (size_t)best * kKeyLimbs, bg)) {
         best = c;
         bg = g;
       }
