@@ -41,7 +41,7 @@ WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
 # Our kernels per kNN call: assign, bin_scan, scatter, gather (query grouping),
 # prep_queries, screen_tc, certify, exact (fallback rows; no-op when none).
 LAUNCHES_PER_STEP = 8
-SCREEN_TRAFFIC_BYTES = 6.84e9
+SCREEN_TRAFFIC_BYTES = 5.77e9
 
 
 def peaks():
