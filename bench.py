@@ -481,7 +481,10 @@ def run_secondary(args):
                      "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
                                       "kind": "reference" if ref else "port",
                                       "sample": "all 2000 queries"},
-                     "parity_vs_cpu_reference": {"indices_bit_exact": bool(np.array_equal(oi, ri))}})
+                     "parity_vs_cpu_reference": {
+                         "queries": len(Q), "indices_bit_exact": bool(np.array_equal(oi, ri)),
+                         "max_rel_dist_err": float(np.max(np.abs(od - rd) /
+                                                          np.maximum(rd, 1e-300)))}})
     print(json.dumps(line), flush=True)
     return 0
 
@@ -658,6 +661,20 @@ def run_chamfer(args):
             ((Pt - Qt[torch.from_numpy(idx[:, 0])]) ** 2).sum().backward()
             cpu_pairs += len(P) * len(Qr)
     cpu_s = time.perf_counter() - t0
+    # parity of the forward: the two sampled pairs (both directions) through the
+    # segment search against the reference's exact scan
+    from mlxlearn_b200.autograd import knn_segments
+
+    exact, err = True, 0.0
+    for a, b in clouds[:2]:
+        for P, Qr in ((a, b), (b, a)):
+            gd, gi = knn_segments(torch.from_numpy(Qr).cuda(), torch.from_numpy(P).cuda(),
+                                  [len(Qr)], [len(P)], 1)
+            rdist = np.empty((len(Qr), 1)); ridx = np.empty((len(Qr), 1), np.int64)
+            _ref_knn_threads(ref, P, Qr, 1, rdist, ridx, threads)
+            exact &= bool(np.array_equal(gi.cpu().numpy(), ridx))
+            gdv = gd.double().cpu().numpy()
+            err = max(err, float(np.max(np.abs(gdv - rdist) / np.maximum(rdist, 1e-300))))
     line = {
         "metric": "differentiable kNN: (query, reference) pairs/s, forward + backward "
                   "(64 Chamfer k=1 pairs of 8192x3 + self k=8 on 4096x64)",
@@ -672,6 +689,10 @@ def run_chamfer(args):
                          "kind": "reference" if ref else "port",
                          "sample": "2 Chamfer pairs both ways: reference exact scan forward, "
                                    "torch float64 CPU autograd backward"},
+        "parity_vs_cpu_reference": {"pairs": 4, "indices_bit_exact": exact,
+                                    "max_rel_dist_err": err,
+                                    "note": "forward k=1 of 2 Chamfer pairs, both directions; "
+                                            "distances are float32 outputs of the autograd path"},
     }
     print(json.dumps(line), flush=True)
     return 0
