@@ -85,3 +85,19 @@ def test_radius_row_shards_equal_one_search(sort_results):
     np.testing.assert_array_equal(res.indptr, ip)
     np.testing.assert_array_equal(res.indices, ii)
     np.testing.assert_array_equal(res.distances, dd)
+
+
+def test_row_shards_lattice_ties():
+    # integer lattice points: exact duplicates and equal distances everywhere,
+    # spread over four shards; every tie breaks by global row
+    rng = np.random.default_rng(95)
+    X = rng.integers(-3, 4, size=(1600, 4)).astype(np.float32)
+    Q = (rng.integers(-3, 4, size=(120, 4)) + 0.5).astype(np.float32)
+    bounds = [0, 300, 800, 1100, 1600]
+    parts = [(CpuShard(X[a:b]), a) for a, b in zip(bounds[:-1], bounds[1:])]
+    ops = CountingOps()
+    d, i = merge_row_shards(parts, torch.from_numpy(Q), 10, ops=ops)
+    od, oi = oracle.knn(X, Q, 10)
+    np.testing.assert_array_equal(i.numpy(), oi)
+    np.testing.assert_array_equal(d.numpy(), od)
+    assert ops.flagged > 0

@@ -109,3 +109,20 @@ def test_radius_row_shards_equal_one_search(sort_results):
     np.testing.assert_array_equal(res.indptr, ip)
     np.testing.assert_array_equal(res.indices, ii)
     np.testing.assert_array_equal(res.distances, dd)
+
+
+def test_row_shards_lattice_ties():
+    import torch
+
+    from mlxlearn_b200.sharding import merge_row_shards
+
+    rng = np.random.default_rng(96)
+    X = rng.integers(-3, 4, size=(20000, 8)).astype(np.float32)
+    Q = (rng.integers(-3, 4, size=(400, 8)) + 0.5).astype(np.float32)
+    ops = _ops()
+    d, i = merge_row_shards(_parts(X, [0, 4000, 11000, 15000, 20000]),
+                            torch.from_numpy(Q).cuda(), 20, ops=ops)
+    od, oi = oracle.knn(X, Q, 20)
+    np.testing.assert_array_equal(i.cpu().numpy(), oi)
+    np.testing.assert_array_equal(d.cpu().numpy(), od)
+    assert ops.flagged > 0
