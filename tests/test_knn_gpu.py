@@ -297,3 +297,32 @@ def test_uncertified_bf16_rows_get_an_fp32_second_pass():
     assert ixs.last_stats["second_pass_rows"] > 0, ixs.last_stats
     o2d, o2i = oracle.knn(Xs, Xs[:50], 60, exclude_self=True)
     np.testing.assert_array_equal(i2.cpu().numpy(), o2i)
+
+
+@pytest.mark.parametrize("k", [64, 65, 200])
+def test_k_across_the_screen_limit(k, rng):
+    """k up to 64 runs the screens; larger k takes the exhaustive exact scan.
+    Both give the oracle's answer, for host and device queries and a
+    self-query; k equal to every row of a small index too."""
+    import torch
+
+    X = rng.normal(size=(6000, 24)).astype(np.float32)
+    Q = rng.normal(size=(150, 24)).astype(np.float32)
+    index = make_index(X)
+    od, oi = oracle.knn(X, Q, k)
+    dist, idx = index.query(Q, k)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
+    dd, di = index.query_device(torch.from_numpy(Q).cuda(), k)
+    np.testing.assert_array_equal(di.cpu().numpy(), oi)
+    np.testing.assert_array_equal(dd.cpu().numpy(), od)
+    od, oi = oracle.knn(X, X[:100], k, exclude_self=True)
+    dd, di = index.query_device(torch.from_numpy(X[:100]).cuda(), k, exclude_self=True,
+                                q_offset=0)
+    np.testing.assert_array_equal(di.cpu().numpy(), oi)
+    np.testing.assert_array_equal(dd.cpu().numpy(), od)
+    small = make_index(X[:k])
+    od, oi = oracle.knn(X[:k], Q[:7], k)
+    dist, idx = small.query(Q[:7], k)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)
