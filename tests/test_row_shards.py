@@ -101,3 +101,26 @@ def test_row_shards_lattice_ties():
     np.testing.assert_array_equal(i.numpy(), oi)
     np.testing.assert_array_equal(d.numpy(), od)
     assert ops.flagged > 0
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_row_shards_random_layouts(seed):
+    # random shard counts and uneven boundaries, duplicates planted across
+    # shards, self-queries on some seeds
+    rng = np.random.default_rng(1000 + seed)
+    n, d = int(rng.integers(200, 900)), int(rng.integers(2, 9))
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    dup = rng.integers(0, n, size=12)
+    X[rng.integers(0, n, size=12)] = X[dup]
+    S = int(rng.integers(2, 7))
+    cuts = np.sort(rng.choice(np.arange(1, n), size=S - 1, replace=False))
+    bounds = [0, *cuts.tolist(), n]
+    parts = [(CpuShard(X[a:b]), int(a)) for a, b in zip(bounds[:-1], bounds[1:])]
+    k = int(rng.integers(1, 12))
+    exclude = bool(seed % 2)
+    Q = X[:50] if exclude else rng.normal(size=(50, d)).astype(np.float32)
+    d_, i_ = merge_row_shards(parts, torch.from_numpy(np.ascontiguousarray(Q)), k,
+                              exclude_self=exclude, q_offset=0, ops=CpuRowShardOps())
+    od, oi = oracle.knn(X, Q, k, exclude_self=exclude)
+    np.testing.assert_array_equal(i_.numpy(), oi)
+    np.testing.assert_array_equal(d_.numpy(), od)
