@@ -211,3 +211,34 @@ def test_radius_estimators_pickle(rng):
         p1 = pickle.loads(pickle.dumps(reg)).predict(Q[:200])
     np.testing.assert_array_equal(np.isnan(p0), np.isnan(p1))
     np.testing.assert_array_equal(p0[~np.isnan(p0)], p1[~np.isnan(p1)])
+
+
+@gpu
+def test_distance_weights_zero_distance_rule_matches_sklearn():
+    # queries that coincide with training rows: only the zero-distance
+    # neighbours vote (weights = indicator of zero distances), the rule of
+    # scikit-learn's distance weights that the reference follows
+    from sklearn.neighbors import KNeighborsClassifier as SkC
+    from sklearn.neighbors import KNeighborsRegressor as SkR
+
+    rng = np.random.default_rng(77)
+    X = rng.normal(size=(3000, 6)).astype(np.float32)
+    y = rng.integers(0, 4, size=3000)
+    t = rng.normal(size=3000)
+    Q = np.concatenate([X[:40], rng.normal(size=(40, 6)).astype(np.float32)])
+    ours = KNeighborsClassifier(n_neighbors=7, weights="distance").fit(X, y)
+    ref = SkC(n_neighbors=7, weights="distance", algorithm="brute").fit(X, y)
+    np.testing.assert_array_equal(ours.predict(Q), ref.predict(Q))
+    # zero-distance rows: the indicator weights, exactly; elsewhere scikit-learn
+    # weighs by float32 distances (its arithmetic for float32 input), this
+    # engine by the canonical float64 ones, hence the float32-level tolerance
+    p, rp = ours.predict_proba(Q), ref.predict_proba(Q)
+    np.testing.assert_array_equal(p[:40], rp[:40])
+    np.testing.assert_allclose(p[40:], rp[40:], rtol=1e-6, atol=1e-7)
+    ours_r = KNeighborsRegressor(n_neighbors=7, weights="distance").fit(X, t)
+    ref_r = SkR(n_neighbors=7, weights="distance", algorithm="brute").fit(X, t)
+    pr, rpr = ours_r.predict(Q), ref_r.predict(Q)
+    np.testing.assert_array_equal(pr[:40], rpr[:40])
+    np.testing.assert_allclose(pr[40:], rpr[40:], rtol=1e-6, atol=1e-7)
+    # the first 40 queries are training rows: their prediction is that row's label
+    np.testing.assert_array_equal(ours.predict(Q[:40]), y[:40])
