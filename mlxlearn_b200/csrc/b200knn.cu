@@ -250,9 +250,10 @@ static int run_exact(Index& ix, const float* dQ, int64_t m, int k, int exclude_s
                      int64_t q_offset, double* d_dist, int64_t* d_idx, const int* rows,
                      const int* row_count, unsigned long long* counters, int* status,
                      cudaStream_t st, StreamFree& fr, bool use_scratch,
-                     const int* perm = nullptr) {
+                     const int* perm = nullptr, int squared = 0) {
   ExactArgs ea{};
   ea.perm = perm;
+  ea.squared = squared;
   ea.X = ix.X;
   ea.Q = dQ;
   ea.n = ix.n;
@@ -289,6 +290,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
                            cudaStream_t st, b2k_stats* stats, const int* ext_perm = nullptr) {
   const int fm = fault_mode();
   if (fm == 2) return fail(B2K_ECUDA, "injected kernel launch failure (B2K_FAULT=launch)");
+  const int squared = (mode & B2K_MODE_SQUARED) ? 1 : 0;
+  const int sq_flag = squared ? B2K_MODE_SQUARED : 0;
+  mode &= ~B2K_MODE_SQUARED;
   if (mode == B2K_MODE_AUTO)
     mode = (!ix.range_ok || k > kMaxK) ? B2K_MODE_EXACT
            : (ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16
@@ -324,7 +328,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   int64_t second_pass_rows = 0, second_exact_rows = 0;
   if (mode == B2K_MODE_EXACT) {
     rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, nullptr, nullptr,
-                   counters, status, st, fr, true, ext_perm);
+                   counters, status, st, fr, true, ext_perm, squared);
     if (rc) return rc;
   } else {
     if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
@@ -420,6 +424,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.fallback_count = status + 2;
     ca.counters = counters;
     ca.perm = perm;
+    ca.squared = squared;
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
     // Rows the screen could not certify (a list past capacity, too many
@@ -441,8 +446,8 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
         launch_gather_fallback(Qs, ix.d, fb_list, perm, nfb, Qfb, pfb, st);
         B2K_CUDA(cudaGetLastError());
         b2k_stats sub{};
-        rc = knn_device_impl(ix, Qfb, nfb, k, exclude_self, q_offset, B2K_MODE_FP32, d_dist,
-                             d_idx, st, &sub, pfb);
+        rc = knn_device_impl(ix, Qfb, nfb, k, exclude_self, q_offset, B2K_MODE_FP32 | sq_flag,
+                             d_dist, d_idx, st, &sub, pfb);
         if (rc) return rc;
         second_pass_rows = nfb;
         second_exact_rows = sub.fallback_rows;
@@ -451,7 +456,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     }
     if (!second_pass) {
       rc = run_exact(ix, Qs, m, k, exclude_self, q_offset, d_dist, d_idx, fb_list, status + 2,
-                     counters, status, st, fr, false, perm);
+                     counters, status, st, fr, false, perm, squared);
       if (rc) return rc;
     }
   }
@@ -472,8 +477,8 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     return fail(B2K_ETIMEOUT, "a bounded device wait gave up (code %d)", hstatus[0]);
   if (hstatus[4] & 1) {
     // Some query coordinate is outside the screens' safe range: redo exactly.
-    return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, B2K_MODE_EXACT, d_dist, d_idx,
-                           st, stats, ext_perm);
+    return knn_device_impl(ix, dQ, m, k, exclude_self, q_offset, B2K_MODE_EXACT | sq_flag,
+                           d_dist, d_idx, st, stats, ext_perm);
   }
   if (stats) {
     stats->splits = S;
@@ -503,7 +508,8 @@ static int validate_knn(const Index& ix, int64_t m, int32_t k, int32_t exclude_s
                 "exclude_self requires the query matrix to be the training matrix: got %lld "
                 "query rows at offset %lld and %lld training rows.",
                 (long long)m, (long long)q_offset, (long long)ix.n);
-  if (mode < B2K_MODE_AUTO || mode > B2K_MODE_EXACT) return fail(B2K_EINVAL, "unknown mode %d", mode);
+  const int32_t base = mode & ~B2K_MODE_SQUARED;
+  if (base < B2K_MODE_AUTO || base > B2K_MODE_EXACT) return fail(B2K_EINVAL, "unknown mode %d", mode);
   return B2K_OK;
 }
 

@@ -404,7 +404,7 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   const int64_t orow = a.perm ? a.perm[row] : row;
   for (int t = lane; t < k; t += 32) {
     a.idx[orow * k + t] = si[t];
-    if (a.dist) a.dist[orow * k + t] = sqrt(cs[t]);
+    if (a.dist) a.dist[orow * k + t] = a.squared ? cs[t] : sqrt(cs[t]);
   }
   if (lane == 0) {
     atomicAdd(&a.counters[0], (unsigned long long)C);
@@ -525,7 +525,7 @@ __device__ __forceinline__ void exact_row(const ExactArgs& a, int64_t row, doubl
     const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
     for (int t = tid; t < a.k; t += 32) {
       a.idx[orow * a.k + t] = ci[t];
-      if (a.dist) a.dist[orow * a.k + t] = sqrt(cs[t]);
+      if (a.dist) a.dist[orow * a.k + t] = a.squared ? cs[t] : sqrt(cs[t]);
     }
     if (tid == 0) {
       atomicAdd(&a.counters[3], 1ull);

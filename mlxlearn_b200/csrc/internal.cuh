@@ -147,6 +147,7 @@ struct CertifyArgs {
   unsigned long long* counters;  // [4]: candidates, entries, exact compares, -
   const int* perm;     // row -> output row (or null)
   int64_t row_base;    // added to the row in fallback_list entries (batched runs)
+  int squared;         // write squared distances (else their square roots)
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
 // problem p owns global rows [row_start[p], row_start[p + 1]) of the batch
@@ -169,6 +170,7 @@ struct ExactArgs {
   unsigned long long* counters;
   int* status;
   const int* perm;      // row -> original query row for output and self (or null)
+  int squared;          // write squared distances (else their square roots)
 };
 void launch_exact(const ExactArgs& a, cudaStream_t st);
 // rows: global row ids of the batch; scratch: [grid][n_max] or null

@@ -20,6 +20,14 @@ __all__ = ["NeighborIndex", "build_index"]
 NUMPY_FLOAT = np.float32
 INDEX_DTYPE = np.int64
 
+# Route names of the reference's query policy (src/mlxlearn/_kernels/
+# distance.py:114-141): "cpu" asks the calling estimator to take results as
+# host arrays through query(), "mlx" to keep them on the device through
+# query_device() and vote with MLX.  This index answers every route on the
+# GPU; it names the host-array route, the one an estimator can consume
+# without MLX (reference src/mlxlearn/neighbors/_classification.py:138-159).
+HOST_ARRAY_ROUTE = "cpu"
+
 
 def _as_f32_c(X) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(X, dtype=NUMPY_FLOAT))
@@ -33,7 +41,8 @@ class NeighborIndex:
     only thing searched.
     """
 
-    def __init__(self, X: np.ndarray, *, device: int = 0, mode: str = "auto"):
+    def __init__(self, X: np.ndarray, *, device: int = 0, mode: str = "auto",
+                 backend: str = "cuda", auto_policy: bool = False):
         if X.ndim != 2 or 0 in X.shape:
             raise ValueError("X must be a nonempty two-dimensional matrix")
         if X.shape[0] >= 2**31:
@@ -42,6 +51,11 @@ class NeighborIndex:
         self._n, self._d = int(X.shape[0]), int(X.shape[1])
         self.device = int(device)
         self.mode = mode
+        # the backend name and policy flag the estimator asked for at fit
+        # (reference distance.py:86-97); every query runs on the GPU anyway
+        self.backend = backend
+        self.auto_policy = bool(auto_policy)
+        self._gpu_available = True
         self._handle = None
         self._lock = threading.Lock()
         self.last_query_backend = None
@@ -63,6 +77,9 @@ class NeighborIndex:
         self._n, self._d = int(Xc.shape[0]), int(Xc.shape[1])
         self.device = Xc.device.index or 0
         self.mode = mode
+        self.backend = "cuda"
+        self.auto_policy = False
+        self._gpu_available = True
         self._lock = threading.Lock()
         self.last_query_backend = None
         self.last_stats = None
@@ -102,10 +119,20 @@ class NeighborIndex:
     def __getstate__(self):
         # Host rows and parameters only; the device index is rebuilt lazily
         # (reference distance.py:191-209).
-        return {"X": self.training_data, "device": self.device, "mode": self.mode}
+        return {"X": self.training_data, "device": self.device, "mode": self.mode,
+                "backend": self.backend, "auto_policy": self.auto_policy}
 
     def __setstate__(self, state):
-        self.__init__(state["X"], device=state.get("device", 0), mode=state.get("mode", "auto"))
+        self.__init__(state["X"], device=state.get("device", 0), mode=state.get("mode", "auto"),
+                      backend=state.get("backend", "cuda"),
+                      auto_policy=state.get("auto_policy", False))
+
+    @property
+    def device_index(self) -> "NeighborIndex":
+        """The device-resident search state (reference distance.py:179-182):
+        this object, with its library index created."""
+        self._ensure_device()
+        return self
 
     # ----------------------------------------------------------- properties
     @property
@@ -130,6 +157,16 @@ class NeighborIndex:
         return self._d
 
     # -------------------------------------------------------------- queries
+    def _query_policy(self, n_query, k, Q=None):
+        """``(route, integer_exact)`` as the reference's policy returns it
+        (distance.py:114-138).  Every batch runs on the GPU; the route is the
+        host-array one (``HOST_ARRAY_ROUTE``) and no integer-exact variant
+        is needed because every answer is exact."""
+        return HOST_ARRAY_ROUTE, None
+
+    def backend_for_query(self, n_query, k, Q=None):
+        return self._query_policy(n_query, k, Q)[0]
+
     def _check_query(self, n_query: int, k: int, exclude_self: bool):
         limit = self.n_samples - int(bool(exclude_self))
         if k > limit:
@@ -140,14 +177,17 @@ class NeighborIndex:
                 f"got {n_query} query rows and {self.n_samples} training rows.")
 
     def query(self, Q, k, *, return_distance=True, exclude_self=False,
-              query_block_size=None, train_block_size=None, mode=None, stats=False, out=None):
+              query_block_size=None, train_block_size=None, _policy=None, mode=None,
+              stats=False, out=None):
         """Float64 distances (or None) and int64 indices, each ``[n_query, k]``.
 
         ``query_block_size`` splits the queries into independent batches;
         results do not depend on it.  ``train_block_size`` is accepted for
         compatibility: the engine tiles the training rows itself and its
-        merge is exact, so blocking never changes an answer.  ``out`` may
-        supply preallocated (e.g. pinned) ``(dist, idx)`` host arrays.
+        merge is exact, so blocking never changes an answer.  ``_policy``
+        (a ``_query_policy`` result, reference distance.py:242-245) does not
+        change the route: every policy runs here.  ``out`` may supply
+        preallocated (e.g. pinned) ``(dist, idx)`` host arrays.
         """
         Q = _as_f32_c(Q)
         k = int(k)
@@ -184,19 +224,28 @@ class NeighborIndex:
         self.last_query_backend = "cuda"
         return dist, idx
 
-    def query_device(self, Q, k, *, return_distance=True, exclude_self=False, q_offset=0,
+    def query_device(self, Q, k, *, return_distance=True, exclude_self=False,
+                     query_block_size=None, train_block_size=None, _squared=False, q_offset=0,
                      mode=None, stats=False, stream=None):
-        """Device-resident query: ``Q`` is a CUDA float32 tensor ``[m, d]``.
+        """Device-resident query (reference distance.py:211-240): ``Q`` is a
+        CUDA float32 tensor ``[m, d]`` (a host array is uploaded first).
 
-        Returns torch tensors on the same device (float64 distances or None,
-        int64 indices), computed on the current torch stream.
+        Returns torch tensors on the device (float64 distances or None, int64
+        indices), computed on the current torch stream.  ``_squared`` returns
+        the canonical float64 squared distances instead of their square
+        roots.  ``query_block_size`` splits the batch (results do not depend
+        on it); ``train_block_size`` is accepted for compatibility.
         """
         import torch
 
         if not (isinstance(Q, torch.Tensor) and Q.is_cuda):
-            raise TypeError("query_device expects a CUDA tensor")
+            if isinstance(Q, torch.Tensor):
+                raise TypeError("query_device expects a CUDA tensor or a host array")
+            Q = torch.from_numpy(_as_f32_c(Q)).to(torch.device("cuda", self.device))
         Q = Q.detach().to(torch.float32).contiguous()
         m, k = int(Q.shape[0]), int(k)
+        if Q.dim() != 2 or (m and Q.shape[1] != self.n_features):
+            raise ValueError(f"Q must have shape (n, {self.n_features})")
         if exclude_self:
             limit = self.n_samples - 1
             if k > limit:
@@ -209,11 +258,16 @@ class NeighborIndex:
             h = self._ensure_device()
             st = _lib.Stats()
             s = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
-            rc = _lib.load().b2k_knn_device(
-                h, Q.data_ptr(), m, k, int(bool(exclude_self)), int(q_offset),
-                _lib.MODES[mode or self.mode], None if dist is None else dist.data_ptr(),
-                idx.data_ptr(), s, ctypes.byref(st) if stats else None)
-            _lib.check(rc, "b2k_knn_device")
+            code = _lib.MODES[mode or self.mode] | (_lib.MODE_SQUARED if _squared else 0)
+            step = m if not query_block_size else max(1, int(query_block_size))
+            for start in range(0, m, step):
+                stop = min(m, start + step)
+                rc = _lib.load().b2k_knn_device(
+                    h, Q[start:stop].data_ptr(), stop - start, k, int(bool(exclude_self)),
+                    int(q_offset) + start, code,
+                    None if dist is None else dist[start:stop].data_ptr(),
+                    idx[start:stop].data_ptr(), s, ctypes.byref(st) if stats else None)
+                _lib.check(rc, "b2k_knn_device")
             self.last_stats = st.as_dict() if stats else None
         self.last_query_backend = "cuda"
         return dist, idx
@@ -228,8 +282,12 @@ class NeighborIndex:
         A training row is returned iff its exact squared distance is at most
         ``fl64(radius ** 2)`` (reference distance.py:285-342).  Rows hold
         ascending training indices, or ``(distance, index)`` order with
-        ``sort_results``.  ``algorithm``/``n_jobs``/``patched``/``raw`` are
-        accepted for signature compatibility.
+        ``sort_results``.  With ``raw`` each batch keeps its device result,
+        so ``votes``/``mean`` reduce it on the GPU and host arrays are only
+        copied if read; otherwise the batches are copied into page-locked
+        host memory at once and the device results freed.
+        ``algorithm``/``n_jobs``/``patched`` are accepted for signature
+        compatibility.
         """
         from .radius_result import RadiusCSR
 
@@ -255,19 +313,12 @@ class NeighborIndex:
                                 int(bool(need_distance or sort_results)),
                                 int(bool(sort_results)), ctypes.byref(res))
             _lib.check(rc, "b2k_radius")
-            try:
-                nnz = ctypes.c_int64()
-                _lib.check(lib.b2k_radius_result_nnz(res, ctypes.byref(nnz)))
-                indptr = np.empty(stop - start + 1, INDEX_DTYPE)
-                indices = np.empty(nnz.value, INDEX_DTYPE)
-                dist = (np.empty(nnz.value, np.float64)
-                        if (need_distance or sort_results) else None)
-                _lib.check(lib.b2k_radius_result_fetch(
-                    res, indptr.ctypes.data, indices.ctypes.data,
-                    None if dist is None else dist.ctypes.data))
-            finally:
-                lib.b2k_radius_result_release(res)
-            parts.append(RadiusCSR(indptr, indices, dist if need_distance else None))
+            part = RadiusCSR.from_device(res, stop - start, device=self.device,
+                                         distances=bool(need_distance))
+            if not raw:
+                part.indptr  # noqa: B018 -- copy out now, then free the device result
+                part.release()
+            parts.append(part)
         self.last_query_backend = "cuda"
         return parts
 
@@ -278,56 +329,24 @@ class NeighborIndex:
         neighbourhoods, reduced on the device without downloading them.
         Returns ``(votes [m, n_classes] or means [m], counts [m])`` as numpy
         arrays, equal to the host reductions over :meth:`query_radius_csr`."""
-        import torch
-
-        radius = validate_radius(radius)
-        Q = _as_f32_c(Q)
-        if Q.ndim != 2 or Q.shape[1] != self.n_features:
-            raise ValueError(f"Q must have shape (n, {self.n_features})")
         if (codes is None) == (targets is None):
             raise ValueError("pass exactly one of codes and targets")
-        n_query = int(Q.shape[0])
-        if exclude_self and n_query != self.n_samples:
-            raise ValueError(
-                "exclude_self requires the query matrix to be the training matrix: "
-                f"got {n_query} query rows and {self.n_samples} training rows.")
-        dev = torch.device("cuda", self.device)
-        width = int(n_classes) if codes is not None else 1
-        out = torch.empty((n_query, width) if codes is not None else (n_query,),
-                          dtype=torch.float64, device=dev)
-        counts = torch.empty(n_query, dtype=torch.int64, device=dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        step = n_query if not query_block_size else max(1, int(query_block_size))
-        lib = _lib.load()
-        h = self._ensure_device()
-        for start in range(0, n_query, max(step, 1)):
-            stop = min(n_query, start + step)
-            block = Q[start:stop]
-            res = ctypes.c_void_p()
-            rc = lib.b2k_radius(h, block.ctypes.data, stop - start, float(radius),
-                                int(bool(exclude_self)), start, int(bool(weighted)), 0,
-                                ctypes.byref(res))
-            _lib.check(rc, "b2k_radius")
-            try:
-                if codes is not None:
-                    rc = lib.b2k_radius_result_class_votes(
-                        res, codes.data_ptr(), width, int(bool(weighted)),
-                        out[start:stop].data_ptr(), counts[start:stop].data_ptr(), stream)
-                else:
-                    rc = lib.b2k_radius_result_means(
-                        res, targets.data_ptr(), int(bool(weighted)),
-                        out[start:stop].data_ptr(), counts[start:stop].data_ptr(), stream)
-                _lib.check(rc, "radius reduction")
-            finally:
-                lib.b2k_radius_result_release(res)
-        self.last_query_backend = "cuda"
-        return out.cpu().numpy(), counts.cpu().numpy()
+        parts = self.query_radius_csr(Q, radius, need_distance=bool(weighted),
+                                      exclude_self=exclude_self,
+                                      query_block_size=query_block_size, raw=True)
+        pieces = [p.votes(codes, n_classes, weighted) if codes is not None
+                  else p.mean(targets, weighted) for p in parts]
+        for p in parts:
+            p.release()
+        if len(pieces) == 1:
+            return pieces[0]
+        return (np.concatenate([a for a, _ in pieces]), np.concatenate([c for _, c in pieces]))
 
     def query_radius(self, Q, radius, *, return_distance=True, exclude_self=False,
                      sort_results=False, query_block_size=None, train_block_size=None,
                      algorithm="auto"):
         """scikit-learn's ragged form of :meth:`query_radius_csr`."""
-        from .radius_result import to_ragged
+        from .radius_result import ragged_rows
 
         if Q.shape[0] == 0:
             empty = np.empty(0, dtype=object)
@@ -335,7 +354,7 @@ class NeighborIndex:
         parts = self.query_radius_csr(Q, radius, need_distance=return_distance or sort_results,
                                       exclude_self=exclude_self, sort_results=sort_results,
                                       query_block_size=query_block_size)
-        return to_ragged(parts, return_distance=return_distance)
+        return ragged_rows(parts, return_distance=return_distance)
 
 
 def validate_radius(radius) -> float:
@@ -359,13 +378,15 @@ def validate_radius(radius) -> float:
     return value + 0.0
 
 
-def build_index(X, *, backend: str = "cuda", _owned: bool = False, device: int = 0,
-                mode: str = "auto") -> NeighborIndex:
+def build_index(X, *, backend: str = "cuda", _owned: bool = False, _auto: bool = False,
+                _gpu_available=True, device: int = 0, mode: str = "auto") -> NeighborIndex:
     """Own a float32 C-order copy of ``X`` (never alias a caller's array).
 
-    ``backend`` is accepted for signature compatibility with the reference
-    (distance.py:366-392); every backend name runs on the CUDA library.
+    Takes the reference's arguments (distance.py:366-392): ``backend`` and
+    ``_auto`` are recorded on the index, ``_gpu_available`` is accepted;
+    every backend name runs on the CUDA library.  ``_owned`` hands over a
+    freshly converted buffer instead of copying it.
     """
     Xf = (np.ascontiguousarray(np.asarray(X, dtype=NUMPY_FLOAT)) if _owned
           else np.array(X, dtype=NUMPY_FLOAT, order="C", copy=True))
-    return NeighborIndex(Xf, device=device, mode=mode)
+    return NeighborIndex(Xf, device=device, mode=mode, backend=backend, auto_policy=_auto)

@@ -13,11 +13,11 @@ from __future__ import annotations
 from numbers import Integral, Real
 
 import numpy as np
-from sklearn import get_config as get_sklearn_config
 from sklearn.utils.validation import check_is_fitted, validate_data
 
 from ..exceptions import SparseInputError, UnsupportedInputError, UnsupportedParameterError
 from ..index import build_index
+from ..radius_result import neighbour_graph, ragged_rows, sparse_graph
 
 __all__ = ["NeighborsMixin", "RadiusMixin", "SUPPORTED_METRICS", "compute_weights"]
 
@@ -163,26 +163,24 @@ class NeighborsMixin:
         return (dist, idx) if return_distance else idx
 
     def kneighbors_graph(self, X=None, n_neighbors=None, mode="connectivity"):
-        """CSR graph of the selected neighbours (reference _base.py:426-444)."""
+        """Sparse ``[n_queries, n_samples_fit]`` graph with one stored entry
+        per selected neighbour: 1.0 (``connectivity``) or the distance
+        (``distance``); X=None excludes each row itself (the contract of
+        reference _base.py:426-444)."""
         check_is_fitted(self, "_index_")
-        if mode not in ("connectivity", "distance"):
-            raise ValueError('Unsupported mode, must be one of "connectivity", '
-                             f'or "distance" but got "{mode}" instead')
-        if mode == "distance":
-            distances, indices = self.kneighbors(X, n_neighbors, return_distance=True)
-            values = distances.ravel()
-        else:
-            indices = self.kneighbors(X, n_neighbors, return_distance=False)
-            values = np.ones(indices.size)
-        from scipy import sparse
+        _check_graph_mode(mode)
+        want_dist = mode == "distance"
+        dist, idx = self._index_query_for_graph(X, n_neighbors, want_dist)
+        m, k = idx.shape
+        # every row holds exactly k entries, so the row offsets are k * row
+        offsets = k * np.arange(m + 1, dtype=np.int64)
+        weights = dist.reshape(-1) if want_dist else np.full(m * k, 1.0)
+        return sparse_graph(offsets, idx.reshape(-1), weights, (m, self.n_samples_fit_))
 
-        count, k = indices.shape
-        indptr = np.arange(0, indices.size + 1, k)
-        constructor = (sparse.csr_array
-                       if get_sklearn_config().get("sparse_interface") == "sparray"
-                       else sparse.csr_matrix)
-        return constructor((values, indices.ravel(), indptr),
-                           shape=(count, self.n_samples_fit_))
+    def _index_query_for_graph(self, X, n_neighbors, want_dist):
+        if want_dist:
+            return self.kneighbors(X, n_neighbors, return_distance=True)
+        return None, self.kneighbors(X, n_neighbors, return_distance=False)
 
     def __getstate__(self):
         state = dict(self.__dict__)
@@ -221,23 +219,23 @@ class RadiusMixin:
         as scikit-learn's ragged object arrays."""
         if sort_results and not return_distance:
             raise ValueError("return_distance must be True if sort_results is True.")
-        from ..radius_result import to_ragged
-
         parts = self._radius_parts(X, radius, need_distance=return_distance,
                                    sort_results=sort_results)
-        return to_ragged(parts, return_distance=return_distance)
+        return ragged_rows(parts, return_distance=return_distance)
 
     def radius_neighbors_graph(self, X=None, radius=None, mode="connectivity",
                                sort_results=False):
-        if mode not in ("connectivity", "distance"):
-            raise ValueError('Unsupported mode, must be one of "connectivity", '
-                             f'or "distance" but got "{mode}" instead')
-        from ..radius_result import to_graph
-
+        _check_graph_mode(mode)
         distance = mode == "distance"
         parts = self._radius_parts(X, radius, need_distance=distance,
                                    sort_results=distance and sort_results)
-        return to_graph(parts, self.n_samples_fit_, mode=mode)
+        return neighbour_graph(parts, self.n_samples_fit_, mode=mode)
+
+
+def _check_graph_mode(mode):
+    if mode not in ("connectivity", "distance"):
+        raise ValueError('Unsupported mode, must be one of "connectivity", '
+                         f'or "distance" but got "{mode}" instead')
 
 
 def compute_weights(dist, weights):

@@ -298,10 +298,10 @@ def kneighbors_row_sharded(index, row_offset: int, n_total: int, Q, k: int, *,
 
 
 def _local_radius(index, Q, radius, need_distance, sort_results):
-    from .radius_result import concatenate
+    from .radius_result import RadiusCSR, join_batches
 
-    return concatenate(index.query_radius_csr(Q, radius, need_distance=need_distance,
-                                              sort_results=sort_results))
+    return RadiusCSR(*join_batches(index.query_radius_csr(Q, radius, need_distance=need_distance,
+                                                         sort_results=sort_results)))
 
 
 def _radius_part(index, row_offset, Q, radius, need, exclude_self, q_offset, local):

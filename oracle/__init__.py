@@ -42,11 +42,21 @@ _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 
 
+def reference_tree() -> str:
+    """Where the reference source tree is read from when it is present
+    (``MLXLEARN_REFERENCE``; the same variable the Makefile and the fixture
+    generator read)."""
+    return os.environ.get("MLXLEARN_REFERENCE", "/root/reference")
+
+
 def build() -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    """Compile liboracle.so and, when the reference tree exists, oracle/_ref
+    and the installed reference package (``make -C oracle refpkg``)."""
     subprocess.check_call(["make", "-s", "-C", _HERE, f"PY={sys.executable}"])
-    if os.path.isdir("/root/reference/src"):
-        subprocess.check_call(["make", "-s", "-C", _HERE, "ref", f"PY={sys.executable}"])
+    ref = reference_tree()
+    if os.path.isdir(os.path.join(ref, "src")):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "refpkg", f"PY={sys.executable}",
+                               f"REF={ref}"])
 
 
 def lib():

@@ -167,15 +167,23 @@ def test_pickle_roundtrip(rng):
 
 @gpu
 @pytest.mark.parametrize("weighted", [False, True])
-def test_device_radius_reductions_equal_host_bincount(weighted):
+def test_device_radius_reductions_equal_reference_reductions(weighted):
     # the device reductions sum each row in the order numpy's bincount does,
-    # so they must equal the host reductions over the downloaded CSR exactly;
-    # queries that coincide with training rows exercise the zero-distance rule
+    # so they must equal the reference's own host reductions
+    # (src/mlxlearn/_kernels/radius_reduce.py:36-72) over the downloaded CSR
+    # exactly; queries that coincide with training rows exercise the
+    # zero-distance rule
     import torch
 
     from mlxlearn_b200.index import build_index
-    from mlxlearn_b200.neighbors._votes import radius_mean, radius_votes
-    from mlxlearn_b200.radius_result import concatenate
+    from mlxlearn_b200.radius_result import join_batches
+    from oracle import refpkg
+
+    ref = refpkg.import_reference()
+    if ref is None:
+        pytest.skip("reference package not installed (make -C oracle refpkg)")
+    from mlxlearn._kernels.radius_reduce import reduce_mean_csr, reduce_votes_csr
+    from mlxlearn._kernels.radius_result import RadiusCSR as RefCSR
 
     rng = np.random.default_rng(31)
     X = rng.normal(size=(6000, 8)).astype(np.float32)
@@ -184,9 +192,9 @@ def test_device_radius_reductions_equal_host_bincount(weighted):
     targets = rng.normal(size=6000)
     ix = build_index(X)
     r = 1.9
-    csr = concatenate(ix.query_radius_csr(Q, r, need_distance=True))
-    hv, hc = radius_votes(csr, labels, 7, weighted=weighted)
-    hm, _ = radius_mean(csr, targets, weighted=weighted)
+    csr = RefCSR(*join_batches(ix.query_radius_csr(Q, r, need_distance=True)))
+    hv, hc = reduce_votes_csr(csr, labels, 7, weighted=weighted)
+    hm, _ = reduce_mean_csr(csr, targets, weighted=weighted)
     dev = torch.device("cuda", 0)
     dv, dc = ix.query_radius_reduce(Q, r, codes=torch.from_numpy(labels.astype(np.int32)).to(dev),
                                     n_classes=7, weighted=weighted)

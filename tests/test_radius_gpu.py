@@ -22,10 +22,9 @@ def make_index(X):
 
 
 def csr(parts):
-    from mlxlearn_b200.radius_result import concatenate
+    from mlxlearn_b200.radius_result import join_batches
 
-    j = concatenate(parts)
-    return j.indptr, j.indices, j.distances
+    return join_batches(parts)
 
 
 def test_radius_matches_reference_fixture():
