@@ -141,6 +141,15 @@ static int dalloc(T** p, size_t count, cudaStream_t st) {
 
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+static bool overlaps(const void* a, size_t an, const void* b, size_t bn);
+
+// Whether kNN outputs overlap the queries or each other (internal.cuh).
+bool buffers_overlap(const float* dQ, int64_t m, int d, int k, const double* dist,
+                     const int64_t* idx) {
+  const size_t q = (size_t)m * d * sizeof(float), o = (size_t)m * k * 8;
+  return overlaps(idx, o, dQ, q) || overlaps(dist, o, dQ, q) || overlaps(idx, o, dist, o);
+}
+
 static bool overlaps(const void* a, size_t an, const void* b, size_t bn) {
   if (!a || !b || !an || !bn) return false;
   auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);

@@ -521,6 +521,13 @@ __device__ __forceinline__ void exact_row(const ExactArgs& a, int64_t row, doubl
   const int C = *sh.count;
   if (C > kExactCap) {
     if (tid == 0) atomicCAS(a.status, DEV_OK, DEV_TOO_MANY_TIES);
+  } else if (C < a.k) {
+    // fewer than k comparable values: only a NaN query coordinate does this
+    // (the call reports it as non-finite input); leave a defined answer
+    for (int t = tid; t < a.k; t += kExactThreads) {
+      a.idx[orow * a.k + t] = -1;
+      if (a.dist) a.dist[orow * a.k + t] = __longlong_as_double(0x7ff8000000000000ll);
+    }
   } else if (tid < 32) {
     const unsigned cmp = warp_sort_resolve(cs, ci, C, a.k, q, a.X, a.d, tid);
     for (int t = tid; t < a.k; t += 32) {

@@ -231,6 +231,10 @@ int report_error(int code, const char* msg);  // sets b2k_last_error(), returns 
 int check_knn_args(const Index& ix, int64_t m, int32_t k, int32_t exclude_self,
                    int64_t q_offset);
 Index* index_of(b2k_index* h);
+// kNN outputs (m x k, 8-byte entries) overlapping the queries (m x d floats)
+// or each other; null outputs overlap nothing
+bool buffers_overlap(const float* dQ, int64_t m, int d, int k, const double* dist,
+                     const int64_t* idx);
 
 // ------------------------------------------------------------ row shards
 void launch_shard_merge(const double* D, const int64_t* I, int S, int64_t m, int kin, int kout,

@@ -65,10 +65,13 @@ int scratch_address(int device, unsigned char** out) {
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-// Bytes of scratch one call needs for m queries and k neighbours.
-size_t scratch_bytes(int64_t m, int k) {
+// Bytes of scratch one call needs for m queries and k neighbours.  The
+// exhaustive scan alone (unscreened calls) needs only the status and counter
+// blocks.
+size_t scratch_bytes(int64_t m, int k, bool screened) {
   const size_t m_pad = (size_t)((m + kSimtBM - 1) / kSimtBM) * kSimtBM;
   size_t b = 256 /*status*/ + 256 /*counters*/;
+  if (!screened) return b;
   b += align256(m_pad * sizeof(float));                       // E
   b += align256(m_pad * sizeof(int));                         // counts
   b += align256(m_pad * (size_t)k * sizeof(float));           // kth
@@ -93,13 +96,18 @@ extern "C" B2K_API int b2k_knn_device_noalloc(b2k_index* h, const float* dQ, int
   if (rc) return rc;
   if (m == 0) return B2K_OK;
   if (!dQ || !d_idx) return report_error(B2K_EINVAL, "queries and indices must not be NULL");
-  const size_t need = scratch_bytes(m, k);
+  if (buffers_overlap(dQ, m, ix.d, k, d_dist, d_idx))
+    return report_error(B2K_EINVAL, "output buffers must not overlap inputs or each other");
+  // the screen runs for in-range indexes and k <= 64; otherwise the
+  // exhaustive scan alone, which needs only the status block
+  const bool screened = ix.range_ok && k <= kMaxK;
+  const size_t need = scratch_bytes(m, k, screened);
   if (need > kNoAllocScratchBytes) {
     // largest batch that fits, for the message
     int64_t lo = 0, hi = m;
     while (lo < hi) {
       const int64_t mid = (lo + hi + 1) / 2;
-      if (scratch_bytes(mid, k) <= kNoAllocScratchBytes) lo = mid;
+      if (scratch_bytes(mid, k, screened) <= kNoAllocScratchBytes) lo = mid;
       else hi = mid - 1;
     }
     char msg[256];
@@ -136,8 +144,10 @@ extern "C" B2K_API int b2k_knn_device_noalloc(b2k_index* h, const float* dQ, int
   if (cudaMemsetAsync(status, 0, 256, st) != cudaSuccess ||
       cudaMemsetAsync(counters, 0, 256, st) != cudaSuccess)
     return report_error(B2K_ECUDA, "cudaMemsetAsync on the no-alloc scratch failed");
+  // NaN / inf queries: flagged on the device (status[5]) and reported after
+  // the search, which stays bounded on such inputs, as in b2k_knn_device
+  launch_nonfinite_check(dQ, m * (int64_t)ix.d, status + 5, st);
 
-  const bool screened = ix.range_ok && k <= kMaxK;
   if (screened) {
     QueryPrep qp{};
     qp.E = E;
@@ -197,6 +207,7 @@ extern "C" B2K_API int b2k_knn_device_noalloc(b2k_index* h, const float* dQ, int
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return report_error(B2K_ECUDA, "reading the device status failed");
+  if (hstatus[5]) return report_error(B2K_ENONFINITE, "training and query coordinates must be finite");
   if (hstatus[0] == DEV_TOO_MANY_TIES)
     return report_error(B2K_EUNSUPPORTED,
                         "too many training rows tie with a query's k-th neighbour");
