@@ -1,22 +1,35 @@
 """Benchmark: exact kNN queries/s at 1M x 128 reference rows, 100k queries, k=10.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload all|knn|small|pixels|radius|batch|chamfer]
 
-One step = kneighbors of the whole 100,000-query batch against the fitted
-1,000,000 x 128 float32 index (Gaussian mixture: 1,024 centres uniform in
-[-1,1]^128, sigma 0.1; reference rows seed 2, queries seed 3), k = 10.  The
-headline `value` is the bf16-screen + certified re-rank form with inputs
-resident in HBM; the plain fp32 form is measured in the same run
-(`plain_fp32`).  `e2e` goes through the public host API with pinned host
-buffers (query upload and result download inside the timed region).
+Headline (one step = kneighbors of the whole 100,000-query batch against the
+fitted 1,000,000 x 128 float32 index; Gaussian mixture: 1,024 centres uniform
+in [-1,1]^128, sigma 0.1; reference rows seed 2, queries seed 3; k = 10).
+`value` is the bf16-screen + certified re-rank form with inputs resident in
+HBM; the plain fp32 form is measured in the same run (`plain_fp32`); `e2e`
+goes through the public host API with page-locked host buffers (query upload
+and result download inside the timed region).  `cpu_baseline` is the
+reference's own stock route, NearestNeighbors(algorithm='brute').kneighbors
+from the installed reference package, on a bounded query sample; every query
+it answers is compared with ours (`parity_vs_cpu_reference`).
+
+The default run (N = 1) also measures the other four configurations and
+nests their lines under `secondary`: config 1 (10k x 64, k = 5), config 2b
+(60k x 784 integer pixels, k = 5), config 3 (radius classifier, 200k x 32),
+config 4 (256 uneven problems in one graph) and config 5 (differentiable kNN:
+Chamfer + self-kNN losses, forward and backward).  Each has its own roofline,
+CPU baseline (the reference's stock estimators), e2e figure and parity.
 
 Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
 index and answers its own 100,000 queries (weak scaling, no collective on the
-data path); time is the max over ranks.
+data path); time is the max over ranks.  Secondary configurations run at
+N = 1 only.
 
---impl reference times the reference's own CPU implementation of this path
-(mlxlearn's exact native scan, compiled from the reference sources into
-oracle/_ref) on the host cores, on bounded query samples.
+--impl reference times the reference's own CPU implementation of this path:
+mlxlearn's NearestNeighbors(n_neighbors=10, algorithm='brute').kneighbors
+(installed into baseline/_ref by `make -C oracle refpkg`; its CPUIndex route
+with the reference's native engines), one bounded query sample per step.
 """
 from __future__ import annotations
 
@@ -41,7 +54,13 @@ WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
 # Our kernels per kNN call: assign, bin_scan, scatter, gather (query grouping),
 # prep_queries, screen_tc, certify, exact (fallback rows; no-op when none).
 LAUNCHES_PER_STEP = 8
+# DRAM bytes (read + write) of one screen launch at the headline size, from the
+# ncu capture summarised in profiles/screen_tc_knn_gauss1Mx128.txt (a 10k-query
+# capture scaled by the (query tile, reference tile) pairs)
 SCREEN_TRAFFIC_BYTES = 5.77e9
+# FP32 CUDA-core rate (no measured figure): 148 SMs x 128 lanes x 2 FLOP x 1.965 GHz
+FP32_NOMINAL_TFLOPS = 74.4
+L2_FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
 
 
 def peaks():
@@ -117,38 +136,82 @@ def dist_env():
     return ws, rank, local
 
 
-def cpu_reference_time(X, Q, sample, threads, k=K):
-    """Time the reference's own exact CPU kNN scan (oracle/_ref) on a query sample.
+# ---------------------------------------------------------------------------
+# The reference's CPU path (checker and baseline only)
+# ---------------------------------------------------------------------------
 
-    Returns (queries/s, results (dist, idx), kind, cores).
-    """
-    import oracle
+def reference_neighbors():
+    """The reference's estimator module (installed package), or None."""
+    from oracle import refpkg
+
+    ref = refpkg.import_reference()
+    return None if ref is None else ref.neighbors
+
+
+def host_threads():
+    """Host threads the reference's CPU path uses (its BLAS pool and native
+    engines run on every core)."""
+    n = os.cpu_count() or 1
+    try:
+        from threadpoolctl import threadpool_info
+
+        blas = [p.get("num_threads", 0) for p in threadpool_info()]
+        if blas:
+            n = max(n, max(blas))
+    except Exception:
+        pass
+    return n
+
+
+def rel_err(ours, ref):
+    ours = np.asarray(ours, np.float64)
+    ref = np.asarray(ref, np.float64)
+    if ours.size == 0:
+        return 0.0
+    return float(np.max(np.abs(ours - ref) / np.maximum(np.abs(ref), 1e-300)))
+
+
+def stock_kneighbors(est, Q, block, seconds, max_queries):
+    """kneighbors of the fitted reference estimator over consecutive blocks
+    of `block` queries until `seconds` of CPU work or `max_queries`; returns
+    (queries/s, dist, idx, queries answered)."""
+    done, spent, ds, ix = 0, 0.0, [], []
+    while spent < seconds and done < max_queries:
+        t0 = time.perf_counter()
+        d, i = est.kneighbors(Q[done:done + block])
+        spent += time.perf_counter() - t0
+        ds.append(d)
+        ix.append(i)
+        done += len(i)
+    return done / spent, np.concatenate(ds), np.concatenate(ix), done
+
+
+def native_kneighbors(X, Q, k, threads):
+    """Fallback when the reference package is not installed: the reference's
+    native exact scan (oracle/_ref), else the oracle port.  Returns
+    (dist, idx, kind)."""
     from concurrent.futures import ThreadPoolExecutor
 
+    import oracle
+
     ref = oracle.ref_native()
-    Qs = np.ascontiguousarray(Q[:sample])
-    dist = np.empty((sample, k), np.float64)
-    idx = np.empty((sample, k), np.int64)
-    if ref is not None:
-        kind = "reference"
-        chunks = np.array_split(np.arange(sample), threads)
+    if ref is None:
+        d, i = oracle.knn(X, Q, k, nthreads=threads)
+        return d, i, "port"
+    Q = np.ascontiguousarray(Q)
+    dist = np.empty((len(Q), k))
+    idx = np.empty((len(Q), k), np.int64)
+    chunks = np.array_split(np.arange(len(Q)), threads)
 
-        def run(rows):
-            if len(rows):
-                a, b = rows[0], rows[-1] + 1
-                # reference: src/mlxlearn/_kernels/_neighbors_cpu_native.cpp:362-418 (GIL released)
-                ref.neighbors.query(X, Qs[a:b], k, False, 0, dist[a:b], idx[a:b])
+    def run(rows):
+        if len(rows):
+            a, b = rows[0], rows[-1] + 1
+            # reference: src/mlxlearn/_kernels/_neighbors_cpu_native.cpp:362-418 (GIL released)
+            ref.neighbors.query(X, Q[a:b], k, False, 0, dist[a:b], idx[a:b])
 
-        t0 = time.perf_counter()
-        with ThreadPoolExecutor(threads) as ex:
-            list(ex.map(run, chunks))
-        el = time.perf_counter() - t0
-    else:
-        kind = "port"
-        t0 = time.perf_counter()
-        dist, idx = oracle.knn(X, Qs, k, nthreads=threads)
-        el = time.perf_counter() - t0
-    return sample / el, (dist, idx), kind
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(run, chunks))
+    return dist, idx, "reference"
 
 
 def run_reference_arm(args):
@@ -158,32 +221,109 @@ def run_reference_arm(args):
     from datasets import cfg2a
 
     X, Q = cfg2a(N_REF, N_QUERY, D)
-    threads = os.cpu_count() or 1
-    # 16 queries per host thread per call: enough to amortise the scan's
-    # per-call work (the full batch is one call of 100k queries); ~4 s per step
-    sample = max(threads, int(os.environ.get("B2K_REF_SAMPLE", "0")) or threads * 16)
-    vals = []
+    threads = host_threads()
+    sample = int(os.environ.get("B2K_REF_SAMPLE", "256"))
+    nb = reference_neighbors()
+    if nb is not None:
+        est = nb.NearestNeighbors(n_neighbors=K, algorithm="brute").fit(X)
+        route = ("mlxlearn NearestNeighbors(n_neighbors=10, algorithm='brute').kneighbors "
+                 "(installed reference, CPUIndex route with its native engines)")
+    else:
+        est, route = None, "mlxlearn's native exact scan (oracle/_ref)"
+    times = []
     kind = "reference"
     for step in range(args.warmup + args.steps):
-        qps, _, kind = cpu_reference_time(X, Q[(step * sample) % N_QUERY:], sample, threads)
+        Qs = Q[(step * sample) % N_QUERY:][:sample]
+        t0 = time.perf_counter()
+        if est is not None:
+            est.kneighbors(Qs)
+        else:
+            _, _, kind = native_kneighbors(X, Qs, K, threads)
+        el = time.perf_counter() - t0
         if step >= args.warmup:
-            vals.append(qps)
-    value = statistics.median(vals)
+            times.append(el)
+    step_s = statistics.median(times)
+    value = sample / step_s
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * N_QUERY / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000.0 * step_s, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_ref": N_REF, "d": D, "n_query": N_QUERY, "k": K},
+        "config": {"workload": WORKLOAD, "n_ref": N_REF, "d": D, "n_query": N_QUERY, "k": K,
+                   "step": f"{sample} consecutive queries of the {N_QUERY}-query batch"},
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": kind,
-                         "sample": f"{sample} queries per step of the {N_QUERY}-query batch; "
-                                   "ms_per_step extrapolates to the full batch"},
+                         "sample": f"{sample} queries per step through {route}"},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
+
+# ---------------------------------------------------------------------------
+# Device timing helpers
+# ---------------------------------------------------------------------------
+
+class L2Flush:
+    """Writes a buffer larger than L2 between timed iterations."""
+
+    def __init__(self, device):
+        import torch
+
+        self.buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def __call__(self):
+        self.buf.fill_(1.0)
+
+
+def event_times(fn, steps, warmup, flush=None):
+    """Per-step device times (ms) of fn on the current stream, each step
+    bracketed by CUDA events; `flush` (untimed) runs before every step."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(steps):
+        if flush is not None:
+            flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def wall_times(fn, steps, warmup):
+    """Per-step wall times (s) of a host-facing call that synchronises."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        out.append(time.perf_counter() - t0)
+    return out
+
+
+def tensor_roofline(kernel, flops, seconds, peak_tf, peak_kind, peak_name="burst bf16"):
+    achieved = flops / seconds / 1e12
+    return {"kernel": kernel, "bound": "tensor", "achieved": achieved, "peak": peak_tf,
+            "unit": "TFLOP/s", "frac": achieved / peak_tf,
+            "peak_source": f"{peak_kind} {peak_name}", "traffic": None}
+
+
+# ---------------------------------------------------------------------------
+# Headline
+# ---------------------------------------------------------------------------
 
 def run_ours(args):
     import torch
@@ -198,15 +338,12 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
-    from datasets import cfg2a
-    from mlxlearn_b200 import _lib
+    from datasets import cfg2a, mixture
     from mlxlearn_b200.index import build_index
     from mlxlearn_b200.sharding import max_over_ranks
 
     X, _ = cfg2a(N_REF, 1, D)
     # each rank answers its own query shard (weak scaling)
-    from datasets import mixture
-
     C = np.random.default_rng(2).uniform(-1, 1, (1024, D))
     Q, _ = mixture(np.random.default_rng(3 + 1000 * rank), N_QUERY, C, 0.1)
     index = build_index(X, device=local)
@@ -241,7 +378,7 @@ def run_ours(args):
     clocks = clk.summary()
     ms_fp32, st_fp32 = timed("fp32", max(1, min(2, args.steps)), 1)
 
-    # e2e: public host API, pinned host buffers, copies inside the timed region
+    # e2e: public host API, page-locked host buffers, copies inside the timed region
     Qh = torch.from_numpy(Q).pin_memory().numpy()
     out_i = torch.empty((N_QUERY, K), dtype=torch.int64).pin_memory().numpy()
     out_d = torch.empty((N_QUERY, K), dtype=torch.float64).pin_memory().numpy()
@@ -261,13 +398,15 @@ def run_ours(args):
         tf_burst, tf_sust, hbm, peak_kind = peaks()
         flops = 2.0 * N_REF * D * N_QUERY
         screen_ms = statistics.median(s["screen_ms"] for s in st_bf16)
-        achieved = flops / (screen_ms * 1e-3) / 1e12
         total_timed_s = ms_bf16 * args.steps / 1000.0
         peak = tf_sust if total_timed_s > 1.0 else tf_burst
-        fp32_screen_ms = statistics.median(s["screen_ms"] for s in st_fp32)
-        # DRAM bytes (read + write) of one screen launch, from the ncu capture in
-        # profiles/screen_tc_knn_gauss1Mx128.txt (10k queries, scaled by tile pairs)
+        roof = tensor_roofline("screen_tc_kernel (bf16 tcgen05 distance tile)", flops,
+                               screen_ms * 1e-3, peak, peak_kind,
+                               "sustained bf16" if peak == tf_sust else "burst bf16")
+        roof["algorithmic_flops_per_launch"] = flops
         traffic = os.environ.get("B2K_SCREEN_TRAFFIC_BYTES", SCREEN_TRAFFIC_BYTES)
+        roof["traffic"] = None if traffic is None else float(traffic)
+        fp32_screen_ms = statistics.median(s["screen_ms"] for s in st_fp32)
         result = {
             "metric": METRIC,
             "value": ws * N_QUERY / (ms_bf16 / 1000.0),
@@ -281,16 +420,14 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "n_ref": N_REF, "d": D, "n_query": N_QUERY, "k": K,
                        "queries_per_gpu": N_QUERY, "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (bf16 index 256 MB, fp32 index 512 MB)"},
-            "roofline": {"kernel": "screen_tc_kernel (bf16 tcgen05 distance tile)",
-                         "bound": "tensor", "achieved": achieved,
-                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "peak_source": f"{peak_kind} "
-                                        f"{'sustained' if peak == tf_sust else 'burst'} bf16",
-                         "algorithmic_flops_per_launch": flops,
-                         "traffic": None if traffic is None else float(traffic)},
+            "roofline": roof,
             "plain_fp32": {"value": ws * N_QUERY / (ms_fp32 / 1000.0), "unit": "queries/s",
+                           "form": "fp32 CUDA-core screen (screen_simt_kernel) + the same "
+                                   "certify pass",
                            "ms_per_step": ms_fp32, "screen_ms": fp32_screen_ms,
                            "screen_tflops": flops / (fp32_screen_ms * 1e-3) / 1e12,
+                           "screen_frac_of_fp32_nominal":
+                               flops / (fp32_screen_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
                            "bf16_speedup": ms_fp32 / ms_bf16},
             "screen_stats": {k: v for k, v in st_bf16[-1].items()},
             "e2e": {"value": ws * N_QUERY / e2e_s, "unit": "queries/s",
@@ -299,208 +436,274 @@ def run_ours(args):
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": clocks,
         }
-        # CPU baseline: the reference's exact CPU scan on a bounded sample, with
-        # our answers for the same queries compared against it.
-        threads = os.cpu_count() or 1
-        # a bounded sample of about 10 s of CPU work: calls of 16 queries per
-        # thread (amortising the scan's per-call work, as the full batch does)
-        # until 10 s have passed (at most 30 calls)
-        block = 16 * threads
-        done, spent, first = 0, 0.0, None
-        while spent < float(os.environ.get("B2K_CPU_SECONDS", "10")) and done < 30 * block:
-            t_b = time.perf_counter()
-            qps_b, res_b, kind = cpu_reference_time(X, Q[done:], block, threads)
-            spent += time.perf_counter() - t_b
-            if first is None:
-                first = res_b
-            done += block
-        qps = done / spent
-        sample = min(block, 64)  # parity: the first 64 queries of the first call
-        rd, ri = first[0][:sample], first[1][:sample]
-        od, oi = index.query(Q[:sample], K, mode="bf16")
-        rel = np.max(np.abs(od - rd) / np.maximum(rd, 1e-300))
-        result["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": threads,
-                                  "kind": kind,
-                                  "sample": f"first {done} queries of the batch, k={K} "
-                                            f"({spent:.1f} s of CPU work)"}
-        result["parity_vs_cpu_reference"] = {"queries": sample,
-                                             "indices_bit_exact": bool(np.array_equal(oi, ri)),
-                                             "max_rel_dist_err": float(rel)}
+        result.update(headline_cpu_baseline(X, Q, index))
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+    if result is not None and ws == 1 and args.workload == "all":
+        result["secondary"] = run_secondaries(args)
     if result is not None:
         print(json.dumps(result), flush=True)
     return 0
 
 
+def headline_cpu_baseline(X, Q, index):
+    """The reference's stock route on a bounded sample (~10 s of CPU work),
+    and every query it answered compared with ours."""
+    threads = host_threads()
+    seconds = float(os.environ.get("B2K_CPU_SECONDS", "10"))
+    nb = reference_neighbors()
+    if nb is not None:
+        est = nb.NearestNeighbors(n_neighbors=K, algorithm="brute").fit(X)
+        qps, rd, ri, done = stock_kneighbors(est, Q, 256, seconds, 4096)
+        kind, route = "reference", ("NearestNeighbors(n_neighbors=10, algorithm='brute')."
+                                    "kneighbors, installed reference (CPUIndex route)")
+    else:
+        done = 16 * threads
+        t0 = time.perf_counter()
+        rd, ri, kind = native_kneighbors(X, Q[:done], K, threads)
+        qps = done / (time.perf_counter() - t0)
+        route = "the reference's native exact scan"
+    od, oi = index.query(Q[:done], K, mode="bf16")
+    return {
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": kind,
+                         "sample": f"first {done} queries of the batch in blocks of 256 "
+                                   f"through {route}"},
+        "parity_vs_cpu_reference": {"queries": int(done),
+                                    "indices_bit_exact": bool(np.array_equal(oi, ri)),
+                                    "max_rel_dist_err": rel_err(od, rd)},
+    }
+
+
 # ---------------------------------------------------------------------------
-# Secondary workloads (not the headline line): --workload pixels|radius|small
+# Secondary configurations (nested under "secondary"; --workload NAME alone)
 # ---------------------------------------------------------------------------
 
-def _radius_threshold_tuple(d, R2):
-    """(R2, f64_in, f64_out, prune_above, bulk_below) as the reference's
-    radius extension takes it (src/mlxlearn/_kernels/radius_contract.py:129-153,
-    radius_cpu.py:137-140)."""
-    import math
-
-    down = lambda v: math.nextafter(v, -math.inf)  # noqa: E731
-    up = lambda v: math.nextafter(v, math.inf)  # noqa: E731
-    u = 2.0 ** -53
-    g = (d + 2) * u / (1.0 - (d + 2) * u)
-    f_in = max(down(down(R2 * down(1.0 - 2.0 * g))), 0.0)
-    f_out = up(up(R2 * up(1.0 + 2.0 * g)))
-    prune = up(up(R2 * up(1.0 + 4.0 * g)))
-    bulk = max(down(down(R2 * down(1.0 - 4.0 * g))), 0.0)
-    return (float(R2), f_in, f_out, prune, bulk)
+def _steps(args, cap=10):
+    return max(1, min(args.steps, cap)), max(3, min(args.warmup, 5))
 
 
-def _timed_wall(fn, steps, warmup):
+def sec_small(args):
+    """Config 1: NearestNeighbors(n_neighbors=5, brute) on 10,000 x 64 N(0,1)
+    rows (seed 0), 2,000 queries (seed 1)."""
     import torch
 
-    for _ in range(warmup):
-        fn()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        out = fn()
-    torch.cuda.synchronize()
-    return (time.perf_counter() - t0) / steps, out
-
-
-def run_secondary(args):
-    import torch
-
-    from mlxlearn_b200.index import build_index
-    from mlxlearn_b200.neighbors import KNeighborsClassifier, NearestNeighbors
-    from mlxlearn_b200.neighbors import RadiusNeighborsClassifier
-
-    torch.cuda.set_device(0)
-    threads = os.cpu_count() or 1
-    line = {"metric": None, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "data": "synthetic", "workload_kind": "secondary"}
     import oracle
+    from datasets import cfg1
+    from mlxlearn_b200.neighbors import NearestNeighbors
 
-    ref = oracle.ref_native()
-    if args.workload == "pixels":
-        from datasets import cfg2b
-
-        X, Q, y = cfg2b()
-        k = 5
-        clf = KNeighborsClassifier(n_neighbors=k).fit(X, y)
-        Qd = torch.from_numpy(Q).cuda()
-        ms = 1000 * _timed_wall(lambda: clf._index_.query_device(Qd, k, mode="bf16"),
-                                args.steps, args.warmup)[0]
-        e2e_s, pred = _timed_wall(lambda: clf.predict(Q), args.steps, args.warmup)
-        st = clf._index_.query_device(Qd, k, mode="bf16", stats=True) and clf._index_.last_stats
-        sample = min(len(Q), 4 * threads)
-        rd = np.empty((sample, k)); ri = np.empty((sample, k), np.int64)
+    X, Q = cfg1()
+    k = 5
+    steps, warmup = _steps(args)
+    nn = NearestNeighbors(n_neighbors=k, algorithm="brute", metric="euclidean").fit(X)
+    index = nn._index_
+    Qd = torch.from_numpy(Q).cuda()
+    flush = L2Flush(Qd.device)
+    ms = statistics.median(event_times(lambda: index.query_device(Qd, k), steps, warmup, flush))
+    index.query_device(Qd, k, stats=True)
+    st = index.last_stats
+    e2e_s = statistics.median(wall_times(lambda: nn.kneighbors(Q), steps, warmup))
+    od, oi = nn.kneighbors(Q)
+    tf_burst, _, _, peak_kind = peaks()
+    line = {
+        "metric": "NearestNeighbors(n_neighbors=5).kneighbors queries/s, 10000 x 64",
+        "value": len(Q) / (ms / 1000), "unit": "queries/s", "ms_per_step": ms,
+        "steps": steps, "warmup": warmup, "dtype": "bf16" if st["mode_used"] == 2 else "f32",
+        "config": {"workload": "knn_gauss_10000x64_2000q_k5",
+                   "l2": "inputs smaller than L2: L2 flushed (256 MB write) before every step"},
+        "roofline": tensor_roofline("screen_tc_kernel (launch/latency bound at this size)",
+                                    2.0 * X.shape[0] * X.shape[1] * len(Q),
+                                    st["screen_ms"] * 1e-3, tf_burst, peak_kind),
+        "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": Q.nbytes,
+                "d2h_bytes_per_step": oi.nbytes + od.nbytes,
+                "api": "NearestNeighbors.kneighbors (host arrays)"},
+    }
+    threads = host_threads()
+    nb = reference_neighbors()
+    ed, ei = oracle.knn(X, Q, k)
+    if nb is not None:
+        est = nb.NearestNeighbors(n_neighbors=k, algorithm="brute", metric="euclidean").fit(X)
+        est.kneighbors(Q[:64])
         t0 = time.perf_counter()
-        _ref_knn_threads(ref, X, Q[:sample], k, rd, ri, threads)
-        cpu_qps = sample / (time.perf_counter() - t0)
-        od, oi = clf.kneighbors(Q[:sample])
-        line.update({"metric": "KNeighborsClassifier(k=5).predict queries/s, 60k x 784 pixels",
-                     "value": len(Q) / (ms / 1000), "ms_per_step": ms, "dtype": "bf16",
-                     "config": {"workload": "knn_pixels_60000x784_10000q_k5"},
-                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
-                             "api": "KNeighborsClassifier.predict (host arrays)"},
-                     "screen_stats": st,
-                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
-                                      "kind": "reference" if ref else "port",
-                                      "sample": f"first {sample} queries"},
-                     "parity_vs_cpu_reference": {"indices_bit_exact": bool(np.array_equal(oi, ri)),
-                                                 "max_rel_dist_err": float(np.max(
-                                                     np.abs(od - rd) / np.maximum(rd, 1e-300)))}})
-    elif args.workload == "radius":
-        from datasets import cfg3
-
-        X, y, Q = cfg3()
-        index = build_index(X)
-        # radius: median 50th-neighbour distance over a 1000-query sample
-        d50, _ = index.query(Q[:1000], 50)
-        r = float(np.median(d50[:, -1]))
-        clf = RadiusNeighborsClassifier(radius=r, outlier_label="most_frequent").fit(X, y)
-        e2e_s, pred = _timed_wall(lambda: clf.predict(Q), args.steps, args.warmup)
-        csr_s, parts = _timed_wall(lambda: clf._index_.query_radius_csr(Q, r),
-                                   args.steps, args.warmup)
-        p = parts[0]
-        sample = min(len(Q), 16 * threads)
+        rd, ri = est.kneighbors(Q)
+        cpu_s, kind = time.perf_counter() - t0, "reference"
+    else:
         t0 = time.perf_counter()
-        ok = None
-        if ref is not None:
-            thr = _radius_threshold_tuple(X.shape[1], r * r)
-            res = ref.radius.brute_query(X, np.ascontiguousarray(Q[:sample]), thr, 0, False, 1,
-                                         threads)
-            cpu_qps = sample / (time.perf_counter() - t0)
-            nq, nnz = ref.radius.result_sizes(res)
-            counts = np.empty(nq, np.int64)
-            ref.radius.result_counts(res, counts)
-            ip = np.zeros(nq + 1, np.int64)
-            np.cumsum(counts, out=ip[1:])
-            ix = np.empty(nnz, np.int64); dd = np.empty(nnz)
-            ref.radius.result_fill_csr(res, ip, ix, dd, threads)
-            ok = (bool(np.array_equal(ip, p.indptr[:sample + 1]))
-                  and bool(np.array_equal(ix, p.indices[:ip[-1]]))
-                  and bool(np.array_equal(dd, p.distances[:ip[-1]])))
-        else:
-            oracle.radius(X, Q[:sample], r)
-            cpu_qps = sample / (time.perf_counter() - t0)
-        line.update({"metric": "RadiusNeighborsClassifier.predict queries/s, 200k x 32",
-                     "value": len(Q) / csr_s, "ms_per_step": 1000 * csr_s, "dtype": "bf16",
-                     "config": {"workload": "radius_200000x32_50000q", "radius": r,
-                                "median_neighbours": float(np.median(p.lengths())),
-                                "zero_neighbour_queries": int((p.lengths() == 0).sum()),
-                                "nnz": p.nnz,
-                                "value_note": "query_radius_csr through the host C ABI "
-                                              "(upload, screen, exact classify, CSR download)"},
-                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
-                             "api": "RadiusNeighborsClassifier.predict (host arrays)"},
-                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
-                                      "kind": "reference" if ref else "port",
-                                      "sample": f"first {sample} queries, brute_query"},
-                     "parity_vs_cpu_reference": {"csr_bit_exact": ok}})
-    else:  # small: config 1
-        from datasets import cfg1
+        rd, ri, kind = native_kneighbors(X, Q, k, threads)
+        cpu_s = time.perf_counter() - t0
+    line["cpu_baseline"] = {"value": len(Q) / cpu_s, "unit": "queries/s", "cores": threads,
+                            "kind": kind, "sample": "all 2000 queries, NearestNeighbors(brute)"
+                                                    ".kneighbors of the installed reference"}
+    line["parity"] = {"queries": len(Q), "indices_bit_exact_vs_reference":
+                      bool(np.array_equal(oi, ri)),
+                      "max_rel_dist_err_vs_reference": rel_err(od, rd),
+                      "indices_bit_exact_vs_fp64_oracle": bool(np.array_equal(oi, ei)),
+                      "max_rel_dist_err_vs_fp64_oracle": rel_err(od, ed)}
+    return line
 
-        X, Q = cfg1()
-        nn = NearestNeighbors(n_neighbors=5, algorithm="brute", metric="euclidean").fit(X)
-        Qd = torch.from_numpy(Q).cuda()
-        ms = 1000 * _timed_wall(lambda: nn._index_.query_device(Qd, 5), args.steps,
-                                args.warmup)[0]
-        e2e_s, (od, oi) = _timed_wall(lambda: nn.kneighbors(Q), args.steps, args.warmup)
-        rd = np.empty((len(Q), 5)); ri = np.empty((len(Q), 5), np.int64)
+
+def sec_pixels(args):
+    """Config 2b: 60,000 x 784 integer pixels, 10,000 queries, k = 5."""
+    import torch
+
+    import oracle
+    from datasets import cfg2b
+    from mlxlearn_b200.neighbors import KNeighborsClassifier
+
+    X, Q, y = cfg2b()
+    k = 5
+    steps, warmup = _steps(args)
+    clf = KNeighborsClassifier(n_neighbors=k).fit(X, y)
+    index = clf._index_
+    Qd = torch.from_numpy(Q).cuda()
+    flush = L2Flush(Qd.device)
+    ms = statistics.median(event_times(lambda: index.query_device(Qd, k, mode="bf16"), steps,
+                                       warmup, flush))
+    index.query_device(Qd, k, mode="bf16", stats=True)
+    st = index.last_stats
+    e2e_s = statistics.median(wall_times(lambda: clf.predict(Q), steps, warmup))
+    pred = clf.predict(Q)
+    tf_burst, _, _, peak_kind = peaks()
+    line = {
+        "metric": "kneighbors queries/s (k=5), 60000 x 784 integer pixels; e2e = "
+                  "KNeighborsClassifier.predict",
+        "value": len(Q) / (ms / 1000), "unit": "queries/s", "ms_per_step": ms,
+        "steps": steps, "warmup": warmup, "dtype": "bf16",
+        "config": {"workload": "knn_pixels_60000x784_10000q_k5",
+                   "l2": "bf16 operand 94 MB: L2 flushed (256 MB write) before every step"},
+        "roofline": tensor_roofline("screen_tc_kernel (bf16 tcgen05 distance tile)",
+                                    2.0 * X.shape[0] * X.shape[1] * len(Q),
+                                    st["screen_ms"] * 1e-3, tf_burst, peak_kind),
+        "screen_stats": st,
+        "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": Q.nbytes,
+                "d2h_bytes_per_step": pred.nbytes,
+                "api": "KNeighborsClassifier.predict (host arrays; votes on the device)"},
+    }
+    threads = host_threads()
+    nb = reference_neighbors()
+    sample = min(len(Q), int(os.environ.get("B2K_PIXELS_CPU_QUERIES", "2000")))
+    od, oi = clf.kneighbors(Q[:sample])
+    ed, ei = oracle.knn(X, Q[:200], k)
+    if nb is not None:
+        ref = nb.KNeighborsClassifier(n_neighbors=k).fit(X, y)
+        ref.predict(Q[:64])
         t0 = time.perf_counter()
-        _ref_knn_threads(ref, X, Q, 5, rd, ri, threads)
-        cpu_qps = len(Q) / (time.perf_counter() - t0)
-        line.update({"metric": "NearestNeighbors(k=5).kneighbors queries/s, 10000 x 64",
-                     "value": len(Q) / (ms / 1000), "ms_per_step": ms, "dtype": "auto",
-                     "config": {"workload": "knn_gauss_10000x64_2000q_k5"},
-                     "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s",
-                             "api": "NearestNeighbors.kneighbors (host arrays)"},
-                     "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": threads,
-                                      "kind": "reference" if ref else "port",
-                                      "sample": "all 2000 queries"},
-                     "parity_vs_cpu_reference": {
-                         "queries": len(Q), "indices_bit_exact": bool(np.array_equal(oi, ri)),
-                         "max_rel_dist_err": float(np.max(np.abs(od - rd) /
-                                                          np.maximum(rd, 1e-300)))}})
-    print(json.dumps(line), flush=True)
-    return 0
+        rpred = ref.predict(Q[:sample])
+        cpu_s, kind = time.perf_counter() - t0, "reference"
+        rd, ri = ref.kneighbors(Q[:sample])
+        pred_equal = bool(np.array_equal(pred[:sample], rpred))
+    else:
+        t0 = time.perf_counter()
+        rd, ri, kind = native_kneighbors(X, Q[:sample], k, threads)
+        cpu_s, pred_equal = time.perf_counter() - t0, None
+    line["cpu_baseline"] = {"value": sample / cpu_s, "unit": "queries/s", "cores": threads,
+                            "kind": kind, "sample": f"first {sample} queries, "
+                                                    "KNeighborsClassifier(5).predict of the "
+                                                    "installed reference"}
+    line["parity"] = {"queries": sample, "indices_bit_exact_vs_reference":
+                      bool(np.array_equal(oi, ri)),
+                      "max_rel_dist_err_vs_reference": rel_err(od, rd),
+                      "predictions_equal_reference": pred_equal,
+                      "indices_bit_exact_vs_fp64_oracle_200q":
+                          bool(np.array_equal(oi[:200], ei)),
+                      "max_rel_dist_err_vs_fp64_oracle_200q": rel_err(od[:200], ed)}
+    return line
 
 
-def run_batch(args):
-    """256 uneven problems (seed 5) as one planned batch vs one call per problem."""
+def sec_radius(args):
+    """Config 3: RadiusNeighborsClassifier on 200,000 x 32 (10-class mixture),
+    50,000 queries, radius = median 50th-neighbour distance of 1,000 queries."""
+    import oracle
+    from datasets import cfg3
+    from mlxlearn_b200.index import build_index
+    from mlxlearn_b200.neighbors import RadiusNeighborsClassifier
+    from mlxlearn_b200.radius_result import join_batches
+
+    X, y, Q = cfg3()
+    steps, warmup = _steps(args, cap=5)
+    index = build_index(X)
+    d50, _ = index.query(Q[:1000], 50)
+    r = float(np.median(d50[:, -1]))
+    clf = RadiusNeighborsClassifier(radius=r, outlier_label="most_frequent").fit(X, y)
+    csr_s = statistics.median(wall_times(lambda: clf._index_.query_radius_csr(Q, r),
+                                         steps, warmup))
+    e2e_s = statistics.median(wall_times(lambda: clf.predict(Q), steps, warmup))
+    pred = clf.predict(Q)
+    ip, ix, dd = join_batches(clf._index_.query_radius_csr(Q, r))
+    tf_burst, _, hbm, peak_kind = peaks()
+    nnz = int(ip[-1])
+    lengths = np.diff(ip)
+    # HBM roofline of the whole call: the index streamed twice by the two
+    # screen passes (bf16) plus 16 B per returned neighbour, over the call time
+    moved = 2 * X.shape[0] * 64 + 16 * nnz
+    line = {
+        "metric": "radius neighbourhoods (CSR) queries/s, 200000 x 32; e2e = "
+                  "RadiusNeighborsClassifier.predict",
+        "value": len(Q) / csr_s, "unit": "queries/s", "ms_per_step": 1000 * csr_s,
+        "steps": steps, "warmup": warmup, "dtype": "bf16",
+        "config": {"workload": "radius_200000x32_50000q", "radius": r,
+                   "median_neighbours": float(np.median(lengths)),
+                   "zero_neighbour_queries": int((lengths == 0).sum()), "nnz": nnz,
+                   "value_note": "query_radius_csr through the host C ABI (upload, two "
+                                 "screen passes, exact classify, CSR download)"},
+        "roofline": {"kernel": "whole radius call", "bound": "tensor",
+                     "achieved": 2.0 * X.shape[0] * X.shape[1] * len(Q) / csr_s / 1e12,
+                     "peak": tf_burst, "unit": "TFLOP/s",
+                     "frac": 2.0 * X.shape[0] * X.shape[1] * len(Q) / csr_s / 1e12 / tf_burst,
+                     "peak_source": f"{peak_kind} burst bf16", "traffic": None,
+                     "hbm_gbs_of_call": moved / csr_s / 1e9},
+        "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": Q.nbytes,
+                "d2h_bytes_per_step": pred.nbytes,
+                "api": "RadiusNeighborsClassifier.predict (host arrays; votes on the device)"},
+    }
+    threads = host_threads()
+    nb = reference_neighbors()
+    sample = min(len(Q), int(os.environ.get("B2K_RADIUS_CPU_QUERIES", "4000")))
+    ip_s = ip[:sample + 1]
+    ix_s, dd_s = ix[:ip_s[-1]], dd[:ip_s[-1]]
+    eip, eix, edd = oracle.radius(X, Q[:500], r)
+    oracle_ok = (bool(np.array_equal(ip[:501], eip)) and bool(np.array_equal(ix[:eip[-1]], eix))
+                 and bool(np.array_equal(dd[:eip[-1]], edd)))
+    if nb is not None:
+        ref = nb.RadiusNeighborsClassifier(radius=r, outlier_label="most_frequent").fit(X, y)
+        ref.predict(Q[:64])
+        t0 = time.perf_counter()
+        rpred = ref.predict(Q[:sample])
+        cpu_s, kind = time.perf_counter() - t0, "reference"
+        rd, ri = ref.radius_neighbors(Q[:sample])
+        rl = np.array([len(a) for a in ri], np.int64)
+        rip = np.concatenate([[0], np.cumsum(rl)])
+        csr_ok = (bool(np.array_equal(rip, ip_s)) and
+                  bool(np.array_equal(np.concatenate(ri), ix_s)))
+        err = rel_err(dd_s, np.concatenate(rd))
+        pred_equal = bool(np.array_equal(pred[:sample], rpred))
+    else:
+        t0 = time.perf_counter()
+        rip, rix, rdd = oracle.radius(X, Q[:sample], r, nthreads=threads)
+        cpu_s, kind = time.perf_counter() - t0, "port"
+        csr_ok = bool(np.array_equal(rip, ip_s)) and bool(np.array_equal(rix, ix_s))
+        err, pred_equal = rel_err(dd_s, rdd), None
+    line["cpu_baseline"] = {"value": sample / cpu_s, "unit": "queries/s", "cores": threads,
+                            "kind": kind, "sample": f"first {sample} queries, "
+                                                    "RadiusNeighborsClassifier.predict of the "
+                                                    "installed reference"}
+    line["parity"] = {"queries": sample, "csr_indices_bit_exact_vs_reference": csr_ok,
+                      "max_rel_dist_err_vs_reference": err,
+                      "predictions_equal_reference": pred_equal,
+                      "csr_bit_exact_vs_fp64_oracle_500q": oracle_ok}
+    return line
+
+
+def sec_batch(args):
+    """Config 4: 256 uneven problems (seed 5) as one planned batch (one CUDA
+    graph) vs one call per problem."""
     import torch
 
     from datasets import cfg4
     from mlxlearn_b200.batch import KnnBatch
     from mlxlearn_b200.index import build_index
 
-    import oracle
-
     torch.cuda.set_device(0)
-    threads = os.cpu_count() or 1
     problems = cfg4(problems=args.problems)
     total_q = sum(Q.shape[0] for _, Q, _ in problems)
     flops = sum(2.0 * X.shape[0] * Q.shape[0] * X.shape[1] for X, Q, _ in problems)
@@ -514,25 +717,26 @@ def run_batch(args):
     t0 = time.perf_counter()
     batch = KnnBatch(items, autotune=not args.profile)
     plan_s = time.perf_counter() - t0
-    stream = torch.cuda.current_stream()
     if args.profile:  # profiling driver: the batched runs only
         for _ in range(args.warmup + args.steps):
             batch.run()
-        print(json.dumps({"profile": True, "stats": batch.finish()}), flush=True)
+        out = {"profile": True, "stats": batch.finish()}
         batch.close()
-        return 0
-    for _ in range(args.warmup):
+        return out
+    steps, warmup = _steps(args)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
         batch.run()
     batch.finish()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         torch.cuda.synchronize()
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             batch.run()
         ev1.record(stream)
         stats = batch.finish()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     # one call per problem through the single-problem device API
     for ix, q, (_, _, k) in zip(indexes, Qd, problems):
         ix.query_device(q, k)
@@ -542,7 +746,7 @@ def run_batch(args):
         ix.query_device(q, k)
     torch.cuda.synchronize()
     one_s = time.perf_counter() - t0
-    # e2e: pinned host queries in, results out, through the batch object
+    # e2e: page-locked host queries in, results out, through the batch object
     Qh = [torch.from_numpy(Q).pin_memory() for _, Q, _ in problems]
     Dh = [torch.empty(d.shape, dtype=d.dtype).pin_memory() for d in batch.dist]
     Ih = [torch.empty(i.shape, dtype=i.dtype).pin_memory() for i in batch.idx]
@@ -558,73 +762,73 @@ def run_batch(args):
             dst.copy_(src, non_blocking=True)
         torch.cuda.synchronize()
 
-    e2e_s = _timed_wall(e2e_step, args.steps, 1)[0]
+    e2e_s = statistics.median(wall_times(e2e_step, steps, 1))
     h2d = sum(q.numel() * 4 for q in Qh)
     d2h = sum(d.numel() * 8 for d in Dh) + sum(i.numel() * 8 for i in Ih)
-    # parity + CPU baseline: the reference's exact scan on a few queries of every problem
-    ref = oracle.ref_native()
+    # CPU baseline + parity: the reference's stock kneighbors on the first
+    # queries of every problem, time scaled by each problem's query count
+    threads = host_threads()
+    nb = reference_neighbors()
     per = int(os.environ.get("B2K_BATCH_CPU_QUERIES", "4"))
     est_cpu_s, sample_q, exact, rel = 0.0, 0, True, 0.0
+    kind = "reference"
     for (X, Q, k), d, i in zip(problems, batch.dist, batch.idx):
         s = min(per, Q.shape[0])
-        rd = np.empty((s, k)); ri = np.empty((s, k), np.int64)
-        t1 = time.perf_counter()
-        _ref_knn_threads(ref, X, Q[:s], k, rd, ri, min(threads, s))
-        est_cpu_s += (time.perf_counter() - t1) * Q.shape[0] / s
+        if nb is not None:
+            est = nb.NearestNeighbors(n_neighbors=k, algorithm="brute").fit(X)
+            t1 = time.perf_counter()
+            rd, ri = est.kneighbors(Q[:s])
+            el = time.perf_counter() - t1
+        else:
+            t1 = time.perf_counter()
+            rd, ri, kind = native_kneighbors(X, Q[:s], k, min(threads, s))
+            el = time.perf_counter() - t1
+        est_cpu_s += el * Q.shape[0] / s
         sample_q += s
         exact &= bool(np.array_equal(ri, i[:s].cpu().numpy()))
-        od = d[:s].cpu().numpy()
-        rel = max(rel, float(np.max(np.abs(od - rd) / np.maximum(rd, 1e-300))))
+        rel = max(rel, rel_err(d[:s].cpu().numpy(), rd))
     tf_burst, tf_sust, hbm, peak_kind = peaks()
-    achieved = flops / (ms * 1e-3) / 1e12
     line = {
         "metric": "batched uneven kNN: aggregate queries/s, 256 problems (one graph) vs one "
                   "call per problem",
-        "value": total_q / (ms / 1000), "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16", "data": "synthetic: cfg4 recipe (seed 5)",
-        "workload_kind": "secondary",
+        "value": total_q / (ms / 1000), "unit": "queries/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": ms, "dtype": "bf16", "data": "synthetic: cfg4 recipe (seed 5)",
         "config": {"workload": f"knn_batch_{len(problems)}_uneven_seed5",
-                   "problems": len(problems),
-                   "queries": total_q, "flops": flops,
+                   "problems": len(problems), "queries": total_q, "flops": flops,
                    "l2": "operands 1.9 GB bf16, larger than L2"},
         "one_call_per_problem": {"value": total_q / one_s, "unit": "queries/s",
                                  "ms_per_step": 1000 * one_s,
                                  "batch_speedup": one_s / (ms / 1000)},
-        "roofline": {"kernel": "whole batched run (prep, screens, certify, exact)",
-                     "bound": "tensor", "achieved": achieved, "peak": tf_burst,
-                     "unit": "TFLOP/s", "frac": achieved / tf_burst,
-                     "peak_source": f"{peak_kind} burst bf16", "traffic": None},
+        "roofline": tensor_roofline("whole batched run (prep, screens, certify, exact)", flops,
+                                    ms * 1e-3, tf_burst, peak_kind),
         "batch_stats": stats, "fit_s": fit_s, "plan_s": plan_s,
         "e2e": {"value": total_q / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "cpu_baseline": {"value": total_q / est_cpu_s, "unit": "queries/s", "cores": threads,
-                         "kind": "reference" if ref else "port",
-                         "sample": f"first {per} queries of every problem, time scaled by "
-                                   "each problem's query count"},
-        "parity_vs_cpu_reference": {"queries": sample_q, "indices_bit_exact": exact,
-                                    "max_rel_dist_err": rel},
+                         "kind": kind,
+                         "sample": f"first {per} queries of every problem through the "
+                                   "installed reference's NearestNeighbors(brute).kneighbors, "
+                                   "time scaled by each problem's query count"},
+        "parity": {"queries": sample_q, "indices_bit_exact_vs_reference": exact,
+                   "max_rel_dist_err_vs_reference": rel},
         "clocks": clk.summary(),
     }
     batch.close()
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
-def run_chamfer(args):
-    """Differentiable kNN losses: 64 symmetric k=1 Chamfer terms on 8192 x 3
-    clouds plus a self k=8 mean-distance term on 4096 x 64, forward + backward."""
+def sec_chamfer(args):
+    """Config 5: 64 symmetric k=1 Chamfer terms on 8192 x 3 clouds plus a self
+    k=8 mean-distance term on 4096 x 64, forward + hand-written backward."""
     import torch
 
     from datasets import cfg5
-    from mlxlearn_b200.autograd import chamfer_loss_batch, knn_distances
-
-    import oracle
+    from mlxlearn_b200.autograd import chamfer_loss_batch, knn_distances, knn_segments
 
     torch.cuda.set_device(0)
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     clouds, S = cfg5()
-    # the 64 pairs as two [64, 8192, 3] tensors
+    steps, warmup = _steps(args)
     A = torch.from_numpy(np.stack([a for a, _ in clouds])).cuda().requires_grad_()
     B = torch.from_numpy(np.stack([b for _, b in clouds])).cuda().requires_grad_()
     Sd = torch.from_numpy(S).cuda().requires_grad_()
@@ -637,120 +841,76 @@ def run_chamfer(args):
         loss.backward()
         return loss
 
-    for _ in range(args.warmup):
-        step()
+    step_ms = [1000 * s for s in wall_times(step, steps, warmup)]
+    loss = step()
     torch.cuda.synchronize()
-    step_ms = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        loss = step()
-        torch.cuda.synchronize()
-        step_ms.append(1000 * (time.perf_counter() - t0))
-    s = sum(step_ms) / len(step_ms) / 1000
-    # CPU baseline: the reference's exact scan for the forward of two pairs
-    # (both directions) and torch float64 autograd on the CPU for their backward
-    ref = oracle.ref_native()
-    t0 = time.perf_counter()
-    cpu_pairs = 0
+    s = statistics.median(step_ms) / 1000
+    # FP32 CUDA-core roofline of the forward scan: 3 d + 1 FLOP per pair (d = 3)
+    cham_pairs = sum(2 * a.shape[0] * b.shape[0] for a, b in clouds)
+    achieved = (cham_pairs * 10 + S.shape[0] ** 2 * 2 * S.shape[1]) / s / 1e12
+    nb = reference_neighbors()
+    cpu_pairs, cpu_s, exact, err = 0, 0.0, True, 0.0
     for a, b in clouds[:2]:
         for P, Qr in ((a, b), (b, a)):
-            dist = np.empty((len(P), 1)); idx = np.empty((len(P), 1), np.int64)
-            _ref_knn_threads(ref, Qr, P, 1, dist, idx, threads)
+            t0 = time.perf_counter()
+            if nb is not None:
+                rdist, ridx = nb.NearestNeighbors(n_neighbors=1, algorithm="brute").fit(
+                    P).kneighbors(Qr)
+                kind = "reference"
+            else:
+                rdist, ridx, kind = native_kneighbors(P, Qr, 1, threads)
             Pt = torch.from_numpy(P).double().requires_grad_()
             Qt = torch.from_numpy(Qr).double().requires_grad_()
-            ((Pt - Qt[torch.from_numpy(idx[:, 0])]) ** 2).sum().backward()
+            ((Qt - Pt[torch.from_numpy(ridx[:, 0])]) ** 2).sum().backward()
+            cpu_s += time.perf_counter() - t0
             cpu_pairs += len(P) * len(Qr)
-    cpu_s = time.perf_counter() - t0
-    # parity of the forward: the two sampled pairs (both directions) through the
-    # segment search against the reference's exact scan
-    from mlxlearn_b200.autograd import knn_segments
-
-    exact, err = True, 0.0
-    for a, b in clouds[:2]:
-        for P, Qr in ((a, b), (b, a)):
             gd, gi = knn_segments(torch.from_numpy(Qr).cuda(), torch.from_numpy(P).cuda(),
                                   [len(Qr)], [len(P)], 1)
-            rdist = np.empty((len(Qr), 1)); ridx = np.empty((len(Qr), 1), np.int64)
-            _ref_knn_threads(ref, P, Qr, 1, rdist, ridx, threads)
             exact &= bool(np.array_equal(gi.cpu().numpy(), ridx))
-            gdv = gd.double().cpu().numpy()
-            err = max(err, float(np.max(np.abs(gdv - rdist) / np.maximum(rdist, 1e-300))))
-    line = {
+            err = max(err, rel_err(gd.double().cpu().numpy(), rdist))
+    return {
         "metric": "differentiable kNN: (query, reference) pairs/s, forward + backward "
                   "(64 Chamfer k=1 pairs of 8192x3 + self k=8 on 4096x64)",
-        "value": pairs / s, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000 * s, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: cfg5 recipe (seed 6)", "workload_kind": "secondary",
+        "value": pairs / s, "unit": "pairs/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": 1000 * s, "dtype": "f32",
+        "data": "synthetic: cfg5 recipe (seed 6)",
         "config": {"workload": "knn_chamfer_64x8192x3_self4096x64", "pairs_per_step": pairs,
                    "api": "mlxlearn_b200.autograd (public), wall clock with device sync"},
+        "roofline": {"kernel": "whole step (segment scans, backward)", "bound": "fp32 cores",
+                     "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                     "frac": achieved / FP32_NOMINAL_TFLOPS,
+                     "peak_source": "nominal fp32 CUDA-core rate at 1965 MHz (no measured "
+                                    "figure)", "traffic": None},
+        "e2e": {"value": pairs / s, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8,
+                "note": "inputs stay on the device (a training loop's tensors); the loss "
+                        "value is read back every step"},
         "loss": float(loss.item()), "step_ms": step_ms,
         "cpu_baseline": {"value": cpu_pairs / cpu_s, "unit": "pairs/s", "cores": threads,
-                         "kind": "reference" if ref else "port",
-                         "sample": "2 Chamfer pairs both ways: reference exact scan forward, "
-                                   "torch float64 CPU autograd backward"},
-        "parity_vs_cpu_reference": {"pairs": 4, "indices_bit_exact": exact,
-                                    "max_rel_dist_err": err,
-                                    "note": "forward k=1 of 2 Chamfer pairs, both directions; "
-                                            "distances are float32 outputs of the autograd path"},
+                         "kind": kind,
+                         "sample": "2 Chamfer pairs both ways: the installed reference's "
+                                   "kneighbors forward, torch float64 CPU autograd backward"},
+        "parity": {"pairs": 4, "indices_bit_exact_vs_reference": exact,
+                   "max_rel_dist_err_vs_reference": err,
+                   "note": "forward k=1 of 2 Chamfer pairs, both directions; distances are "
+                           "float32 outputs of the autograd path"},
     }
-    print(json.dumps(line), flush=True)
-    return 0
 
 
-def _ref_knn_threads(ref, X, Q, k, dist, idx, threads):
-    """The reference's exact native kNN scan over query blocks in threads."""
-    from concurrent.futures import ThreadPoolExecutor
-
-    import oracle
-
-    if ref is None:
-        d, i = oracle.knn(X, Q, k, nthreads=threads)
-        dist[:] = d
-        idx[:] = i
-        return
-    Q = np.ascontiguousarray(Q)
-    chunks = np.array_split(np.arange(len(Q)), threads)
-
-    def run(rows):
-        if len(rows):
-            a, b = rows[0], rows[-1] + 1
-            ref.neighbors.query(X, Q[a:b], k, False, 0, dist[a:b], idx[a:b])
-
-    with ThreadPoolExecutor(threads) as ex:
-        list(ex.map(run, chunks))
+SECONDARY = {"small": sec_small, "pixels": sec_pixels, "radius": sec_radius,
+             "batch": sec_batch, "chamfer": sec_chamfer}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="knn",
-                    choices=["knn", "pixels", "radius", "small", "batch", "chamfer"])
-    ap.add_argument("--profile", action="store_true",
-                    help="profiling driver: only the bf16 device-resident steps of the "
-                         "headline workload (no fp32 leg, e2e or CPU baseline)")
-    ap.add_argument("--mode", default="bf16", choices=["bf16", "fp32", "exact", "auto"],
-                    help="screen form for --profile")
-    ap.add_argument("--k", type=int, default=K, help="neighbours for --profile")
-    ap.add_argument("--problems", type=int, default=256,
-                    help="problem count of the batch workload (the benchmark uses 256)")
-    ap.add_argument("--queries", type=int, default=N_QUERY,
-                    help="query count for --profile (the headline uses 100,000)")
-    args = ap.parse_args()
-    if args.impl == "reference":
-        return run_reference_arm(args)
-    if args.workload == "batch":
-        return run_batch(args)
-    if args.workload == "chamfer":
-        return run_chamfer(args)
-    if args.profile:
-        return run_profile(args)
-    if args.workload != "knn":
-        return run_secondary(args)
-    return run_ours(args)
+def run_secondaries(args):
+    out = {}
+    for name, fn in SECONDARY.items():
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(args)
+        except Exception as e:  # one configuration's failure must not hide the others
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def run_profile(args):
@@ -773,6 +933,41 @@ def run_profile(args):
     print(json.dumps({"profile": True, "queries": args.queries, "mode": args.mode, "k": args.k,
                       "stats": index.last_stats}))
     return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="all", choices=["all", "knn", *SECONDARY])
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling driver: only the device steps of the headline workload "
+                         "(or of --workload batch)")
+    ap.add_argument("--mode", default="bf16", choices=["bf16", "fp32", "exact", "auto"],
+                    help="screen form for --profile")
+    ap.add_argument("--k", type=int, default=K, help="neighbours for --profile")
+    ap.add_argument("--problems", type=int, default=256,
+                    help="problem count of the batch workload (the benchmark uses 256)")
+    ap.add_argument("--queries", type=int, default=N_QUERY,
+                    help="query count for --profile (the headline uses 100,000)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.workload in SECONDARY:
+        import torch
+
+        torch.cuda.set_device(0)
+        line = SECONDARY[args.workload](args)
+        line.setdefault("n_gpus", 1)
+        line.update({"higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                     "workload_kind": "secondary"})
+        print(json.dumps(line), flush=True)
+        return 0
+    if args.profile:
+        return run_profile(args)
+    return run_ours(args)
 
 
 if __name__ == "__main__":

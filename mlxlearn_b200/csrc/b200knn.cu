@@ -188,14 +188,77 @@ static int finish_index(Index& ix, cudaStream_t st) {
   return B2K_OK;
 }
 
+// Pivots for query grouping and row grouping (the caller holds ix.mu).
+static int make_pivots(Index& ix) {
+  if (ix.pivots) return B2K_OK;
+  ix.n_pivots = pivot_count(ix.n);
+  B2K_CUDA(cudaMalloc(&ix.pivots, (size_t)ix.n_pivots * ix.d * sizeof(float)));
+  B2K_CUDA(cudaMalloc(&ix.pivot_norms, (size_t)ix.n_pivots * sizeof(float)));
+  launch_pivots(&ix, ix.stream);
+  B2K_CUDA(cudaGetLastError());
+  B2K_CUDA(cudaStreamSynchronize(ix.stream));
+  return B2K_OK;
+}
+
+// Indexes of at least this many rows get grouped operand rows (unless
+// B2K_GROUP_ROWS=0; tests run both ways).
+constexpr int64_t kGroupMinRows = 8192;
+static bool group_rows_enabled(const Index& ix) {
+  const char* e = getenv("B2K_GROUP_ROWS");
+  return ix.n >= kGroupMinRows && !(e && e[0] == '0');
+}
+
+// Operand row order grouped by nearest pivot (the caller holds ix.mu): a
+// counting sort on the host, stable, so rows keep their training order
+// within a group and the layout is the same on every build.
+static int make_row_groups(Index& ix) {
+  cudaStream_t st = ix.stream;
+  int rc = make_pivots(ix);
+  if (rc) return rc;
+  const int P = ix.n_pivots;
+  int *key = nullptr, *hist = nullptr;
+  B2K_CUDA(cudaMalloc(&key, (size_t)ix.n * sizeof(int)));
+  if (cudaMalloc(&hist, (size_t)P * sizeof(int)) != cudaSuccess) {
+    cudaFree(key);
+    return fail(B2K_ENOMEM, "device allocation failed");
+  }
+  launch_assign_rows(&ix, ix.X, ix.n, key, hist, st);
+  std::vector<int> hkey((size_t)ix.n);
+  cudaError_t e = cudaMemcpyAsync(hkey.data(), key, (size_t)ix.n * sizeof(int),
+                                  cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(key);
+  cudaFree(hist);
+  if (e != cudaSuccess) return fail(B2K_ECUDA, "row grouping: %s", cudaGetErrorString(e));
+  std::vector<int64_t> start((size_t)P + 1, 0);
+  for (int64_t r = 0; r < ix.n; ++r) ++start[(size_t)hkey[(size_t)r] + 1];
+  for (int p = 0; p < P; ++p) start[(size_t)p + 1] += start[(size_t)p];
+  std::vector<int> perm((size_t)ix.n), inv((size_t)ix.n);
+  for (int64_t r = 0; r < ix.n; ++r) {
+    const int64_t pos = start[(size_t)hkey[(size_t)r]]++;
+    perm[(size_t)pos] = (int)r;
+    inv[(size_t)r] = (int)pos;
+  }
+  B2K_CUDA(cudaMalloc(&ix.xperm, (size_t)ix.n * sizeof(int)));
+  B2K_CUDA(cudaMalloc(&ix.xinv, (size_t)ix.n * sizeof(int)));
+  B2K_CUDA(cudaMemcpyAsync(ix.xperm, perm.data(), (size_t)ix.n * sizeof(int),
+                           cudaMemcpyHostToDevice, st));
+  B2K_CUDA(cudaMemcpyAsync(ix.xinv, inv.data(), (size_t)ix.n * sizeof(int),
+                           cudaMemcpyHostToDevice, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  return B2K_OK;
+}
+
 static int ensure_bf16(Index& ix) {
   std::lock_guard<std::mutex> lock(ix.mu);
   if (ix.bf16_ready) return B2K_OK;
   cudaStream_t st = ix.stream;
   ix.dp = (int32_t)round_up(ix.d, kTcBK);
   ix.n_pad_tc = round_up(ix.n, kTcBN);
+  int rc;
+  if (group_rows_enabled(ix) && (rc = make_row_groups(ix))) return rc;
   B2K_CUDA(cudaMalloc(&ix.Xh, (size_t)ix.n_pad_tc * ix.dp * sizeof(uint16_t)));
-  launch_prep_index_bf16(&ix, ix.Xh, st);
+  launch_prep_index_bf16(&ix, ix.Xh, st, ix.xperm);
   B2K_CUDA(cudaGetLastError());
   float stats[8];
   B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
@@ -207,7 +270,7 @@ static int ensure_bf16(Index& ix) {
   // norm columns of the reference rows and the matching query-side ones
   B2K_CUDA(cudaMalloc(&ix.Xaug, (size_t)ix.n_pad_tc * kTcAug * sizeof(uint16_t)));
   B2K_CUDA(cudaMalloc(&ix.aug_ones, (size_t)kTcBM * kTcAug * sizeof(uint16_t)));
-  launch_prep_aug(&ix, ix.Xaug, ix.aug_ones, st);
+  launch_prep_aug(&ix, ix.Xaug, ix.aug_ones, st, ix.xperm);
   B2K_CUDA(cudaGetLastError());
   B2K_CUDA(cudaStreamSynchronize(st));
   if (!tensor_map_2d_bf16(&ix.tmap_baug, ix.Xaug, kTcAug, (uint64_t)ix.n_pad_tc, kTcAug, kTcBN,
@@ -220,14 +283,7 @@ static int ensure_bf16(Index& ix) {
 
 static int ensure_pivots(Index& ix) {
   std::lock_guard<std::mutex> lock(ix.mu);
-  if (ix.pivots) return B2K_OK;
-  ix.n_pivots = pivot_count(ix.n);
-  B2K_CUDA(cudaMalloc(&ix.pivots, (size_t)ix.n_pivots * ix.d * sizeof(float)));
-  B2K_CUDA(cudaMalloc(&ix.pivot_norms, (size_t)ix.n_pivots * sizeof(float)));
-  launch_pivots(&ix, ix.stream);
-  B2K_CUDA(cudaGetLastError());
-  B2K_CUDA(cudaStreamSynchronize(ix.stream));
-  return B2K_OK;
+  return make_pivots(ix);
 }
 
 // Query grouping is on unless B2K_REORDER=0 (tests run both ways).
@@ -434,6 +490,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.counters = counters;
     ca.perm = perm;
     ca.squared = squared;
+    ca.cols = tc ? ix.xperm : nullptr;  // lists of the grouped bf16 operand
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
     // Rows the screen could not certify (a list past capacity, too many
@@ -682,6 +739,8 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.pivot_norms);
   cudaFree(ix.Xaug);
   cudaFree(ix.aug_ones);
+  cudaFree(ix.xperm);
+  cudaFree(ix.xinv);
   if (ix.stream) cudaStreamDestroy(ix.stream);
   delete h;
   return B2K_OK;
@@ -852,6 +911,10 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   if ((rc = dalloc(&sa.rcols, (size_t)ncand, st))) return rc;
   fr.keep(sa.rcols);
   if ((rc = screen(kSinkRadiusFill))) return rc;
+  // grouped operand rows: candidates to training rows (rows are re-sorted
+  // by index after the compaction)
+  const bool grouped = tc && ix.xperm;
+  if (grouped) launch_translate_cols(sa.rcols, ncand, ix.xperm, st);
 
   RadiusPlanArgs ra{};
   ra.X = ix.X;
@@ -893,12 +956,16 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   }
   launch_compact(ra, indptr, indices, dist, st);
   B2K_CUDA(cudaGetLastError());
-  if (sort_results && nnz > 1) {
+  if ((sort_results || grouped) && nnz > 1) {
+    // (distance, index) order when asked for, else ascending training index
+    // (grouped operand rows list candidates out of index order)
+    const bool by_dist = sort_results;
     int* big = nullptr;
     if ((rc = dalloc(&big, (size_t)m + 1, st))) return rc;
     fr.keep(big);
     B2K_CUDA(cudaMemsetAsync(big + m, 0, sizeof(int), st));
-    launch_sort_rows(indptr, m, indices, dist, big, big + m, std::min<int64_t>(m, 4 * sms), st);
+    launch_sort_rows(indptr, m, indices, dist, big, big + m, std::min<int64_t>(m, 4 * sms), st,
+                     by_dist);
     int nbig = 0;
     B2K_CUDA(cudaMemcpyAsync(&nbig, big + m, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2K_CUDA(cudaStreamSynchronize(st));
@@ -913,7 +980,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
       fr.keep(td);
       if ((rc = dalloc(&ti, (size_t)grid * P, st))) return rc;
       fr.keep(ti);
-      launch_sort_big_rows(indptr, big, nbig, indices, dist, td, ti, P, grid, st);
+      launch_sort_big_rows(indptr, big, nbig, indices, dist, td, ti, P, grid, st, by_dist);
       B2K_CUDA(cudaGetLastError());
     }
   }

@@ -358,6 +358,8 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
       }
       const unsigned bal = __ballot_sync(0xffffffffu, pass);
       const int pos = C + __popc(bal & ((1u << lane) - 1));
+      // grouped operand rows: the list holds operand rows, the answer training rows
+      if (pass && a.cols) col = __ldg(a.cols + col);
       if (pass && pos < kCertifyCap) ci[pos] = col;
       C += __popc(bal);
       if (C > kCertifyCap) {

@@ -60,6 +60,11 @@ struct Index {
   uint16_t* aug_ones = nullptr;  // [128, 16] bf16 [1, 1, 1, 0...] (query side)
   CUtensorMap tmap_baug;         // over Xaug, box 16 x 256, 32-byte swizzle
   CUtensorMap tmap_aaug;         // over aug_ones, box 16 x 128, 32-byte swizzle
+  // Row grouping of the bf16 operand (reorder.cu): operand row i holds
+  // training row xperm[i]; rows sharing a nearest pivot are consecutive, so a
+  // query tile's candidates fall in few reference tiles.  Null: identity.
+  int* xperm = nullptr;          // [n] operand row -> training row
+  int* xinv = nullptr;           // [n] training row -> operand row
   // pivots for query ordering (reorder.cu)
   int n_pivots = 0;
   float* pivots = nullptr;       // [n_pivots, d] centred rows
@@ -72,12 +77,15 @@ struct Index {
 void launch_prep_index(Index* ix, cudaStream_t st);
 // flag |= 1 when some value is NaN or infinite
 void launch_nonfinite_check(const float* v, int64_t count, int* flag, cudaStream_t st);
-// bf16 operand rows [n_pad, dp] (n_pad = n rounded up to 256) into Xh; the
-// operand statistics go to the index's stats_dev [3], [4].
-void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st);
-// norm columns [n_pad, 16] into Xaug; when `ones` is set, also the query-side
-// columns [128, 16].
-void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st);
+// bf16 operand rows [n_pad, dp] (n_pad = n rounded up to 256) into Xh, row i
+// from training row rows[i] (rows null: row i); the operand statistics go to
+// the index's stats_dev [3], [4].
+void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st,
+                            const int* rows = nullptr);
+// norm columns [n_pad, 16] into Xaug (row i from training row rows[i]); when
+// `ones` is set, also the query-side columns [128, 16].
+void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st,
+                     const int* rows = nullptr);
 // Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
 struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
@@ -127,6 +135,10 @@ void launch_pivots(Index* ix, cudaStream_t st);
 // perm[i] = original row of sorted position i; Qp = Q[perm]
 void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,
                         int* perm, float* Qp, cudaStream_t st);
+// key[r] = nearest pivot of row r of X [n, d] (the index's centre applied);
+// hist[p] = rows per pivot
+void launch_assign_rows(const Index* ix, const float* X, int64_t n, int* key, int* hist,
+                        cudaStream_t st);
 
 // second pass over uncertified rows: Qout[i] = Qs[rows[i]], pout[i] = perm[rows[i]]
 void launch_gather_fallback(const float* Qs, int d, const int* rows, const int* perm, int count,
@@ -148,6 +160,7 @@ struct CertifyArgs {
   const int* perm;     // row -> output row (or null)
   int64_t row_base;    // added to the row in fallback_list entries (batched runs)
   int squared;         // write squared distances (else their square roots)
+  const int* cols;     // list column -> training row (grouped operand rows), or null
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
 // problem p owns global rows [row_start[p], row_start[p + 1]) of the batch
@@ -179,6 +192,8 @@ void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, c
                         cudaStream_t st);
 
 // ------------------------------------------------------------------ radius
+// cols[i] = xperm[cols[i]]: candidate columns of a grouped operand to training rows
+void launch_translate_cols(int* cols, int64_t count, const int* xperm, cudaStream_t st);
 struct RadiusPlanArgs {
   const float* X;
   const float* Q;
@@ -201,11 +216,14 @@ void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, cudaStr
 void launch_classify(const RadiusPlanArgs& r, cudaStream_t st);
 void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* indices,
                     double* dist, cudaStream_t st);
+// Per-row sort by (distance, index), or by index alone when !by_dist (dist,
+// if not null, then moves with its index).
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
-                      int* big_rows, int* big_count, int grid, cudaStream_t st);
+                      int* big_rows, int* big_count, int grid, cudaStream_t st,
+                      bool by_dist = true);
 void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
                           double* dist, double* tmp_d, int64_t* tmp_i, int64_t tmp_stride,
-                          int grid, cudaStream_t st);
+                          int grid, cudaStream_t st, bool by_dist = true);
 int radius_sort_cap();
 
 // ------------------------------------------------------------------- votes

@@ -106,6 +106,7 @@ __global__ void prep_index_kernel(const float* __restrict__ X, int64_t n, int d,
 
 __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, int d,
                                        int64_t n_pad, int dp, const float* __restrict__ center,
+                                       const int* __restrict__ rows,
                                        __nv_bfloat16* __restrict__ Xh,
                                        float* __restrict__ stats) {
   int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
@@ -117,7 +118,7 @@ __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, i
     for (int i = lane; i < dp; i += 32) xh[i] = __float2bfloat16_rn(0.0f);
     return;
   }
-  const float* x = X + row * d;
+  const float* x = X + (rows ? (int64_t)rows[row] : row) * d;
   double hn = 0.0, en = 0.0, yy = 0.0;
   for (int i = lane; i < dp; i += 32) {
     const float v = i < d ? x[i] : 0.0f;
@@ -144,6 +145,7 @@ __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, i
 // parts hi + mid + lo (residual below 2^-26 of the value), NaN on padding
 // rows; the query side is [1, 1, 1, 0, ...].
 __global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int64_t n_pad,
+                                const int* __restrict__ rows,
                                 __nv_bfloat16* __restrict__ Xaug,
                                 __nv_bfloat16* __restrict__ ones) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,7 +163,7 @@ __global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int6
     a[2] = __float2bfloat16_rn(0.0f);
     return;
   }
-  const double v = nx64[row];
+  const double v = nx64[rows ? (int64_t)rows[row] : row];
   const __nv_bfloat16 hi = __float2bfloat16_rn((float)v);
   const double r1 = v - (double)__bfloat162float(hi);
   const __nv_bfloat16 mid = __float2bfloat16_rn((float)r1);
@@ -287,21 +289,22 @@ void launch_prep_index(Index* ix, cudaStream_t st) {
       ix->X, ix->n, ix->d, ix->center, ix->nx32, ix->nx64, ix->stats_dev);
 }
 
-void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st) {
+void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st, const int* rows) {
   const int warps = 8;
   const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
   const int dp = (ix->d + kTcBK - 1) / kTcBK * kTcBK;
   const int64_t blocks = (n_pad + warps - 1) / warps;
   prep_index_bf16_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(
-      ix->X, ix->n, ix->d, n_pad, dp, ix->center, reinterpret_cast<__nv_bfloat16*>(Xh),
+      ix->X, ix->n, ix->d, n_pad, dp, ix->center, rows, reinterpret_cast<__nv_bfloat16*>(Xh),
       ix->stats_dev);
 }
 
-void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st) {
+void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st,
+                     const int* rows) {
   const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
-  const int64_t rows = n_pad > kTcBM ? n_pad : kTcBM;
-  prep_aug_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
-      ix->nx64, ix->n, n_pad, reinterpret_cast<__nv_bfloat16*>(Xaug),
+  const int64_t threads = n_pad > kTcBM ? n_pad : kTcBM;
+  prep_aug_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      ix->nx64, ix->n, n_pad, rows, reinterpret_cast<__nv_bfloat16*>(Xaug),
       reinterpret_cast<__nv_bfloat16*>(ones));
 }
 

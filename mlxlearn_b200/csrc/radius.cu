@@ -14,6 +14,9 @@
 //                  distances sqrt(min(s, R2)), rows in ascending index order.
 //   5. sort      : optional per-row (distance, index) order
 //                  (src/mlxlearn/_kernels/radius_result.py:160-187).
+// With grouped operand rows (reorder.cu) the fill pass yields operand rows:
+// they are translated to training rows before step 3, and rows are sorted by
+// training index after step 4 when no distance order is asked for.
 // Replaces the reference's Metal screen + host finisher
 // (src/mlxlearn/_kernels/radius_metal_v1.py:257-611, src/mlxlearn_device/_radius.py:54-330).
 #include <cfloat>
@@ -204,10 +207,25 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
   }
 }
 
-// Per-row (distance, index) sort, one CTA per row, rows of at most kRadiusSortCap.
+__global__ void translate_cols_kernel(int* __restrict__ cols, int64_t count,
+                                      const int* __restrict__ xperm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) cols[i] = __ldg(xperm + cols[i]);
+}
+
+// Sort order of the per-row sorts: (distance, index), or index alone.
+template <bool BY_DIST>
+__device__ __forceinline__ bool sort_after(double x, int64_t xi, double y, int64_t yi) {
+  if constexpr (BY_DIST) return (x > y) || (x == y && xi > yi);
+  return xi > yi;
+}
+
+// Per-row sort, one CTA per row, rows of at most kRadiusSortCap; `dist` may
+// be null for an index sort.
 constexpr int kRadiusSortCap = 4096;
 constexpr int kSortThreads = 512;
 
+template <bool BY_DIST>
 __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
                                  int64_t* __restrict__ indices, double* __restrict__ dist,
                                  int* __restrict__ big_rows, int* __restrict__ big_count) {
@@ -224,7 +242,7 @@ __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
     int P = 2;
     while (P < len) P <<= 1;
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-      sd[i] = i < len ? dist[a0 + i] : DBL_MAX;
+      sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
       si[i] = i < len ? indices[a0 + i] : INT64_MAX;
     }
     __syncthreads();
@@ -235,7 +253,7 @@ __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
           const bool up = (i & size) == 0;
           const double x = sd[i], y = sd[j];
           const int64_t xi = si[i], yi = si[j];
-          const bool gt = (x > y) || (x == y && xi > yi);
+          const bool gt = sort_after<BY_DIST>(x, xi, y, yi);
           if (gt == up) {
             sd[i] = y;
             sd[j] = x;
@@ -246,7 +264,7 @@ __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
         __syncthreads();
       }
     for (int i = threadIdx.x; i < len; i += blockDim.x) {
-      dist[a0 + i] = sd[i];
+      if (dist) dist[a0 + i] = sd[i];
       indices[a0 + i] = si[i];
     }
     __syncthreads();
@@ -255,6 +273,7 @@ __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
 
 // Rows longer than the shared-memory sort: bitonic sort in global scratch
 // (padded to a power of two), one CTA per row.
+template <bool BY_DIST>
 __global__ void sort_big_rows_kernel(const int64_t* __restrict__ indptr,
                                      const int* __restrict__ rows, int count,
                                      int64_t* __restrict__ indices, double* __restrict__ dist,
@@ -268,7 +287,7 @@ __global__ void sort_big_rows_kernel(const int64_t* __restrict__ indptr,
     double* sd = tmp_d + (size_t)blockIdx.x * tmp_stride;
     int64_t* si = tmp_i + (size_t)blockIdx.x * tmp_stride;
     for (int64_t i = threadIdx.x; i < P; i += blockDim.x) {
-      sd[i] = i < len ? dist[a0 + i] : DBL_MAX;
+      sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
       si[i] = i < len ? indices[a0 + i] : INT64_MAX;
     }
     __syncthreads();
@@ -279,7 +298,7 @@ __global__ void sort_big_rows_kernel(const int64_t* __restrict__ indptr,
           const bool up = (i & size) == 0;
           const double x = sd[i], y = sd[j];
           const int64_t xi = si[i], yi = si[j];
-          const bool gt = (x > y) || (x == y && xi > yi);
+          const bool gt = sort_after<BY_DIST>(x, xi, y, yi);
           if (gt == up) {
             sd[i] = y;
             sd[j] = x;
@@ -290,7 +309,7 @@ __global__ void sort_big_rows_kernel(const int64_t* __restrict__ indptr,
         __syncthreads();
       }
     for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
-      dist[a0 + i] = sd[i];
+      if (dist) dist[a0 + i] = sd[i];
       indices[a0 + i] = si[i];
     }
     __syncthreads();
@@ -395,21 +414,26 @@ void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* ind
                                                                                  indices, dist);
 }
 
+void launch_translate_cols(int* cols, int64_t count, const int* xperm, cudaStream_t st) {
+  if (count <= 0) return;
+  translate_cols_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(cols, count, xperm);
+}
+
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
-                      int* big_rows, int* big_count, int grid, cudaStream_t st) {
+                      int* big_rows, int* big_count, int grid, cudaStream_t st, bool by_dist) {
   if (m <= 0) return;
   const size_t smem = (size_t)kRadiusSortCap * (sizeof(double) + sizeof(int64_t));
-  cudaFuncSetAttribute(sort_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  sort_rows_kernel<<<grid, kSortThreads, smem, st>>>(indptr, m, indices, dist, big_rows,
-                                                     big_count);
+  auto kern = by_dist ? sort_rows_kernel<true> : sort_rows_kernel<false>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<grid, kSortThreads, smem, st>>>(indptr, m, indices, dist, big_rows, big_count);
 }
 
 void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
                           double* dist, double* tmp_d, int64_t* tmp_i, int64_t tmp_stride,
-                          int grid, cudaStream_t st) {
+                          int grid, cudaStream_t st, bool by_dist) {
   if (count <= 0) return;
-  sort_big_rows_kernel<<<grid, 1024, 0, st>>>(indptr, rows, count, indices, dist, tmp_d, tmp_i,
-                                              tmp_stride);
+  auto kern = by_dist ? sort_big_rows_kernel<true> : sort_big_rows_kernel<false>;
+  kern<<<grid, 1024, 0, st>>>(indptr, rows, count, indices, dist, tmp_d, tmp_i, tmp_stride);
 }
 
 int radius_sort_cap() { return kRadiusSortCap; }

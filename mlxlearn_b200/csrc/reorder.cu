@@ -1,4 +1,4 @@
-// Query ordering for the screens.
+// Query ordering (and index row grouping) for the screens.
 //
 // A screen tile holds 128 query rows and each epilogue warp 32 of them; the
 // warp leaves its fast path whenever ANY of its rows admits a column.  With
@@ -13,6 +13,10 @@
 // original query row) and the permuted query matrix.  Results are written
 // back to the original rows by the certify / exact kernels, so the answer
 // does not depend on the order.
+//
+// The same assignment groups the rows of the index's bf16 operand by pivot
+// (b200knn.cu): a tile of grouped queries then finds its candidates in a few
+// consecutive reference tiles, and the other tiles' chunks skip admission.
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -158,6 +162,13 @@ int pivot_count(int64_t n) {
 void launch_pivots(Index* ix, cudaStream_t st) {
   pivot_rows_kernel<<<ix->n_pivots, 32, 0, st>>>(ix->X, ix->n, ix->d, ix->n_pivots, ix->center,
                                                  ix->pivots, ix->pivot_norms);
+}
+
+void launch_assign_rows(const Index* ix, const float* X, int64_t n, int* key, int* hist,
+                        cudaStream_t st) {
+  cudaMemsetAsync(hist, 0, (size_t)ix->n_pivots * sizeof(int), st);
+  assign_kernel<<<(unsigned)((n + kAssignThreads - 1) / kAssignThreads), kAssignThreads, 0, st>>>(
+      X, n, ix->d, ix->center, ix->pivots, ix->pivot_norms, ix->n_pivots, key, hist);
 }
 
 void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,

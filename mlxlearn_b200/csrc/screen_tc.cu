@@ -463,15 +463,21 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       // warp-collective sinks run on every lane (inactive past the block's end)
       const bool live = Sink::kWarpWide || valid;
       Sink sink;
+      // the excluded column of a self-query: its training row, or that row's
+      // place among grouped reference rows
+      auto self_column = [&](int orig) -> int {
+        const long long r = pr.q_offset + orig;
+        return pr.self_col ? pr.self_col[r] : (int)r;
+      };
       if constexpr (Sink::kWarpWide) {
         const int orig = valid ? (pr.perm ? pr.perm[row] : row) : 0;
         sink.init_warp(pr.sink, row, x.slot * kHalves + half, valid ? pr.E[row] : 0.0f,
-                       (valid && pr.exclude_self) ? (int)(pr.q_offset + orig) : -1, valid,
+                       (valid && pr.exclude_self) ? self_column(orig) : -1, valid,
                        reinterpret_cast<unsigned*>(spill_all + (size_t)ew * 32 * kSpillStride));
       } else if (valid) {
         const int orig = pr.perm ? pr.perm[row] : row;
         sink.init(pr.sink, row, x.slot * kHalves + half, pr.E[row],
-                  pr.exclude_self ? (int)(pr.q_offset + orig) : -1);
+                  pr.exclude_self ? self_column(orig) : -1);
       }
       uint32_t pending_key = kNoKey;
       for (int j = x.j0; j < x.j1; ++j) {
@@ -616,6 +622,7 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   one.q_offset = q_offset;
   one.E = E;
   one.perm = perm;
+  one.self_col = ix->xinv;
   one.sink = sa;
   p.S = S;
   p.m_tiles = (int)(m_pad / kTcBM);

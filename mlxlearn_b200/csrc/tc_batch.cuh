@@ -27,6 +27,7 @@ struct TcProblem {
   long long q_offset;
   const float* E;       // [m_pad] screen error bound per query row
   const int* perm;      // tile row -> original query row (or null)
+  const int* self_col;  // training row -> its reference column (grouped operand), or null
   SinkArgs sink;
 };
 

@@ -1,0 +1,60 @@
+"""Parity at the headline scale: 1,000,000 x 128 mixture rows, k = 10.
+
+The benchmark answers 100,000 queries against the full index in one call,
+where the screen runs its production configuration (row grouping, query
+grouping, reference splits, shared k-th values, the certify band of this
+data).  1,024 of those queries are checked bit-exact against the oracle
+(indices, and distances to the canonical float64 value), both as answered
+inside the full 100,000-query batch and as a batch of their own, in the
+bf16 form and the plain fp32 form.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from datasets import cfg2a
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def headline():
+    import torch
+
+    from mlxlearn_b200.index import build_index
+
+    X, Q = cfg2a(1_000_000, 100_000, 128)
+    # 512 leading queries and 512 spread over the batch
+    pick = np.concatenate([np.arange(512), np.linspace(512, 99_999, 512).astype(np.int64)])
+    od, oi = oracle.knn(X, Q[pick], 10)
+    index = build_index(X)
+    Qd = torch.from_numpy(Q).cuda()
+    return index, Q, Qd, pick, od, oi
+
+
+@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+def test_full_batch_matches_oracle(headline, mode):
+    index, Q, Qd, pick, od, oi = headline
+    dist, idx = index.query_device(Qd, 10, mode=mode, stats=True)
+    st = index.last_stats
+    di = idx.cpu().numpy()[pick]
+    dd = dist.cpu().numpy()[pick]
+    np.testing.assert_array_equal(di, oi)
+    np.testing.assert_array_equal(dd, od)
+    assert st["fallback_rows"] == 0, st
+    # every answer is a valid, strictly ordered list of distinct rows
+    all_idx = idx.cpu().numpy()
+    all_d = dist.cpu().numpy()
+    assert all_idx.min() >= 0 and all_idx.max() < 1_000_000
+    assert np.all(np.diff(all_d, axis=1) >= 0)
+    s = np.sort(all_idx, axis=1)
+    assert np.all(s[:, 1:] != s[:, :-1])
+
+
+def test_sample_alone_matches_oracle(headline):
+    index, Q, Qd, pick, od, oi = headline
+    dist, idx = index.query(Q[pick], 10, mode="bf16")
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(dist, od)

@@ -326,3 +326,33 @@ def test_k_across_the_screen_limit(k, rng):
     dist, idx = small.query(Q[:7], k)
     np.testing.assert_array_equal(idx, oi)
     np.testing.assert_array_equal(dist, od)
+
+
+@pytest.mark.parametrize("group", ["0", "1"])
+def test_row_grouping_both_ways(group, monkeypatch):
+    """The bf16 operand's rows are grouped by nearest pivot (the screen's
+    lists hold operand rows, certify maps them back to training rows, a
+    self-query excludes its row's operand column); both layouts give the
+    oracle's answer, ties between duplicated rows included."""
+    import torch
+
+    monkeypatch.setenv("B2K_GROUP_ROWS", group)
+    C = np.random.default_rng(15).uniform(-1, 1, (128, 48))
+    X, _ = mixture(np.random.default_rng(16), 30000, C, 0.1)
+    X[20000:20060] = X[:60]  # exact duplicates: ties resolved by training index
+    Q, _ = mixture(np.random.default_rng(17), 3000, C, 0.1)
+    Q[:20] = X[:20]
+    index = make_index(X)
+    for k in (1, 10, 40):
+        od, oi = oracle.knn(X, Q, k)
+        dist, idx = index.query(Q, k, mode="bf16", stats=True)
+        np.testing.assert_array_equal(idx, oi)
+        np.testing.assert_array_equal(dist, od)
+        assert index.last_stats["fallback_rows"] == 0
+    Xd = torch.from_numpy(X).cuda()
+    for lo in (0, 19990):
+        od, oi = oracle.knn(X, X[lo:lo + 3000], 9, exclude_self=True, q_offset=lo)
+        dd, di = index.query_device(Xd[lo:lo + 3000], 9, exclude_self=True, q_offset=lo,
+                                    mode="bf16")
+        np.testing.assert_array_equal(di.cpu().numpy(), oi)
+        np.testing.assert_array_equal(dd.cpu().numpy(), od)

@@ -112,3 +112,32 @@ def test_radius_big_rows_sort(rng):
     np.testing.assert_array_equal(ip, op)
     np.testing.assert_array_equal(ix, oix)
     np.testing.assert_array_equal(dd, od)
+
+
+@pytest.mark.parametrize("group", ["0", "1"])
+def test_radius_row_grouping_both_ways(group, monkeypatch):
+    """With grouped operand rows the fill pass lists operand rows; they are
+    mapped to training rows and each row re-sorted by index (or by distance
+    when asked), rows past the shared-memory sort included."""
+    monkeypatch.setenv("B2K_GROUP_ROWS", group)
+    C = np.random.default_rng(18).normal(0, 2.0, (12, 24))
+    X, _ = mixture(np.random.default_rng(19), 24000, C, 1.0)
+    Q, _ = mixture(np.random.default_rng(20), 400, C, 1.0)
+    index = make_index(X)
+    for r, sort in ((5.0, False), (5.0, True), (9.0, False), (9.0, True)):
+        op, oix, od = oracle.radius(X, Q, r, sort_results=sort)
+        ip, ix, dd = csr(index.query_radius_csr(Q, r, sort_results=sort))
+        np.testing.assert_array_equal(ip, op)
+        np.testing.assert_array_equal(ix, oix)
+        np.testing.assert_array_equal(dd, od)
+    assert np.diff(op).max() > 4096  # the r = 9 rows exceed the shared-memory sort
+    ip, ix, dd = csr(index.query_radius_csr(Q, 5.0, need_distance=False))
+    op, oix, _ = oracle.radius(X, Q, 5.0)
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    assert dd is None
+    op, oix, od = oracle.radius(X, X, 4.0, exclude_self=True)
+    ip, ix, dd = csr(index.query_radius_csr(X, 4.0, exclude_self=True))
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    np.testing.assert_array_equal(dd, od)
