@@ -61,6 +61,15 @@ static int fault_mode() {
   return 0;
 }
 
+uint32_t device_spin_limit() {
+  const char* e = getenv("B2K_SPIN_LIMIT");
+  if (e && *e) {
+    const unsigned long v = strtoul(e, nullptr, 10);
+    if (v > 0 && v <= kSpinLimit) return (uint32_t)v;
+  }
+  return kSpinLimit;
+}
+
 int num_sms(int device) {
   static int cached[64] = {0};
   if (device < 0 || device >= 64) return 148;
@@ -491,6 +500,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.perm = perm;
     ca.squared = squared;
     ca.cols = tc ? ix.xperm : nullptr;  // lists of the grouped bf16 operand
+    ca.status = status;
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
     // Rows the screen could not certify (a list past capacity, too many
@@ -914,7 +924,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   // grouped operand rows: candidates to training rows (rows are re-sorted
   // by index after the compaction)
   const bool grouped = tc && ix.xperm;
-  if (grouped) launch_translate_cols(sa.rcols, ncand, ix.xperm, st);
+  if (grouped) launch_translate_cols(sa.rcols, ncand, ix.xperm, status, st);
 
   RadiusPlanArgs ra{};
   ra.X = ix.X;
@@ -928,6 +938,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   ra.cols = sa.rcols;
   ra.R2 = R2;
   ra.exact_tests = counters;
+  ra.status = status;
   if ((rc = dalloc(&ra.cdist, (size_t)ncand, st))) return rc;
   fr.keep(ra.cdist);
   if ((rc = dalloc(&ra.mcount, (size_t)m, st))) return rc;
@@ -941,7 +952,12 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   unsigned long long hc[2];
   B2K_CUDA(cudaMemcpyAsync(&nnz, indptr + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
+  if (hstatus[0] != DEV_OK) {  // the fill pass gave up (classify skipped its rows)
+    cudaFreeAsync(indptr, st);
+    return fail(B2K_ETIMEOUT, "a bounded device wait gave up (code %d)", hstatus[0]);
+  }
   int64_t* indices = nullptr;
   double* dist = nullptr;
   if ((rc = dalloc(&indices, (size_t)nnz, st))) {

@@ -454,6 +454,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
       c.counters = b->counters;
       c.perm = nullptr;
       c.row_base = p.row0;
+      c.status = b->zero_block;  // a screen that gave up leaves its lists unfinished
     }
   }
   TcProblem* d_tc = nullptr;

@@ -289,6 +289,12 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   unsigned* hist = reinterpret_cast<unsigned*>(si + kSurvivorCap);  // [256] radix histogram
   const ScreenOut& so = a.scr;
   const int k = a.k, S = a.S;
+  // a screen that gave up left the lists unfinished: touch nothing (the call
+  // reports the error); lane 0's read decides for the whole warp
+  if (a.status) {
+    const int st = lane == 0 ? *reinterpret_cast<volatile const int*>(a.status) : 0;
+    if (__shfl_sync(0xffffffffu, st, 0) != DEV_OK) return;
+  }
 
   // 1. overflow check
   bool overflow = false;
@@ -458,12 +464,20 @@ struct ExactShared {
   unsigned long long* prefix;
   int* rank;
   int* count;
+  int* flag;   // the call's error word as thread 0 read it for this row
 };
 
 // One query row of one problem, by the whole CTA.  `sc` is the CTA's scratch
 // of a.n canonical values (or null: recompute per pass).
 __device__ __forceinline__ void exact_row(const ExactArgs& a, int64_t row, double* sc, const ExactShared& sh) {
   const int tid = threadIdx.x;
+  // an earlier kernel of the call gave up (its fallback rows may be
+  // unfinished), or another row of this launch failed: leave the outputs
+  // alone.  Thread 0's read decides for the CTA (the word can change while
+  // this kernel runs).
+  if (tid == 0) *sh.flag = *reinterpret_cast<volatile const int*>(a.status);
+  __syncthreads();
+  if (*sh.flag != DEV_OK) return;
   double* cs = sh.cs;
   int* ci = sh.ci;
   unsigned* hist = sh.hist;
@@ -548,14 +562,15 @@ __device__ __forceinline__ void exact_row(const ExactArgs& a, int64_t row, doubl
   extern __shared__ uint8_t smem[];                                        \
   __shared__ unsigned hist[256];                                           \
   __shared__ unsigned long long s_prefix;                                  \
-  __shared__ int s_rank, s_count;                                          \
+  __shared__ int s_rank, s_count, s_flag;                                  \
   ExactShared sh;                                                          \
   sh.cs = reinterpret_cast<double*>(smem);                                 \
   sh.ci = reinterpret_cast<int*>(sh.cs + kExactCap);                       \
   sh.hist = hist;                                                          \
   sh.prefix = &s_prefix;                                                   \
   sh.rank = &s_rank;                                                       \
-  sh.count = &s_count;
+  sh.count = &s_count;                                                     \
+  sh.flag = &s_flag;
 
 __global__ void __launch_bounds__(kExactThreads)
     exact_kernel(const __grid_constant__ ExactArgs a) {

@@ -21,10 +21,13 @@ enum DevError : int {
   DEV_TIMEOUT_ACC = 3,     // MMA / epilogue accumulator hand-off timed out
   DEV_TIMEOUT_A = 4,       // query tile hand-off timed out
   DEV_TOO_MANY_TIES = 5,   // exact fallback candidate buffer overflowed
+  DEV_TIMEOUT_DRAIN = 6,   // the exit path's wait for the CTA's own async work gave up
 };
 
 // ~2^26 polls of try_wait (each poll may itself suspend for a short time):
-// several seconds, far beyond any legitimate wait in these kernels.
+// several seconds, far beyond any legitimate wait in these kernels.  Kernels
+// take their limit as a parameter (default this); drain waits on the exit
+// path always use it.
 constexpr uint32_t kSpinLimit = 1u << 26;
 
 B2K_DEV uint32_t smem_u32(const void* p) {
@@ -62,14 +65,24 @@ B2K_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase with the given parity to complete.  Returns false
-// (after recording `code` in *status) if the limit is reached or another role
-// of this kernel already reported an error.
-B2K_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* status, int code) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+// (after recording `code` in *status) after `limit` polls, or when another
+// role of this kernel already reported an error.
+B2K_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* status, int code,
+                       uint32_t limit = kSpinLimit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 1023u) == 1023u && *status != DEV_OK) return false;
   }
   atomicCAS(const_cast<int*>(status), DEV_OK, code);
+  return false;
+}
+// Exit-path wait for this CTA's own asynchronous work (a bulk copy or the
+// tensor-core operations it issued): those complete by themselves, so it
+// ignores other roles' errors and uses the full limit.
+B2K_DEV bool mbar_wait_drain(uint64_t* bar, uint32_t parity, volatile int* status) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicCAS(const_cast<int*>(status), DEV_OK, DEV_TIMEOUT_DRAIN);
   return false;
 }
 

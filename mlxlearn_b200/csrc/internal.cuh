@@ -161,6 +161,7 @@ struct CertifyArgs {
   int64_t row_base;    // added to the row in fallback_list entries (batched runs)
   int squared;         // write squared distances (else their square roots)
   const int* cols;     // list column -> training row (grouped operand rows), or null
+  const int* status;   // error word of the call: nonzero (a screen gave up) = do nothing
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
 // problem p owns global rows [row_start[p], row_start[p + 1]) of the batch
@@ -192,8 +193,10 @@ void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, c
                         cudaStream_t st);
 
 // ------------------------------------------------------------------ radius
-// cols[i] = xperm[cols[i]]: candidate columns of a grouped operand to training rows
-void launch_translate_cols(int* cols, int64_t count, const int* xperm, cudaStream_t st);
+// cols[i] = xperm[cols[i]]: candidate columns of a grouped operand to training
+// rows (nothing when *status records an error: the fill pass may be unfinished)
+void launch_translate_cols(int* cols, int64_t count, const int* xperm, const int* status,
+                           cudaStream_t st);
 struct RadiusPlanArgs {
   const float* X;
   const float* Q;
@@ -207,6 +210,7 @@ struct RadiusPlanArgs {
   int64_t* mcount;       // [m] members per query
   double R2;
   unsigned long long* exact_tests;
+  const int* status;     // error word of the call: nonzero = leave the outputs alone
 };
 void launch_radius_threshold(const double* nq, const float* E, int64_t m, int64_t m_pad,
                              double R2, float* thr, cudaStream_t st);
@@ -275,5 +279,8 @@ int index_prepare_bf16_stats(Index& ix, uint16_t* Xh, uint16_t* Xaug, uint16_t* 
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
                         uint32_t box_inner, uint32_t box_outer, int swizzle_bytes = 128);
 int num_sms(int device);
+// Polls a screen's bounded waits make before giving up: 2^26 unless
+// B2K_SPIN_LIMIT sets it (tests force the timeout path with it).
+uint32_t device_spin_limit();
 
 }  // namespace b2k

@@ -179,6 +179,7 @@ extern "C" B2K_API int b2k_knn_device_noalloc(b2k_index* h, const float* dQ, int
     ca.fallback_list = fb_list;
     ca.fallback_count = status + 2;
     ca.counters = counters;
+    ca.status = status;
     launch_certify(ca, st);
   }
   ExactArgs ea{};

@@ -124,7 +124,14 @@ struct ClassifyArgs {
   int r2_huge;           // R2 * 2^298 exceeds every key
   ExactKey r2key;        // floor(R2 * 2^298)
   unsigned long long* exact_tests;
+  const int* status;     // nonzero: the fill pass gave up, its candidates are unfinished
 };
+
+// Warp-uniform: lane 0's read of the call's error word decides for the warp.
+__device__ __forceinline__ bool call_failed(const int* status, int lane) {
+  const int st = lane == 0 ? *reinterpret_cast<volatile const int*>(status) : 0;
+  return __shfl_sync(0xffffffffu, st, 0) != DEV_OK;
+}
 
 __device__ __forceinline__ bool key_le(const ExactKey& a, const ExactKey& b) {
   return key_cmp(a, b) <= 0;
@@ -135,6 +142,10 @@ __global__ void classify_kernel(const ClassifyArgs a) {
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= a.m) return;
+  if (call_failed(a.status, lane)) {  // no members: the host reports the error
+    if (lane == 0) a.mcount[row] = 0;
+    return;
+  }
   const float* q = a.Q + (size_t)row * a.d;
   int64_t members = 0;
   unsigned exact = 0;
@@ -181,7 +192,7 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
                                int64_t* __restrict__ indices, double* __restrict__ dist) {
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (row >= a.m) return;
+  if (row >= a.m || call_failed(a.status, lane)) return;
   int64_t out = indptr[row];
   for (int s = 0; s < a.S; ++s) {
     const size_t slot = (size_t)s * a.m_pad + row;
@@ -208,8 +219,10 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
 }
 
 __global__ void translate_cols_kernel(int* __restrict__ cols, int64_t count,
-                                      const int* __restrict__ xperm) {
+                                      const int* __restrict__ xperm,
+                                      const int* __restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (*reinterpret_cast<volatile const int*>(status) != DEV_OK) return;
   if (i < count) cols[i] = __ldg(xperm + cols[i]);
 }
 
@@ -392,6 +405,7 @@ void launch_classify(const RadiusPlanArgs& r, cudaStream_t st) {
   a.mcount = r.mcount;
   a.R2 = r.R2;
   a.exact_tests = r.exact_tests;
+  a.status = r.status;
   radius_band(r.d, r.R2, &a.f_in, &a.f_out, &a.all, &a.r2_huge, a.r2key.w);
   if (r.m <= 0) return;
   const int warps = 8;
@@ -408,15 +422,18 @@ void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* ind
   a.rcount = r.rcount;
   a.cols = r.cols;
   a.cdist = r.cdist;
+  a.status = r.status;
   if (r.m <= 0) return;
   const int warps = 8;
   compact_kernel<<<(unsigned)((r.m + warps - 1) / warps), warps * 32, 0, st>>>(a, indptr,
                                                                                  indices, dist);
 }
 
-void launch_translate_cols(int* cols, int64_t count, const int* xperm, cudaStream_t st) {
+void launch_translate_cols(int* cols, int64_t count, const int* xperm, const int* status,
+                           cudaStream_t st) {
   if (count <= 0) return;
-  translate_cols_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(cols, count, xperm);
+  translate_cols_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(cols, count, xperm,
+                                                                          status);
 }
 
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,

@@ -61,6 +61,7 @@ namespace b2k {
 namespace {
 
 struct TcParams {
+  uint32_t spin_limit;       // polls of a main-loop wait before it gives up
   int stages;
   int a_blocks;              // 64-column query blocks the resident A region holds
   int m_tiles, S;            // single problem: m_tiles * S units, dealt round-robin
@@ -137,14 +138,14 @@ struct UnitCursor {
     if (producer) {
       int w = atomicAdd(p.unit_counter, 1);
       if (w >= end) w = -1;
-      ok = mbar_wait(&ring.empty[rs], rph ^ 1, p.status, DEV_TIMEOUT_A);
+      ok = mbar_wait(&ring.empty[rs], rph ^ 1, p.status, DEV_TIMEOUT_A, p.spin_limit);
       if (ok) {
         ring.idx[rs] = w;
         mbar_arrive(&ring.full[rs]);
       }
       *v = w;
     } else {
-      ok = mbar_wait(&ring.full[rs], rph, p.status, DEV_TIMEOUT_A);
+      ok = mbar_wait(&ring.full[rs], rph, p.status, DEV_TIMEOUT_A, p.spin_limit);
       if (ok) {
         *v = *reinterpret_cast<volatile int*>(&ring.idx[rs]);
         mbar_arrive(&ring.empty[rs]);
@@ -201,7 +202,7 @@ __host__ __device__ inline uint32_t tc_stage_bytes(bool a_stream) {
 __host__ __device__ inline size_t tc_smem_bytes(int KB, int stages, bool a_stream, int ew) {
   size_t a = a_stream ? 0 : (size_t)KB * kATileBytes;
   size_t spill = (size_t)ew * 32 * kSpillStride * sizeof(float);
-  size_t bars = (2 * (size_t)stages + 7 + kGoRing + 2 * kUnitRing) * sizeof(uint64_t) + 16 +
+  size_t bars = (2 * (size_t)stages + 8 + kGoRing + 2 * kUnitRing) * sizeof(uint64_t) + 16 +
                 kUnitRing * sizeof(int);
   return 1024 /*alignment slack*/ + kAAugBytes + a + (size_t)tc_stage_bytes(a_stream) * stages +
          spill + bars;
@@ -250,7 +251,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   uint64_t* acc_full = a_empty + 1;   // [2]
   uint64_t* acc_empty = acc_full + 2; // [2]
   uint64_t* aaug_full = acc_empty + 2;
-  uint64_t* go = aaug_full + 1;       // [kGoRing] gate -> MMA issuer, one per chunk in turn
+  uint64_t* mma_drain = aaug_full + 1;  // the MMA issuer's exit: all its MMAs complete
+  uint64_t* go = mma_drain + 1;       // [kGoRing] gate -> MMA issuer, one per chunk in turn
   UnitRing ring;
   ring.full = go + kGoRing;            // [kUnitRing]
   ring.empty = ring.full + kUnitRing;  // [kUnitRing]
@@ -260,6 +262,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   volatile int* status = p.status;
+  const uint32_t lim = p.spin_limit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < nst; ++s) {
@@ -275,6 +278,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
     mbar_init(&acc_empty[0], kEpiThreads);
     mbar_init(&acc_empty[1], kEpiThreads);
     mbar_init(aaug_full, 1);
+    mbar_init(mma_drain, 1);
     for (int g = 0; g < kGoRing; ++g) mbar_init(&go[g], 1);
     for (int r = 0; r < kUnitRing; ++r) {
       mbar_init(&ring.full[r], 1);
@@ -305,6 +309,9 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       mbar_arrive_expect_tx(aaug_full, kAAugBytes);
       tma_load_2d(aaug_smem, &maps.aaug, aaug_full, 0, 0);
       uint32_t stage = 0, phase = 0, a_phase = 0;
+      // copies issued, for the exit path: per stage the parity of the full
+      // phase its latest load completes, and the same for the query tile
+      uint32_t pend = 0, pend_par = 0, a_loads = 0;
       UnitCursor<BATCH> cur(p, ring, true);
       TcUnit x;
       while (cur.next(p, x)) {
@@ -316,8 +323,9 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
         const CUtensorMap* tmB = &maps.b[g];
         const CUtensorMap* tmBaug = &maps.baug[g];
         if (!A_STREAM) {
-          if (!mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A)) goto prod_done;
+          if (!mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A, lim)) goto prod_done;
           a_phase ^= 1;
+          ++a_loads;
           mbar_arrive_expect_tx(a_full, KB * kATileBytes);
           for (int kb = 0; kb < KB; ++kb)
             tma_load_2d(a_smem + kb * kATileBytes, tmA, a_full, kb * kTcBK, a_row);
@@ -325,7 +333,10 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
         for (int j = x.j0; j < x.j1; ++j) {
           const int b_row = b_row0 + j * kTcBN;
           for (int kb = 0; kb < KB; ++kb) {
-            if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) goto prod_done;
+            if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY, lim))
+              goto prod_done;
+            pend |= 1u << stage;
+            pend_par = (pend_par & ~(1u << stage)) | (phase << stage);
             uint8_t* st = b_smem + (size_t)stage * stage_bytes;
             const bool last = kb == KB - 1;
             mbar_arrive_expect_tx(&full[stage], (A_STREAM ? kATileBytes : 0) + kBTileBytes +
@@ -340,26 +351,32 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
           }
         }
       }
-      // Drain: wait until the consumer released every stage we filled, so no
-      // bulk copy is still in flight when the CTA exits.
+      // Drain: wait until the consumer released every stage we filled.
       for (int s = 0; s < nst; ++s) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY)) break;
+        if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_TIMEOUT_EMPTY, lim)) break;
         if (++stage == (uint32_t)nst) {
           stage = 0;
           phase ^= 1;
         }
       }
-      mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A);
       // with claimed units the MMA warp releases the query tile after every
       // unit: take the last release so no arrival lands after the CTA exits
-      if (!A_STREAM && cur.dyn) mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A);
-    prod_done:;
+      if (!A_STREAM && cur.dyn) mbar_wait(a_empty, a_phase ^ 1, status, DEV_TIMEOUT_A, lim);
+    prod_done:
+      // Whichever way the loop ended (a wait that gave up included), no bulk
+      // copy of this CTA may still be in flight when it exits: wait for the
+      // latest load of every stage, of the query tile and of the ones columns.
+      for (int s = 0; s < nst; ++s)
+        if (pend & (1u << s)) mbar_wait_drain(&full[s], (pend_par >> s) & 1u, status);
+      if (a_loads) mbar_wait_drain(a_full, (a_loads - 1) & 1u, status);
+      mbar_wait_drain(aaug_full, 0, status);
     }
   } else if (warp == 1) {
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
       uint32_t stage = 0, acc_it = 0, chunk = 0;
+      bool issued = false;  // any MMA (for the exit path's drain)
       {
         const uint64_t aaug_desc = smem_desc_sw32(aaug_smem);
         UnitCursor<BATCH> cur(p, ring, false);
@@ -375,11 +392,12 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
                 // the chunk's operands are in shared memory (and, at kb 0, the
                 // accumulator is free)
                 if (!mbar_wait(&go[chunk % kGoRing], (chunk / kGoRing) & 1, status,
-                               DEV_TIMEOUT_ACC))
+                               DEV_TIMEOUT_ACC, lim))
                   goto mma_done;
                 ++chunk;
                 tc_fence_after();
               }
+              issued = true;
               uint8_t* st = b_smem + (size_t)stage * stage_bytes;
               const uint8_t* a_tile = A_STREAM ? st : a_smem + kb * kATileBytes;
               const uint64_t adesc = smem_desc_sw128(a_tile);
@@ -402,13 +420,19 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
           if (!A_STREAM && cur.more()) mma_commit(a_empty);
         }
       }
-    mma_done:;
+    mma_done:
+      // every MMA this thread issued has completed before the CTA moves on to
+      // free its TMEM (on the normal path the epilogue has seen them all)
+      if (issued) {
+        mma_commit(mma_drain);
+        mbar_wait_drain(mma_drain, 0, status);
+      }
     }
   } else if (warp == 2 + EW) {
     // --------------------------------------------------------------- gate
     if (lane == 0) {
       uint32_t stage = 0, phase = 0, a_phase = 0, acc_it = 0, chunk = 0;
-      if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A)) goto gate_done;
+      if (!mbar_wait(aaug_full, 0, status, DEV_TIMEOUT_A, lim)) goto gate_done;
       {
         UnitCursor<BATCH> cur(p, ring, false);
         TcUnit x;
@@ -416,15 +440,16 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
           const int KB = x.pr->KB;
           const int C = max(1, min(KB, nst / 2));  // as the MMA issuer
           if (!A_STREAM) {
-            if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A)) goto gate_done;
+            if (!mbar_wait(a_full, a_phase, status, DEV_TIMEOUT_A, lim)) goto gate_done;
             a_phase ^= 1;
           }
           for (int j = x.j0; j < x.j1; ++j) {
             const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
             // the epilogue has read this buffer's previous tile
-            if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC)) goto gate_done;
+            if (!mbar_wait(&acc_empty[buf], apar ^ 1, status, DEV_TIMEOUT_ACC, lim))
+              goto gate_done;
             for (int kb = 0; kb < KB; ++kb) {
-              if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL)) goto gate_done;
+              if (!mbar_wait(&full[stage], phase, status, DEV_TIMEOUT_FULL, lim)) goto gate_done;
               if (++stage == (uint32_t)nst) {
                 stage = 0;
                 phase ^= 1;
@@ -487,7 +512,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
         pending_key = live ? sink.tile_fetch() : 0u;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
         // warp-uniform outcome, so collective sinks never run on a partial warp
-        if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC)))
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC, lim)))
           goto epi_done;
         tc_fence_after();
         const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN + c0 * 32;
@@ -580,6 +606,7 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
   TcParams q = p;
   q.stages = stages;
   q.a_blocks = KB_max;
+  q.spin_limit = device_spin_limit();
   auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
