@@ -377,6 +377,7 @@ def run_ours(args):
         ms_bf16, st_bf16 = timed("bf16", args.steps, args.warmup)
     clocks = clk.summary()
     ms_fp32, st_fp32 = timed("fp32", max(1, min(2, args.steps)), 1)
+    ms_tf32, st_tf32 = timed("tf32", max(1, min(5, args.steps)), 2)
 
     # e2e: public host API, page-locked host buffers, copies inside the timed region
     Qh = torch.from_numpy(Q).pin_memory().numpy()
@@ -407,6 +408,10 @@ def run_ours(args):
         traffic = os.environ.get("B2K_SCREEN_TRAFFIC_BYTES", SCREEN_TRAFFIC_BYTES)
         roof["traffic"] = None if traffic is None else float(traffic)
         fp32_screen_ms = statistics.median(s["screen_ms"] for s in st_fp32)
+        tf32_screen_ms = statistics.median(s["screen_ms"] for s in st_tf32)
+        # no measured tf32 figure: kind::tf32 does half the FLOPs of kind::f16
+        # per instruction at the same rate, so half the measured bf16 peak
+        tf32_peak = tf_burst / 2
         result = {
             "metric": METRIC,
             "value": ws * N_QUERY / (ms_bf16 / 1000.0),
@@ -429,6 +434,16 @@ def run_ours(args):
                            "screen_frac_of_fp32_nominal":
                                flops / (fp32_screen_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
                            "bf16_speedup": ms_fp32 / ms_bf16},
+            "plain_tf32": {"value": ws * N_QUERY / (ms_tf32 / 1000.0), "unit": "queries/s",
+                           "form": "tf32 tcgen05 screen (kind::tf32, operands rounded to tf32) "
+                                   "+ the same certify pass",
+                           "ms_per_step": ms_tf32, "screen_ms": tf32_screen_ms,
+                           "screen_tflops": flops / (tf32_screen_ms * 1e-3) / 1e12,
+                           "screen_frac_of_tf32_peak":
+                               flops / (tf32_screen_ms * 1e-3) / 1e12 / tf32_peak,
+                           "tf32_peak_source": f"half the {peak_kind} burst bf16 figure",
+                           "candidates_per_query": st_tf32[-1]["candidates"] / N_QUERY,
+                           "bf16_speedup": ms_tf32 / ms_bf16},
             "screen_stats": {k: v for k, v in st_bf16[-1].items()},
             "e2e": {"value": ws * N_QUERY / e2e_s, "unit": "queries/s",
                     "h2d_bytes_per_step": int(Qh.nbytes),

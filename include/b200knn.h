@@ -49,6 +49,8 @@ extern "C" {
 #define B2K_MODE_FP32 1        /* plain form: fp32 CUDA-core Gram screen      */
 #define B2K_MODE_BF16 2        /* bf16 tcgen05 screen + certified re-rank     */
 #define B2K_MODE_EXACT 3       /* float64 exhaustive scan + exact ties (slow) */
+#define B2K_MODE_TF32 4        /* plain form on the tensor cores: tf32 tcgen05
+                                  screen + the same certified re-rank         */
 /* Flag ORed into the mode of b2k_knn / b2k_knn_device: distances are returned
  * as the canonical float64 squared distance instead of its square root (the
  * `_squared` option of DeviceNeighborIndex.query,

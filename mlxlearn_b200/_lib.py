@@ -29,8 +29,10 @@ MODE_AUTO = 0
 MODE_FP32 = 1
 MODE_BF16 = 2
 MODE_EXACT = 3
+MODE_TF32 = 4
 MODE_SQUARED = 16  # flag: squared distances (B2K_MODE_SQUARED)
-MODES = {"auto": MODE_AUTO, "fp32": MODE_FP32, "bf16": MODE_BF16, "exact": MODE_EXACT}
+MODES = {"auto": MODE_AUTO, "fp32": MODE_FP32, "bf16": MODE_BF16, "exact": MODE_EXACT,
+         "tf32": MODE_TF32}
 
 
 class Stats(ctypes.Structure):

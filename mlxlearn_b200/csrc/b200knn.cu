@@ -103,21 +103,34 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
-                        uint32_t box_inner, uint32_t box_outer, int swizzle_bytes) {
+static bool tensor_map_2d(CUtensorMap* map, CUtensorMapDataType type, uint64_t elem_bytes,
+                          const void* base, uint64_t inner, uint64_t outer, uint32_t box_inner,
+                          uint32_t box_outer, int swizzle_bytes) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {inner, outer};
-  cuuint64_t strides[1] = {inner * 2};
+  cuuint64_t strides[1] = {inner * elem_bytes};
   cuuint32_t box[2] = {box_inner, box_outer};
   cuuint32_t estr[2] = {1, 1};
   const CUtensorMapSwizzle sw = swizzle_bytes == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
                                 : swizzle_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
                                                       : CU_TENSOR_MAP_SWIZZLE_128B;
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
-                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = fn(map, type, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
+}
+
+bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                        uint32_t box_inner, uint32_t box_outer, int swizzle_bytes) {
+  return tensor_map_2d(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, inner, outer, box_inner,
+                       box_outer, swizzle_bytes);
+}
+
+bool tensor_map_2d_f32(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                       uint32_t box_inner, uint32_t box_outer, int swizzle_bytes) {
+  return tensor_map_2d(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, inner, outer, box_inner,
+                       box_outer, swizzle_bytes);
 }
 
 // ------------------------------------------------------------------ helpers
@@ -258,6 +271,13 @@ static int make_row_groups(Index& ix) {
   return B2K_OK;
 }
 
+// Row grouping shared by the tensor-core operands (the caller holds ix.mu):
+// decided once, with the first operand built.
+static int ensure_row_groups(Index& ix) {
+  if (ix.xperm || ix.bf16_ready || ix.tf32_ready || !group_rows_enabled(ix)) return B2K_OK;
+  return make_row_groups(ix);
+}
+
 static int ensure_bf16(Index& ix) {
   std::lock_guard<std::mutex> lock(ix.mu);
   if (ix.bf16_ready) return B2K_OK;
@@ -265,7 +285,7 @@ static int ensure_bf16(Index& ix) {
   ix.dp = (int32_t)round_up(ix.d, kTcBK);
   ix.n_pad_tc = round_up(ix.n, kTcBN);
   int rc;
-  if (group_rows_enabled(ix) && (rc = make_row_groups(ix))) return rc;
+  if ((rc = ensure_row_groups(ix))) return rc;
   B2K_CUDA(cudaMalloc(&ix.Xh, (size_t)ix.n_pad_tc * ix.dp * sizeof(uint16_t)));
   launch_prep_index_bf16(&ix, ix.Xh, st, ix.xperm);
   B2K_CUDA(cudaGetLastError());
@@ -287,6 +307,37 @@ static int ensure_bf16(Index& ix) {
       !tensor_map_2d_bf16(&ix.tmap_aaug, ix.aug_ones, kTcAug, kTcBM, kTcAug, kTcBM, 32))
     return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the norm columns");
   ix.bf16_ready = true;
+  return B2K_OK;
+}
+
+// tf32 operand of the kind::tf32 screen, in the same row order as the bf16 one.
+static int ensure_tf32(Index& ix) {
+  std::lock_guard<std::mutex> lock(ix.mu);
+  if (ix.tf32_ready) return B2K_OK;
+  cudaStream_t st = ix.stream;
+  ix.dpt = (int32_t)round_up(ix.d, kTcBKf);
+  ix.n_pad_tc = round_up(ix.n, kTcBN);
+  int rc;
+  if ((rc = ensure_row_groups(ix))) return rc;
+  B2K_CUDA(cudaMalloc(&ix.Xt, (size_t)ix.n_pad_tc * ix.dpt * sizeof(float)));
+  launch_prep_index_tf32(&ix, ix.Xt, st, ix.xperm);
+  B2K_CUDA(cudaGetLastError());
+  B2K_CUDA(cudaMalloc(&ix.Xtaug, (size_t)ix.n_pad_tc * kTcAugF * sizeof(float)));
+  B2K_CUDA(cudaMalloc(&ix.taug_ones, (size_t)kTcBM * kTcAugF * sizeof(float)));
+  launch_prep_aug_tf32(&ix, ix.Xtaug, ix.taug_ones, st, ix.xperm);
+  B2K_CUDA(cudaGetLastError());
+  float stats[8];
+  B2K_CUDA(cudaMemcpyAsync(stats, ix.stats_dev, sizeof(stats), cudaMemcpyDeviceToHost, st));
+  B2K_CUDA(cudaStreamSynchronize(st));
+  ix.xt_max = stats[6];
+  ix.ext_max = stats[7];
+  if (!tensor_map_2d_f32(&ix.tmap_bt, ix.Xt, (uint64_t)ix.dpt, (uint64_t)ix.n_pad_tc, kTcBKf,
+                         kTcBN) ||
+      !tensor_map_2d_f32(&ix.tmap_btaug, ix.Xtaug, kTcAugF, (uint64_t)ix.n_pad_tc, kTcAugF, kTcBN,
+                         32) ||
+      !tensor_map_2d_f32(&ix.tmap_ataug, ix.taug_ones, kTcAugF, kTcBM, kTcAugF, kTcBM, 32))
+    return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the tf32 operand");
+  ix.tf32_ready = true;
   return B2K_OK;
 }
 
@@ -371,8 +422,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     mode = (!ix.range_ok || k > kMaxK) ? B2K_MODE_EXACT
            : (ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16
                                          : B2K_MODE_FP32;
-  if ((mode == B2K_MODE_BF16 || mode == B2K_MODE_FP32) && (!ix.range_ok || k > kMaxK))
-    mode = B2K_MODE_EXACT;
+  if (mode != B2K_MODE_EXACT && (!ix.range_ok || k > kMaxK)) mode = B2K_MODE_EXACT;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->mode_used = mode;
@@ -406,7 +456,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if (rc) return rc;
   } else {
     if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
-    const bool tc = mode == B2K_MODE_BF16;
+    if (mode == B2K_MODE_TF32 && (rc = ensure_tf32(ix))) return rc;
+    const bool tf32 = mode == B2K_MODE_TF32;
+    const bool tc = mode == B2K_MODE_BF16 || tf32;
     const int64_t bm = tc ? kTcBM : kSimtBM;
     const int64_t m_pad = round_up(m, bm);
     const int64_t n_tiles = tc ? ix.n_pad_tc / kTcBN : (ix.n + kSimtBN - 1) / kSimtBN;
@@ -442,9 +494,13 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if ((rc = dalloc(&qp.E, (size_t)m_pad, st))) return rc;
     fr.keep(qp.E);
     qp.flags = status + 4;  // shares the zeroed status block
-    if (tc) {
+    if (tc && !tf32) {
       if ((rc = dalloc(&qp.Ah, (size_t)m_pad * ix.dp, st))) return rc;
       fr.keep(qp.Ah);
+    }
+    if (tf32) {
+      if ((rc = dalloc(&qp.At, (size_t)m_pad * ix.dpt, st))) return rc;
+      fr.keep(qp.At);
     }
     launch_prep_queries(&ix, Qs, m, m_pad, mode, qp, st);
     B2K_CUDA(cudaGetLastError());
@@ -466,11 +522,15 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if (stats) cudaEventRecord(ev[1], st);
     if (tc) {
       CUtensorMap tmap_a;
-      if (!tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
-        return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
+      const bool map_ok =
+          tf32 ? tensor_map_2d_f32(&tmap_a, qp.At, (uint64_t)ix.dpt, (uint64_t)m_pad, kTcBKf,
+                                   kTcBM)
+               : tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK,
+                                    kTcBM);
+      if (!map_ok) return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
       // status[6] (zeroed above) counts the claimed work units
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
-                                kSinkKnn, sa, status, st, perm, status + 6);
+                                kSinkKnn, sa, status, st, perm, status + 6, tf32);
       if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
                           cudaGetErrorString((cudaError_t)lr));
     } else {
@@ -585,7 +645,7 @@ static int validate_knn(const Index& ix, int64_t m, int32_t k, int32_t exclude_s
                 "query rows at offset %lld and %lld training rows.",
                 (long long)m, (long long)q_offset, (long long)ix.n);
   const int32_t base = mode & ~B2K_MODE_SQUARED;
-  if (base < B2K_MODE_AUTO || base > B2K_MODE_EXACT) return fail(B2K_EINVAL, "unknown mode %d", mode);
+  if (base < B2K_MODE_AUTO || base > B2K_MODE_TF32) return fail(B2K_EINVAL, "unknown mode %d", mode);
   return B2K_OK;
 }
 
@@ -751,6 +811,9 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.aug_ones);
   cudaFree(ix.xperm);
   cudaFree(ix.xinv);
+  cudaFree(ix.Xt);
+  cudaFree(ix.Xtaug);
+  cudaFree(ix.taug_ones);
   if (ix.stream) cudaStreamDestroy(ix.stream);
   delete h;
   return B2K_OK;

@@ -130,6 +130,19 @@ B2K_DEV void mma_f16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::tf32 (fp32 operands read as tf32,
+// f32 accumulation; the operands here are already rounded to tf32).
+B2K_DEV void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                      uint32_t accumulate) {
+  asm volatile(
+      "{\n"
+      ".reg .pred p;\n"
+      "setp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n"
+      "}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // Arrive on `bar` when all previously issued tcgen05.mma of this thread complete.
 B2K_DEV void mma_commit(uint64_t* bar) {
   asm volatile(
@@ -190,6 +203,22 @@ B2K_DEV uint64_t smem_desc_sw128(const void* smem_tile) {
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_bf16) {
   return (1u << 4) | (uint32_t(ab_bf16) << 7) | (uint32_t(ab_bf16) << 10) |
          (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+// Instruction descriptor, kind::tf32: D f32, A/B tf32 (format 2), both
+// K-major, shape M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(N >> 3) << 17) |
+         (uint32_t(M >> 4) << 24);
+}
+
+// Round a finite float to the nearest tf32 value (10 explicit mantissa bits,
+// ties to even): the low 13 bits become zero, so the tensor core reads the
+// value exactly.
+B2K_DEV float tf32_rne(float v) {
+  uint32_t u = __float_as_uint(v);
+  u += 0x0FFFu + ((u >> 13) & 1u);
+  return __uint_as_float(u & 0xFFFFE000u);
 }
 
 // --------------------------------------------------------------- arithmetic

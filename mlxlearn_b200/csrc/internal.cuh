@@ -14,6 +14,8 @@ constexpr int kTcBM = 128;   // query rows per tcgen05 tile (TMEM lanes)
 constexpr int kTcBN = 256;   // reference rows per tcgen05 tile (TMEM columns)
 constexpr int kTcBK = 64;    // 16-bit elements per 128-byte swizzle row
 constexpr int kTcAug = 16;   // norm columns appended to every operand row (one K=16 step)
+constexpr int kTcBKf = 32;   // fp32 (tf32) elements per 128-byte swizzle row
+constexpr int kTcAugF = 8;   // tf32 norm columns (one K=8 step, 32 bytes like kTcAug)
 constexpr int kSimtBM = 128; // query rows per CUDA-core tile
 constexpr int kSimtBN = 64;  // reference rows per CUDA-core tile
 constexpr int kListCap = 512;      // screen list entries per (split, query)
@@ -60,6 +62,14 @@ struct Index {
   uint16_t* aug_ones = nullptr;  // [128, 16] bf16 [1, 1, 1, 0...] (query side)
   CUtensorMap tmap_baug;         // over Xaug, box 16 x 256, 32-byte swizzle
   CUtensorMap tmap_aaug;         // over aug_ones, box 16 x 128, 32-byte swizzle
+  // tf32 copy for the tcgen05 kind::tf32 screen (lazy, same row order as Xh)
+  bool tf32_ready = false;
+  int32_t dpt = 0;               // d padded to a multiple of kTcBKf
+  float* Xt = nullptr;           // [n_pad_tc, dpt] tf32-rounded centred rows
+  float* Xtaug = nullptr;        // [n_pad_tc, 8] tf32 [n_hi, n_mid, n_lo, 0...] of ||x - c||^2
+  float* taug_ones = nullptr;    // [128, 8] [1, 1, 1, 0...] (query side)
+  float xt_max = 0, ext_max = 0; // max ||tf32 operand||, max ||(x - c) - tf32 operand||
+  CUtensorMap tmap_bt, tmap_btaug, tmap_ataug;
   // Row grouping of the bf16 operand (reorder.cu): operand row i holds
   // training row xperm[i]; rows sharing a nearest pivot are consecutive, so a
   // query tile's candidates fall in few reference tiles.  Null: identity.
@@ -86,10 +96,16 @@ void launch_prep_index_bf16(const Index* ix, uint16_t* Xh, cudaStream_t st,
 // `ones` is set, also the query-side columns [128, 16].
 void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream_t st,
                      const int* rows = nullptr);
+// The same for the tf32 screen: operand rows [n_pad, dpt] (statistics into
+// stats_dev [6], [7]) and norm columns [n_pad, 8] with the ones [128, 8].
+void launch_prep_index_tf32(const Index* ix, float* Xt, cudaStream_t st, const int* rows);
+void launch_prep_aug_tf32(const Index* ix, float* Xtaug, float* ones, cudaStream_t st,
+                          const int* rows);
 // Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
 struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
   uint16_t* Ah;    // [m_pad, dp] -2*bf16(q - center) (bf16 mode only)
+  float* At;       // [m_pad, dpt] -2*tf32(q - center) (tf32 mode only)
   int* flags;      // [1]: bit 0 = some coordinate outside the screen range
   double* nq;      // [m_pad] ||q - center||^2 (float64), optional
 };
@@ -104,6 +120,7 @@ struct PrepProblem {
   float xh_max, nx_max, ex_max;  // operand statistics of the index for `mode`
   float* E;
   uint16_t* Ah;                  // [m_pad, dp] (bf16 mode)
+  float* At;                     // [m_pad, dp] (tf32 mode; dp is then the tf32 width)
   double* nq;
   int* flags;
 };
@@ -115,10 +132,11 @@ void launch_prep_queries_batch(const PrepProblem* tab, const int64_t* row_start,
 // ---------------------------------------------------------- screen kernels
 constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
 struct SinkArgs;
+// tf32: the kind::tf32 form over the index's tf32 operand (kNN sinks only)
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st,
-                     const int* perm = nullptr, int* unit_counter = nullptr);
+                     const int* perm = nullptr, int* unit_counter = nullptr, bool tf32 = false);
 int tc_column_groups(int k);
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
 // noalloc: one scanner per row (half the list memory of the default two)
@@ -278,6 +296,8 @@ int index_prepare_bf16_stats(Index& ix, uint16_t* Xh, uint16_t* Xaug, uint16_t* 
                              cudaStream_t st, float* xh_max, float* ex_max);
 bool tensor_map_2d_bf16(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
                         uint32_t box_inner, uint32_t box_outer, int swizzle_bytes = 128);
+bool tensor_map_2d_f32(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                       uint32_t box_inner, uint32_t box_outer, int swizzle_bytes = 128);
 int num_sms(int device);
 // Polls a screen's bounded waits make before giving up: 2^26 unless
 // B2K_SPIN_LIMIT sets it (tests force the timeout path with it).

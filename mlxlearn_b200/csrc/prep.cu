@@ -21,6 +21,10 @@
 // with the x-side norms replaced by their maxima over the index and
 //   g = (d + 4) u (1.01)          fp32 FMA chains (CUDA-core screen),
 //   g = (dp + 16) 2^-20           tcgen05 fp32 accumulation (16 ulp per add).
+// The tf32 screen (kind::tf32) works the same way on operands rounded to
+// tf32 here (10 explicit mantissa bits, so the tensor core reads them
+// exactly) with the norm split into three tf32 parts in 8 columns; its
+// measured operand errors are about 8x smaller than bf16's.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -70,7 +74,8 @@ __global__ void center_kernel(const double* __restrict__ sums, int64_t n, int d,
 }
 
 // stats: [0] max |x^| fp32 operand, [1] max ||y||^2, [2] range violations (int),
-//        [3] max |x~| bf16 operand, [4] max |e| bf16, [5] max |e| fp32
+//        [3] max |x~| bf16 operand, [4] max |e| bf16, [5] max |e| fp32,
+//        [6] max |x~| tf32 operand, [7] max |e| tf32
 __global__ void prep_index_kernel(const float* __restrict__ X, int64_t n, int d,
                                   const float* __restrict__ center, float* __restrict__ nx32,
                                   double* __restrict__ nx64, float* __restrict__ stats) {
@@ -141,6 +146,69 @@ __global__ void prep_index_bf16_kernel(const float* __restrict__ X, int64_t n, i
   }
 }
 
+// tf32 operand rows of the index (row i from training row rows[i]).
+__global__ void prep_index_tf32_kernel(const float* __restrict__ X, int64_t n, int d,
+                                       int64_t n_pad, int dpt, const float* __restrict__ center,
+                                       const int* __restrict__ rows, float* __restrict__ Xt,
+                                       float* __restrict__ stats) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  if (row >= n_pad) return;
+  float* xt = Xt + row * dpt;
+  if (row >= n) {
+    for (int i = lane; i < dpt; i += 32) xt[i] = 0.0f;
+    return;
+  }
+  const float* x = X + (rows ? (int64_t)rows[row] : row) * d;
+  double hn = 0.0, en = 0.0, yy = 0.0;
+  for (int i = lane; i < dpt; i += 32) {
+    const float v = i < d ? x[i] : 0.0f;
+    const float c = i < d ? center[i] : 0.0f;
+    const double y = (double)v - (double)c;
+    const float h = tf32_rne(v - c);
+    xt[i] = h;
+    const double e = y - (double)h;
+    hn += (double)h * (double)h;
+    en += e * e;
+    yy += y * y;
+  }
+  hn = warp_sum(hn);
+  en = warp_sum(en);
+  yy = warp_sum(yy);
+  if (lane == 0) {
+    atomic_max_pos(stats + 6, __double2float_ru(sqrt(hn) * (1.0 + 1e-15)));
+    atomic_max_pos(stats + 7, __double2float_ru(sqrt(en) * (1.0 + 1e-15) + 0x1p-50 * sqrt(yy)));
+  }
+}
+
+// Norm columns of the tf32 screen: ||y_x||^2 as three tf32 parts (residual
+// below 2^-33 of the value), NaN on padding rows; query side [1, 1, 1, 0...].
+__global__ void prep_aug_tf32_kernel(const double* __restrict__ nx64, int64_t n, int64_t n_pad,
+                                     const int* __restrict__ rows, float* __restrict__ Xtaug,
+                                     float* __restrict__ ones) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ones && row < kTcBM) {
+    for (int c = 0; c < kTcAugF; ++c) ones[row * kTcAugF + c] = c < 3 ? 1.0f : 0.0f;
+  }
+  if (row >= n_pad) return;
+  float* a = Xtaug + row * kTcAugF;
+  for (int c = 3; c < kTcAugF; ++c) a[c] = 0.0f;
+  if (row >= n) {
+    a[0] = __uint_as_float(0x7fc00000u);
+    a[1] = 0.0f;
+    a[2] = 0.0f;
+    return;
+  }
+  const double v = nx64[rows ? (int64_t)rows[row] : row];
+  const float hi = tf32_rne((float)v);
+  const double r1 = v - (double)hi;
+  const float mid = tf32_rne((float)r1);
+  const double r2 = r1 - (double)mid;
+  a[0] = hi;
+  a[1] = mid;
+  a[2] = tf32_rne((float)r2);
+}
+
 // Norm columns for the tensor-core screen: ||y_x||^2 (float64) as three bf16
 // parts hi + mid + lo (residual below 2^-26 of the value), NaN on padding
 // rows; the query side is [1, 1, 1, 0, ...].
@@ -177,18 +245,22 @@ __global__ void prep_aug_kernel(const double* __restrict__ nx64, int64_t n, int6
 __device__ __forceinline__ void prep_query_row(const PrepProblem& P, int64_t row, int lane) {
   const double u = 0x1p-24;
   const bool bf16 = P.mode == B2K_MODE_BF16;
+  const bool tf32 = P.mode == B2K_MODE_TF32;
+  const bool tc = bf16 || tf32;  // tensor-core screens: padded width, norm columns
   const int d = P.d, dp = P.dp;
   __nv_bfloat16* Ah = reinterpret_cast<__nv_bfloat16*>(P.Ah);
   if (row >= P.m) {
     if (bf16)
       for (int i = lane; i < dp; i += 32) Ah[row * dp + i] = __float2bfloat16_rn(0.0f);
+    if (tf32)
+      for (int i = lane; i < dp; i += 32) P.At[row * dp + i] = 0.0f;
     if (lane == 0) P.E[row] = 0.0f;
     return;
   }
   const float* q = P.Q + row * d;
   double yy = 0.0, hn = 0.0, en = 0.0;
   bool ok = true;
-  const int width = bf16 ? dp : d;
+  const int width = tc ? dp : d;
   for (int i = lane; i < width; i += 32) {
     const float v = i < d ? q[i] : 0.0f;
     const float c = i < d ? P.center[i] : 0.0f;
@@ -200,6 +272,10 @@ __device__ __forceinline__ void prep_query_row(const PrepProblem& P, int64_t row
       const __nv_bfloat16 h = __float2bfloat16_rn(h32);
       hv = (double)__bfloat162float(h);
       Ah[row * dp + i] = __float2bfloat16_rn(-2.0f * __bfloat162float(h));  // exact
+    } else if (tf32) {
+      const float h = tf32_rne(h32);
+      hv = (double)h;
+      P.At[row * dp + i] = -2.0f * h;  // exact
     } else {
       hv = (double)h32;
     }
@@ -218,9 +294,11 @@ __device__ __forceinline__ void prep_query_row(const PrepProblem& P, int64_t row
     const double XH = P.xh_max, EX = P.ex_max, NX = P.nx_max;
     // tensor cores: dp feature columns + 16 norm columns accumulated in fp32;
     // the accumulation also carries ||y_x||^2 itself (the g * NX term)
-    const double g = bf16 ? (double)(dp + kTcAug + 16) * 0x1p-20 : (double)(d + 4) * u * 1.01;
+    const double g = bf16   ? (double)(dp + kTcAug + 16) * 0x1p-20
+                     : tf32 ? (double)(dp + kTcAugF + 16) * 0x1p-20
+                            : (double)(d + 4) * u * 1.01;
     double bound = 2.0 * (qh * EX + eq * XH + eq * EX) + 2.0 * g * qh * XH + 2.0 * u * NX +
-                   2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy + (bf16 ? g * NX * 1.01 : 0.0);
+                   2.0 * u * qh * XH * 1.01 + 0x1p-50 * yy + (tc ? g * NX * 1.01 : 0.0);
     bound = bound * (1.0 + 0x1p-16) + (double)width * 0x1p-120;
     P.E[row] = __double2float_ru(bound);
     if (P.nq) P.nq[row] = yy;
@@ -308,22 +386,42 @@ void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream
       reinterpret_cast<__nv_bfloat16*>(ones));
 }
 
+void launch_prep_index_tf32(const Index* ix, float* Xt, cudaStream_t st, const int* rows) {
+  const int warps = 8;
+  const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
+  const int dpt = (ix->d + kTcBKf - 1) / kTcBKf * kTcBKf;
+  const int64_t blocks = (n_pad + warps - 1) / warps;
+  prep_index_tf32_kernel<<<(unsigned)blocks, warps * 32, 0, st>>>(ix->X, ix->n, ix->d, n_pad, dpt,
+                                                                  ix->center, rows, Xt,
+                                                                  ix->stats_dev);
+}
+
+void launch_prep_aug_tf32(const Index* ix, float* Xtaug, float* ones, cudaStream_t st,
+                          const int* rows) {
+  const int64_t n_pad = (ix->n + kTcBN - 1) / kTcBN * kTcBN;
+  const int64_t threads = n_pad > kTcBM ? n_pad : kTcBM;
+  prep_aug_tf32_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      ix->nx64, ix->n, n_pad, rows, Xtaug, ones);
+}
+
 PrepProblem prep_problem(const Index* ix, const float* Q, int64_t m, int64_t m_pad, int mode,
                          const QueryPrep& qp) {
   const bool bf16 = mode == B2K_MODE_BF16;
+  const bool tf32 = mode == B2K_MODE_TF32;
   PrepProblem P{};
   P.Q = Q;
   P.m = m;
   P.m_pad = m_pad;
   P.d = ix->d;
-  P.dp = (ix->d + kTcBK - 1) / kTcBK * kTcBK;
+  P.dp = tf32 ? (ix->d + kTcBKf - 1) / kTcBKf * kTcBKf : (ix->d + kTcBK - 1) / kTcBK * kTcBK;
   P.mode = mode;
   P.center = ix->center;
-  P.xh_max = bf16 ? ix->xh_max : ix->xn_max;
+  P.xh_max = bf16 ? ix->xh_max : tf32 ? ix->xt_max : ix->xn_max;
   P.nx_max = ix->nx_max;
-  P.ex_max = bf16 ? ix->ex_max : ix->ex32_max;
+  P.ex_max = bf16 ? ix->ex_max : tf32 ? ix->ext_max : ix->ex32_max;
   P.E = qp.E;
   P.Ah = qp.Ah;
+  P.At = qp.At;
   P.nq = qp.nq;
   P.flags = qp.flags;
   return P;

@@ -47,6 +47,12 @@
 // Operands are the centred coordinates rounded to bf16 (A = -2 bf16(q - c),
 // B = bf16(x - c)); the certified error bound of v is derived in prep.cu with
 // g = (dp + 32) 2^-20 for the tensor-core fp32 accumulation.
+//
+// The TF32 instantiation is the plain (full-width) form on the tensor cores:
+// kind::tf32 MMAs (M=128, N=256, K=8) over operands rounded to tf32.  In bytes
+// nothing changes: a 128-byte swizzle row holds 32 fp32 instead of 64 bf16,
+// each MMA still advances 32 bytes of K, and the norm columns are 8 fp32
+// (three tf32 parts) instead of 16 bf16 -- the same 32 bytes per row.
 #include <cuda_bf16.h>
 
 #include <cstdlib>
@@ -224,7 +230,7 @@ B2K_DEV uint64_t smem_desc_sw32(const void* smem_tile) {
 // Threads per CTA: producer warp, MMA warp, EW epilogue warps, gate warp.
 __host__ __device__ constexpr int tc_block_threads(int ew) { return 96 + 32 * ew; }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32>
 __global__ void __launch_bounds__(tc_block_threads(EW), 1)
     screen_tc_kernel(const __grid_constant__ TcMapSet<BATCH ? kBatchGroups : 1> maps,
                      const __grid_constant__ TcParams p) {
@@ -374,7 +380,14 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   } else if (warp == 1) {
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_f16(kTcBM, kTcBN, 1);
+      constexpr uint32_t idesc = TF32 ? idesc_tf32(kTcBM, kTcBN) : idesc_f16(kTcBM, kTcBN, 1);
+      // one MMA of the screen's kind: 32 bytes of K (16 bf16 or 8 tf32)
+      auto mma = [&](uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+        if constexpr (TF32)
+          mma_tf32(d_tmem, a, b, idesc, acc);
+        else
+          mma_f16(d_tmem, a, b, idesc, acc);
+      };
       uint32_t stage = 0, acc_it = 0, chunk = 0;
       bool issued = false;  // any MMA (for the exit path's drain)
       {
@@ -403,12 +416,12 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
               const uint64_t adesc = smem_desc_sw128(a_tile);
               const uint64_t bdesc = smem_desc_sw128(st + b_off);
 #pragma unroll
-              for (int kk = 0; kk < kTcBK / 16; ++kk) {
-                // advance 16 bf16 = 32 bytes inside the swizzle atom: +2 in 16-byte units
-                mma_f16(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, idesc, (kb | kk) != 0);
+              for (int kk = 0; kk < 4; ++kk) {
+                // advance 32 bytes inside the 128-byte swizzle atom: +2 in 16-byte units
+                mma(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, (kb | kk) != 0);
               }
               if (kb == KB - 1)  // + ||y_x||^2 through the norm columns
-                mma_f16(d_tmem, aaug_desc, smem_desc_sw32(st + baug_off), idesc, 1);
+                mma(d_tmem, aaug_desc, smem_desc_sw32(st + baug_off), 1);
               mma_commit(&empty[stage]);
               if (++stage == (uint32_t)nst) stage = 0;
             }
@@ -581,7 +594,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   }
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
 size_t tc_variant_smem(int KB_max, int* stages_out) {
   const size_t budget = 227 * 1024;
   int stages = 8;
@@ -591,14 +604,14 @@ size_t tc_variant_smem(int KB_max, int* stages_out) {
   return smem < kMinCtaSmem ? kMinCtaSmem : smem;
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
 int prepare_tc_variant(int KB_max) {
   const size_t smem = tc_variant_smem<Sink, A_STREAM, EW, BATCH>(KB_max, nullptr);
-  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH>;
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, TF32>;
   return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
 int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcParams& p, int KB_max,
                       int grid, cudaStream_t st) {
   int stages = 0;
@@ -607,7 +620,7 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
   q.stages = stages;
   q.a_blocks = KB_max;
   q.spin_limit = device_spin_limit();
-  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH>;
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, TF32>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
@@ -637,12 +650,13 @@ bool tc_lazy_sink(int k) { return k > 16; }
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st, const int* perm,
-                     int* unit_counter) {
+                     int* unit_counter, bool tf32) {
+  if (tf32 && sink_kind != kSinkKnn) return (int)cudaErrorInvalidValue;
   TcParams p{};
   p.unit_counter = unit_counter;
   TcProblem& one = p.one;
   one.m = (int)m;
-  one.KB = ix->dp / kTcBK;
+  one.KB = tf32 ? ix->dpt / kTcBKf : ix->dp / kTcBK;
   one.n_tiles = (int)(ix->n_pad_tc / kTcBN);
   one.tiles_per_split = (one.n_tiles + S - 1) / S;
   one.exclude_self = exclude_self;
@@ -661,9 +675,24 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   if (grid <= 0) return 0;
   TcMapSet<1> maps;
   maps.a[0] = *tmap_a;
-  maps.b[0] = ix->tmap_b;
-  maps.baug[0] = ix->tmap_baug;
-  maps.aaug = ix->tmap_aaug;
+  maps.b[0] = tf32 ? ix->tmap_bt : ix->tmap_b;
+  maps.baug[0] = tf32 ? ix->tmap_btaug : ix->tmap_baug;
+  maps.aaug = tf32 ? ix->tmap_ataug : ix->tmap_aaug;
+  if (tf32) {
+#define B2K_TC_LAUNCH_TF32(SINK, EW)                                                 \
+  (a_stream ? launch_tc_variant<SINK, true, EW, false, true>(maps, p, KB, grid, st) \
+            : launch_tc_variant<SINK, false, EW, false, true>(maps, p, KB, grid, st))
+    if (tc_knn_ew(sa.k) == 16) {
+      if (sa.k <= 8) return B2K_TC_LAUNCH_TF32(KnnSink<8>, 16);
+      if (sa.k <= 12) return B2K_TC_LAUNCH_TF32(KnnSink<12>, 16);
+      return B2K_TC_LAUNCH_TF32(KnnSink<16>, 16);
+    }
+    if (sa.k <= 8) return B2K_TC_LAUNCH_TF32(KnnSink<8>, 8);
+    if (sa.k <= 12) return B2K_TC_LAUNCH_TF32(KnnSink<12>, 8);
+    if (!tc_lazy_sink(sa.k)) return B2K_TC_LAUNCH_TF32(KnnSink<16>, 8);
+    return B2K_TC_LAUNCH_TF32(LazyKnnSink, 8);
+#undef B2K_TC_LAUNCH_TF32
+  }
 #define B2K_TC_LAUNCH(SINK, EW)                                                \
   (a_stream ? launch_tc_variant<SINK, true, EW, false>(maps, p, KB, grid, st) \
             : launch_tc_variant<SINK, false, EW, false>(maps, p, KB, grid, st))

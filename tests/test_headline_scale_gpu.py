@@ -6,7 +6,7 @@ grouping, reference splits, shared k-th values, the certify band of this
 data).  1,024 of those queries are checked bit-exact against the oracle
 (indices, and distances to the canonical float64 value), both as answered
 inside the full 100,000-query batch and as a batch of their own, in the
-bf16 form and the plain fp32 form.
+bf16 form and the two plain forms (tf32 tensor cores, fp32 CUDA cores).
 """
 from __future__ import annotations
 
@@ -34,7 +34,7 @@ def headline():
     return index, Q, Qd, pick, od, oi
 
 
-@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+@pytest.mark.parametrize("mode", ["bf16", "tf32", "fp32"])
 def test_full_batch_matches_oracle(headline, mode):
     index, Q, Qd, pick, od, oi = headline
     dist, idx = index.query_device(Qd, 10, mode=mode, stats=True)

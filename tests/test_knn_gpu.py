@@ -16,7 +16,7 @@ from datasets import cfg1, mixture, pixels
 
 pytestmark = pytest.mark.gpu
 
-MODES = ["bf16", "fp32", "exact"]
+MODES = ["bf16", "tf32", "fp32", "exact"]
 
 
 def make_index(X, **kw):
@@ -53,7 +53,7 @@ def test_self_query_with_duplicates(mode):
     assert not np.any(idx == np.arange(len(Xs))[:, None])
 
 
-@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+@pytest.mark.parametrize("mode", ["bf16", "tf32", "fp32"])
 def test_mixture128_subset(mode):
     C = np.random.default_rng(2).uniform(-1, 1, (1024, 128))
     X, _ = mixture(np.random.default_rng(2), 50000, C, 0.1)
@@ -66,7 +66,7 @@ def test_mixture128_subset(mode):
     assert st["fallback_rows"] == 0, st
 
 
-@pytest.mark.parametrize("mode", ["bf16", "fp32"])
+@pytest.mark.parametrize("mode", ["bf16", "tf32", "fp32"])
 def test_pixels784_subset(mode):
     rng = np.random.default_rng(7)
     X, y, T = pixels(rng, 8000)
@@ -328,8 +328,9 @@ def test_k_across_the_screen_limit(k, rng):
     np.testing.assert_array_equal(dist, od)
 
 
+@pytest.mark.parametrize("mode", ["bf16", "tf32"])
 @pytest.mark.parametrize("group", ["0", "1"])
-def test_row_grouping_both_ways(group, monkeypatch):
+def test_row_grouping_both_ways(group, mode, monkeypatch):
     """The bf16 operand's rows are grouped by nearest pivot (the screen's
     lists hold operand rows, certify maps them back to training rows, a
     self-query excludes its row's operand column); both layouts give the
@@ -345,14 +346,15 @@ def test_row_grouping_both_ways(group, monkeypatch):
     index = make_index(X)
     for k in (1, 10, 40):
         od, oi = oracle.knn(X, Q, k)
-        dist, idx = index.query(Q, k, mode="bf16", stats=True)
+        dist, idx = index.query(Q, k, mode=mode, stats=True)
         np.testing.assert_array_equal(idx, oi)
         np.testing.assert_array_equal(dist, od)
         assert index.last_stats["fallback_rows"] == 0
+        assert index.last_stats["mode_used"] == (2 if mode == "bf16" else 4)
     Xd = torch.from_numpy(X).cuda()
     for lo in (0, 19990):
         od, oi = oracle.knn(X, X[lo:lo + 3000], 9, exclude_self=True, q_offset=lo)
         dd, di = index.query_device(Xd[lo:lo + 3000], 9, exclude_self=True, q_offset=lo,
-                                    mode="bf16")
+                                    mode=mode)
         np.testing.assert_array_equal(di.cpu().numpy(), oi)
         np.testing.assert_array_equal(dd.cpu().numpy(), od)
