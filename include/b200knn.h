@@ -70,6 +70,7 @@ typedef struct b2k_stats {
   int64_t exact_compares;   /* near-tie pairs resolved with exact integer keys */
   double screen_ms;         /* device time of the screen kernel (if timed)     */
   double total_ms;          /* device time of the whole call (if timed)        */
+  int64_t refined;          /* candidates refined in fp32 by the certify pass  */
 } b2k_stats;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -46,6 +46,7 @@ class Stats(ctypes.Structure):
         ("exact_compares", ctypes.c_int64),
         ("screen_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("refined", ctypes.c_int64),
     ]
 
     def as_dict(self):

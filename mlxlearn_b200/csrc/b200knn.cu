@@ -440,10 +440,10 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   int rc;
   if ((rc = dalloc(&status, 8, st))) return rc;
   fr.keep(status);
-  if ((rc = dalloc(&counters, 4, st))) return rc;
+  if ((rc = dalloc(&counters, 8, st))) return rc;
   fr.keep(counters);
   B2K_CUDA(cudaMemsetAsync(status, 0, 8 * sizeof(int), st));
-  B2K_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+  B2K_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
   // NaN / inf queries: flagged on the device, reported with the final status
   // read (the search itself stays bounded on such inputs)
   launch_nonfinite_check(dQ, m * (int64_t)ix.d, status + 5, st);
@@ -494,6 +494,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if ((rc = dalloc(&qp.E, (size_t)m_pad, st))) return rc;
     fr.keep(qp.E);
     qp.flags = status + 4;  // shares the zeroed status block
+    // ||y_q||^2 for the certify pass's two-stage refinement
+    if ((rc = dalloc(&qp.nq, (size_t)m_pad, st))) return rc;
+    fr.keep(qp.nq);
     if (tc && !tf32) {
       if ((rc = dalloc(&qp.Ah, (size_t)m_pad * ix.dp, st))) return rc;
       fr.keep(qp.Ah);
@@ -561,6 +564,8 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     ca.squared = squared;
     ca.cols = tc ? ix.xperm : nullptr;  // lists of the grouped bf16 operand
     ca.status = status;
+    ca.nq = qp.nq;
+    ca.refined = counters + 4;
     launch_certify(ca, st);
     B2K_CUDA(cudaGetLastError());
     // Rows the screen could not certify (a list past capacity, too many
@@ -598,7 +603,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   }
   if (stats) cudaEventRecord(ev[3], st);
   int hstatus[8];
-  unsigned long long hcnt[4];
+  unsigned long long hcnt[5];
   B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaMemcpyAsync(hcnt, counters, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
@@ -623,6 +628,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     stats->exact_compares = (int64_t)hcnt[2];
     stats->fallback_rows = (int64_t)hcnt[3] + second_exact_rows;
     stats->second_pass_rows = second_pass_rows;
+    stats->refined = (int64_t)hcnt[4];
     float ms = 0;
     if (mode != B2K_MODE_EXACT && cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess)
       stats->screen_ms = ms;

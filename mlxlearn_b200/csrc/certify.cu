@@ -6,7 +6,14 @@
 //      splits' k smallest values); threshold Tf = V_k + 2E (rounded up).
 //   2. Candidates = list entries with v <= Tf (tracker.cuh proves that no other
 //      row can be in the answer).
-//   3. Canonical float64 squared distance of each candidate (strictly
+//   3. fp32 refinement with a certified relative bound, in two stages when
+//      the query's squared norm is known: first the k candidates with the
+//      smallest screen values, whose k-th smallest upper bound U0 then drops
+//      every other candidate whose screen lower bound (||y_q||^2 + v - E)
+//      exceeds it -- such a row cannot reach the top k -- and only the rest
+//      are refined.  The survivors are those whose fp32 lower bound reaches
+//      the k-th smallest fp32 upper bound.
+//   3b. Canonical float64 squared distance of each survivor (strictly
 //      sequential, no FMA: bit-identical to the host canonical value).
 //   4. Sort by (value, index); within every run of neighbours whose float64
 //      error intervals overlap (and which reaches into the first k), order by
@@ -279,6 +286,77 @@ __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
   }
 }
 
+// fp32 refinement of the C gathered candidates (ci columns, cv screen values
+// on entry).  Returns C' and leaves ci[0..C') / cv[0..C') = the refined
+// candidates and their fp32 squared distances; every dropped candidate has a
+// certified lower bound above the k-th smallest upper bound of the refined
+// ones, so it could not have survived.  `sa` / `av` are scratch for at most
+// kSurvivorCap stage-one candidates.
+__device__ __forceinline__ int refine_candidates(const CertifyArgs& a, int64_t row,
+                                                 const float* q, int* ci, float* cv, int* sa,
+                                                 float* av, unsigned* hist, int C, float up_f,
+                                                 float abs32, int lane) {
+  const int k = a.k;
+  if (a.nq && C >= 4 * k) {
+    // stage one: the candidates whose screen value is at most the k-th smallest
+    const float Vsel =
+        key_float(warp_radix_kth([&](int c) { return float_key(cv[c]); }, C, k, hist, lane));
+    int nA = 0;
+    for (int base = 0; base < C; base += 32) {
+      const int c = base + lane;
+      const bool in = c < C && cv[c] <= Vsel;
+      const unsigned bal = __ballot_sync(0xffffffffu, in);
+      const int pos = nA + __popc(bal & ((1u << lane) - 1));
+      if (in && pos < kSurvivorCap) sa[pos] = ci[c];
+      nA += __popc(bal);
+    }
+    if (nA <= kSurvivorCap) {
+      __syncwarp();
+      refine_fp32(q, a.X, a.d, sa, av, nA, lane);
+      __syncwarp();
+      const float U0 = key_float(warp_radix_kth(
+          [&](int j) { return float_key(__fadd_ru(__fmul_ru(av[j], up_f), abs32)); }, nA, k,
+          hist, lane));
+      // stage two: the other candidates whose screen lower bound
+      // ||y_q||^2 + v - E (rounded down) reaches U0, compacted in place
+      const double nq = a.nq[row], E = (double)a.E[row];
+      int w = 0;
+      for (int base = 0; base < C; base += 32) {
+        const int c = base + lane;
+        int col = 0;
+        float v = 0.0f;
+        bool keep = false;
+        if (c < C) {
+          col = ci[c];
+          v = cv[c];
+          keep = v > Vsel && __dadd_rd(__dadd_rd(nq, (double)v), -E) <= (double)U0;
+        }
+        // every lane has read its entry before any write (a write lands at or
+        // below its writer's own position)
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int p = w + __popc(bal & ((1u << lane) - 1));
+          ci[p] = col;
+        }
+        w += __popc(bal);
+      }
+      __syncwarp();
+      refine_fp32(q, a.X, a.d, ci, cv, w, lane);
+      __syncwarp();
+      for (int j = lane; j < nA; j += 32) {
+        ci[w + j] = sa[j];
+        cv[w + j] = av[j];
+      }
+      __syncwarp();
+      return w + nA;
+    }
+    __syncwarp();
+  }
+  refine_fp32(q, a.X, a.d, ci, cv, C, lane);
+  __syncwarp();
+  return C;
+}
+
 // One query row of one problem, by one warp; `wbase` is the warp's shared
 // memory (kCertWarpBytes).
 __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, uint8_t* wbase, int lane) {
@@ -357,16 +435,21 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
       const int i = base + lane;
       bool pass = false;
       int col = 0;
+      float v = 0.0f;
       if (i < cnt) {
         const int2 e = lst[i];
-        pass = __int_as_float(e.x) <= Tf;
+        v = __int_as_float(e.x);
+        pass = v <= Tf;
         col = e.y;
       }
       const unsigned bal = __ballot_sync(0xffffffffu, pass);
       const int pos = C + __popc(bal & ((1u << lane) - 1));
       // grouped operand rows: the list holds operand rows, the answer training rows
       if (pass && a.cols) col = __ldg(a.cols + col);
-      if (pass && pos < kCertifyCap) ci[pos] = col;
+      if (pass && pos < kCertifyCap) {
+        ci[pos] = col;
+        cv[pos] = v;  // the screen value until the refinement overwrites it
+      }
       C += __popc(bal);
       if (C > kCertifyCap) {
         too_many = true;
@@ -379,22 +462,22 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
     return;
   }
   __syncwarp();
-  // 4. fp32 refine of every candidate with a certified relative bound
+  // 4. fp32 refine with a certified relative bound
   const float* q = a.Q + (size_t)row * a.d;
-  refine_fp32(q, a.X, a.d, ci, cv, C, lane);
-  __syncwarp();
   const float g32 = (float)((double)(a.d + 5) * 0x1p-24 * 1.01);
   const float abs32 = (float)a.d * 0x1p-126f;
   const float up_f = 1.0f + g32, lo_f = 1.0f - g32;
+  const int Cr = refine_candidates(a, row, q, ci, cv, si, reinterpret_cast<float*>(cs), hist, C,
+                                   up_f, abs32, lane);
   // 5. U = k-th smallest upper bound (radix select over ordered keys)
   const float U = key_float(warp_radix_kth(
-      [&](int c) { return float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)); }, C, k, hist,
+      [&](int c) { return float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)); }, Cr, k, hist,
       lane));
   // 6. survivors: lower bound <= U (everything that can still be in the top k)
   int Cs = 0;
-  for (int base = 0; base < C; base += 32) {
+  for (int base = 0; base < Cr; base += 32) {
     const int c = base + lane;
-    const bool keep = c < C && __fsub_rd(__fmul_rd(cv[c], lo_f), abs32) <= U;
+    const bool keep = c < Cr && __fsub_rd(__fmul_rd(cv[c], lo_f), abs32) <= U;
     const unsigned bal = __ballot_sync(0xffffffffu, keep);
     const int pos = Cs + __popc(bal & ((1u << lane) - 1));
     if (keep && pos < kSurvivorCap) si[pos] = ci[c];
@@ -417,6 +500,7 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   if (lane == 0) {
     atomicAdd(&a.counters[0], (unsigned long long)C);
     atomicAdd(&a.counters[1], (unsigned long long)entries);
+    if (a.refined) atomicAdd(a.refined, (unsigned long long)Cr);
     if (cmp) atomicAdd(&a.counters[2], (unsigned long long)cmp);
   }
 }

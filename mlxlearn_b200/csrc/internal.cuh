@@ -180,6 +180,8 @@ struct CertifyArgs {
   int squared;         // write squared distances (else their square roots)
   const int* cols;     // list column -> training row (grouped operand rows), or null
   const int* status;   // error word of the call: nonzero (a screen gave up) = do nothing
+  const double* nq;    // [m] ||q - center||^2 (float64): enables the two-stage refine, or null
+  unsigned long long* refined;  // candidates refined in fp32 (counter), or null
 };
 void launch_certify(const CertifyArgs& a, cudaStream_t st);
 // problem p owns global rows [row_start[p], row_start[p + 1]) of the batch
