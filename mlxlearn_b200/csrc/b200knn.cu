@@ -924,6 +924,8 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   const int64_t n_tiles = tc ? ix.n_pad_tc / kTcBN : (ix.n + kSimtBN - 1) / kSimtBN;
   const int sms = num_sms(ix.device);
   const int S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
+  // candidate lists per row: one per (split, column group of the screen)
+  const int S_lists = S * (tc ? tc_radius_groups() : simt_column_groups(kSinkRadiusCount));
 
   int* status = nullptr;
   if ((rc = dalloc(&status, 8, st))) return rc;
@@ -953,10 +955,10 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   SinkArgs sa{};
   sa.thr = thr;
   sa.m_pad = (int)m_pad;
-  if ((rc = dalloc(&sa.rcount, (size_t)S * m_pad, st))) return rc;
+  if ((rc = dalloc(&sa.rcount, (size_t)S_lists * m_pad, st))) return rc;
   fr.keep(sa.rcount);
   int64_t* roff = nullptr;
-  if ((rc = dalloc(&roff, (size_t)S * m_pad + 1, st))) return rc;
+  if ((rc = dalloc(&roff, (size_t)S_lists * m_pad + 1, st))) return rc;
   fr.keep(roff);
   sa.roff = roff;
   CUtensorMap tmap_a;
@@ -975,10 +977,11 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
     return B2K_OK;
   };
   if ((rc = screen(kSinkRadiusCount))) return rc;
-  launch_scan_split_counts(sa.rcount, S, m, m_pad, roff, roff + (size_t)S * m_pad, st);
+  launch_scan_split_counts(sa.rcount, S_lists, m, m_pad, roff, roff + (size_t)S_lists * m_pad,
+                           st);
   int64_t ncand = 0;
   int hstatus[8];
-  B2K_CUDA(cudaMemcpyAsync(&ncand, roff + (size_t)S * m_pad, sizeof(int64_t),
+  B2K_CUDA(cudaMemcpyAsync(&ncand, roff + (size_t)S_lists * m_pad, sizeof(int64_t),
                            cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
@@ -990,10 +993,12 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   if ((rc = dalloc(&sa.rcols, (size_t)ncand, st))) return rc;
   fr.keep(sa.rcols);
   if ((rc = screen(kSinkRadiusFill))) return rc;
-  // grouped operand rows: candidates to training rows (rows are re-sorted
-  // by index after the compaction)
+  // grouped operand rows: candidates to training rows; rows are re-sorted by
+  // index after the compaction when their lists are out of index order
+  // (grouped rows, or several lists per row, whose columns interleave)
   const bool grouped = tc && ix.xperm;
   if (grouped) launch_translate_cols(sa.rcols, ncand, ix.xperm, status, st);
+  const bool unordered = grouped || S_lists > S;
 
   RadiusPlanArgs ra{};
   ra.X = ix.X;
@@ -1001,7 +1006,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   ra.d = ix.d;
   ra.m = m;
   ra.m_pad = m_pad;
-  ra.S = S;
+  ra.S = S_lists;
   ra.roff = roff;
   ra.rcount = sa.rcount;
   ra.cols = sa.rcols;
@@ -1041,7 +1046,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   }
   launch_compact(ra, indptr, indices, dist, st);
   B2K_CUDA(cudaGetLastError());
-  if ((sort_results || grouped) && nnz > 1) {
+  if ((sort_results || unordered) && nnz > 1) {
     // (distance, index) order when asked for, else ascending training index
     // (grouped operand rows list candidates out of index order)
     const bool by_dist = sort_results;

@@ -138,6 +138,7 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
                      const SinkArgs& sa, int* status, cudaStream_t st,
                      const int* perm = nullptr, int* unit_counter = nullptr, bool tf32 = false);
 int tc_column_groups(int k);
+int tc_radius_groups();  // candidate lists per (split, row) of the tcgen05 radius screens
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
 // noalloc: one scanner per row (half the list memory of the default two)
 void launch_screen_simt(const Index* ix, const float* Q, int64_t m, int64_t m_pad,

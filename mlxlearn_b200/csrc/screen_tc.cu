@@ -645,6 +645,10 @@ static int tc_knn_ew(int k) {
   return ew;
 }
 int tc_column_groups(int k) { return tc_knn_ew(k) / 4; }
+// Radius screens: four epilogue warps per TMEM lane group, one list per
+// (split, column group, row).
+constexpr int kRadiusEW = 16;
+int tc_radius_groups() { return kRadiusEW / 4; }
 bool tc_lazy_sink(int k) { return k > 16; }
 
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
@@ -696,8 +700,8 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
 #define B2K_TC_LAUNCH(SINK, EW)                                                \
   (a_stream ? launch_tc_variant<SINK, true, EW, false>(maps, p, KB, grid, st) \
             : launch_tc_variant<SINK, false, EW, false>(maps, p, KB, grid, st))
-  if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, 4);
-  if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, 4);
+  if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, kRadiusEW);
+  if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, kRadiusEW);
   if (tc_knn_ew(sa.k) == 16) {
     if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 16);
     if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 16);
