@@ -322,6 +322,9 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       TcUnit x;
       while (cur.next(p, x)) {
         const int KB = x.pr->KB;
+        // TMA coordinates count elements of the map's type: a 128-byte block
+        // is 64 bf16 or 32 fp32 columns
+        constexpr int kx = TF32 ? kTcBKf : kTcBK;
         const int g = G == 1 ? 0 : x.pr->group;
         const int a_row = x.pr->a_row0 + x.t * kTcBM;
         const int b_row0 = x.pr->b_row0;
@@ -334,7 +337,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
           ++a_loads;
           mbar_arrive_expect_tx(a_full, KB * kATileBytes);
           for (int kb = 0; kb < KB; ++kb)
-            tma_load_2d(a_smem + kb * kATileBytes, tmA, a_full, kb * kTcBK, a_row);
+            tma_load_2d(a_smem + kb * kATileBytes, tmA, a_full, kb * kx, a_row);
         }
         for (int j = x.j0; j < x.j1; ++j) {
           const int b_row = b_row0 + j * kTcBN;
@@ -347,8 +350,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
             const bool last = kb == KB - 1;
             mbar_arrive_expect_tx(&full[stage], (A_STREAM ? kATileBytes : 0) + kBTileBytes +
                                                     (last ? kBAugBytes : 0));
-            if (A_STREAM) tma_load_2d(st, tmA, &full[stage], kb * kTcBK, a_row);
-            tma_load_2d(st + b_off, tmB, &full[stage], kb * kTcBK, b_row);
+            if (A_STREAM) tma_load_2d(st, tmA, &full[stage], kb * kx, a_row);
+            tma_load_2d(st + b_off, tmB, &full[stage], kb * kx, b_row);
             if (last) tma_load_2d(st + baug_off, tmBaug, &full[stage], 0, b_row);
             if (++stage == (uint32_t)nst) {
               stage = 0;

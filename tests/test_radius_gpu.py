@@ -124,13 +124,13 @@ def test_radius_row_grouping_both_ways(group, monkeypatch):
     X, _ = mixture(np.random.default_rng(19), 24000, C, 1.0)
     Q, _ = mixture(np.random.default_rng(20), 400, C, 1.0)
     index = make_index(X)
-    for r, sort in ((5.0, False), (5.0, True), (9.0, False), (9.0, True)):
+    for r, sort in ((5.0, False), (5.0, True), (12.0, False), (12.0, True)):
         op, oix, od = oracle.radius(X, Q, r, sort_results=sort)
         ip, ix, dd = csr(index.query_radius_csr(Q, r, sort_results=sort))
         np.testing.assert_array_equal(ip, op)
         np.testing.assert_array_equal(ix, oix)
         np.testing.assert_array_equal(dd, od)
-    assert np.diff(op).max() > 4096  # the r = 9 rows exceed the shared-memory sort
+    assert np.diff(op).max() > 4096  # the r = 12 rows exceed the shared-memory sort
     ip, ix, dd = csr(index.query_radius_csr(Q, 5.0, need_distance=False))
     op, oix, _ = oracle.radius(X, Q, 5.0)
     np.testing.assert_array_equal(ip, op)
