@@ -960,7 +960,7 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="profiling driver: only the device steps of the headline workload "
                          "(or of --workload batch)")
-    ap.add_argument("--mode", default="bf16", choices=["bf16", "fp32", "exact", "auto"],
+    ap.add_argument("--mode", default="bf16", choices=["bf16", "tf32", "fp32", "exact", "auto"],
                     help="screen form for --profile")
     ap.add_argument("--k", type=int, default=K, help="neighbours for --profile")
     ap.add_argument("--problems", type=int, default=256,

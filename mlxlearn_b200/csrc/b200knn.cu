@@ -255,6 +255,7 @@ static int make_row_groups(Index& ix) {
   std::vector<int64_t> start((size_t)P + 1, 0);
   for (int64_t r = 0; r < ix.n; ++r) ++start[(size_t)hkey[(size_t)r] + 1];
   for (int p = 0; p < P; ++p) start[(size_t)p + 1] += start[(size_t)p];
+  std::vector<int> gstart(start.begin(), start.end());  // before the scatter advances them
   std::vector<int> perm((size_t)ix.n), inv((size_t)ix.n);
   for (int64_t r = 0; r < ix.n; ++r) {
     const int64_t pos = start[(size_t)hkey[(size_t)r]]++;
@@ -266,6 +267,9 @@ static int make_row_groups(Index& ix) {
   B2K_CUDA(cudaMemcpyAsync(ix.xperm, perm.data(), (size_t)ix.n * sizeof(int),
                            cudaMemcpyHostToDevice, st));
   B2K_CUDA(cudaMemcpyAsync(ix.xinv, inv.data(), (size_t)ix.n * sizeof(int),
+                           cudaMemcpyHostToDevice, st));
+  B2K_CUDA(cudaMalloc(&ix.group_start, gstart.size() * sizeof(int)));
+  B2K_CUDA(cudaMemcpyAsync(ix.group_start, gstart.data(), gstart.size() * sizeof(int),
                            cudaMemcpyHostToDevice, st));
   B2K_CUDA(cudaStreamSynchronize(st));
   return B2K_OK;
@@ -352,13 +356,24 @@ static bool reorder_enabled() {
   return !(e && e[0] == '0');
 }
 
+// Seeding pass over each query tile's home window (grouped rows): on unless
+// B2K_SEED=0 (tests run both ways).
+constexpr int kSeedTiles = 16;
+static bool seed_enabled() {
+  const char* e = getenv("B2K_SEED");
+  return !(e && e[0] == '0');
+}
+
 // Reference splits: fill the GPU with (query tile, split) work units while
-// keeping the number of candidate lists per query small.
+// keeping the number of candidate lists per query small.  Up to 64 splits, so
+// a batch of one or two query tiles (a small call, or the second pass over a
+// few uncertified rows) still spreads over most of the SMs.
+constexpr int kMaxSplits = 64;
 static int choose_splits(int64_t m_tiles, int64_t n_tiles, int64_t slots) {
   if (m_tiles <= 0 || n_tiles <= 0) return 1;
   int best = 1;
   double best_cost = 1e300;
-  for (int S = 1; S <= 16 && S <= n_tiles; ++S) {
+  for (int S = 1; S <= kMaxSplits && S <= n_tiles; ++S) {
     const double units = (double)m_tiles * S;
     const double waves = std::ceil(units / (double)slots);
     // time ~ waves * (n_tiles / S); small penalty per extra split (more list traffic)
@@ -469,9 +484,10 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     // Group nearby queries (reorder.cu); results go back to the original rows.
     const int* perm = ext_perm;
     const float* Qs = dQ;
+    int* key = nullptr;  // nearest pivot of each query (query grouping)
     if (!ext_perm && m >= 2048 && reorder_enabled()) {
       if ((rc = ensure_pivots(ix))) return rc;
-      int *key = nullptr, *hist = nullptr, *pm = nullptr;
+      int *hist = nullptr, *pm = nullptr;
       float* Qp = nullptr;
       if ((rc = dalloc(&key, (size_t)m, st))) return rc;
       fr.keep(key);
@@ -531,6 +547,40 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
                : tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK,
                                     kTcBM);
       if (!map_ok) return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
+      // Seeding: with grouped rows, a query's neighbours sit in the few
+      // reference tiles of its pivot's group, which the main screen may
+      // reach late; until then its lists would admit the band around the
+      // nearest other clusters.  A first pass over each query tile's home
+      // window publishes k-th screen values (its sink keeps no list:
+      // capacity 0) to the per-query words the main screen's lists start
+      // from.  A published value is the k-th smallest of real screen values
+      // of the query, so it is >= the final V_k and the certificate holds.
+      const int64_t m_tiles = m_pad / kTcBM;
+      if (key && ix.group_start && !tc_lazy_sink(k) && n_tiles >= 2 * kSeedTiles &&
+          seed_enabled()) {
+        const int G = tc_column_groups(k);
+        int* home = nullptr;
+        int* seed_counts = nullptr;
+        float* seed_kth = nullptr;
+        if ((rc = dalloc(&home, (size_t)m_tiles, st))) return rc;
+        fr.keep(home);
+        if ((rc = dalloc(&seed_counts, (size_t)G * m_pad, st))) return rc;
+        fr.keep(seed_counts);
+        if ((rc = dalloc(&seed_kth, (size_t)G * m_pad * k, st))) return rc;
+        fr.keep(seed_kth);
+        launch_home_tiles(perm, key, m, ix.group_start, (int)n_tiles, kSeedTiles, home,
+                          (int)m_tiles, st);
+        SinkArgs sb = sa;
+        sb.out.cap = 0;  // the trackers only: no list entry is written
+        sb.out.counts = seed_counts;
+        sb.out.kth = seed_kth;
+        // status[7] (zeroed above) counts this pass's claimed units
+        int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, 1, qp.E,
+                                  kSinkKnn, sb, status, st, perm, status + 7, tf32, home,
+                                  kSeedTiles);
+        if (lr) return fail(B2K_ECUDA, "tcgen05 seeding screen launch failed: %s",
+                            cudaGetErrorString((cudaError_t)lr));
+      }
       // status[6] (zeroed above) counts the claimed work units
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
                                 kSinkKnn, sa, status, st, perm, status + 6, tf32);
@@ -817,6 +867,7 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.aug_ones);
   cudaFree(ix.xperm);
   cudaFree(ix.xinv);
+  cudaFree(ix.group_start);
   cudaFree(ix.Xt);
   cudaFree(ix.Xtaug);
   cudaFree(ix.taug_ones);

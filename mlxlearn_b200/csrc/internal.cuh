@@ -75,6 +75,7 @@ struct Index {
   // query tile's candidates fall in few reference tiles.  Null: identity.
   int* xperm = nullptr;          // [n] operand row -> training row
   int* xinv = nullptr;           // [n] training row -> operand row
+  int* group_start = nullptr;    // [n_pivots + 1] first operand row of each pivot's group
   // pivots for query ordering (reorder.cu)
   int n_pivots = 0;
   float* pivots = nullptr;       // [n_pivots, d] centred rows
@@ -132,11 +133,14 @@ void launch_prep_queries_batch(const PrepProblem* tab, const int64_t* row_start,
 // ---------------------------------------------------------- screen kernels
 constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
 struct SinkArgs;
-// tf32: the kind::tf32 form over the index's tf32 operand (kNN sinks only)
+// tf32: the kind::tf32 form over the index's tf32 operand (kNN sinks only).
+// home (with S = 1): query tile t scans only reference tiles
+// [home[t], home[t] + home_tiles) -- the seeding pass of grouped rows.
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st,
-                     const int* perm = nullptr, int* unit_counter = nullptr, bool tf32 = false);
+                     const int* perm = nullptr, int* unit_counter = nullptr, bool tf32 = false,
+                     const int* home = nullptr, int home_tiles = 0);
 int tc_column_groups(int k);
 int tc_radius_groups();  // candidate lists per (split, row) of the tcgen05 radius screens
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
@@ -158,6 +162,12 @@ void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, in
 // hist[p] = rows per pivot
 void launch_assign_rows(const Index* ix, const float* X, int64_t n, int* key, int* hist,
                         cudaStream_t st);
+// home[t] = first reference tile of query tile t's window of `window` tiles:
+// the tiles holding the grouped rows of the pivot nearest to the tile's
+// middle query (perm, key: the query order and pivot keys of
+// launch_query_order)
+void launch_home_tiles(const int* perm, const int* key, int64_t m, const int* group_start,
+                       int n_tiles, int window, int* home, int m_tiles, cudaStream_t st);
 
 // second pass over uncertified rows: Qout[i] = Qs[rows[i]], pout[i] = perm[rows[i]]
 void launch_gather_fallback(const float* Qs, int d, const int* rows, const int* perm, int count,

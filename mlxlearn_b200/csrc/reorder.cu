@@ -144,7 +144,27 @@ __global__ void gather_fallback_kernel(const float* __restrict__ Qs, int d,
   if ((threadIdx.x & 31) == 0) pout[i] = perm ? perm[r] : r;
 }
 
+__global__ void home_tiles_kernel(const int* __restrict__ perm, const int* __restrict__ key,
+                                  int64_t m, const int* __restrict__ group_start, int n_tiles,
+                                  int window, int* __restrict__ home, int m_tiles) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m_tiles) return;
+  const int64_t mid = min((int64_t)t * kTcBM + kTcBM / 2, m - 1);
+  const int row = group_start[key[perm[mid]]];
+  // one tile of margin before the group; the window stays inside the index
+  int j0 = row / kTcBN - 1;
+  j0 = min(j0, n_tiles - window);
+  home[t] = max(j0, 0);
+}
+
 }  // namespace
+
+void launch_home_tiles(const int* perm, const int* key, int64_t m, const int* group_start,
+                       int n_tiles, int window, int* home, int m_tiles, cudaStream_t st) {
+  if (m_tiles <= 0 || m <= 0) return;
+  home_tiles_kernel<<<(unsigned)((m_tiles + 127) / 128), 128, 0, st>>>(
+      perm, key, m, group_start, n_tiles, window, home, m_tiles);
+}
 
 void launch_gather_fallback(const float* Qs, int d, const int* rows, const int* perm, int count,
                             float* Qout, int* pout, cudaStream_t st) {

@@ -76,6 +76,7 @@ struct TcParams {
   const int* cta_begin;      // batched: CTA b runs items [cta_begin[b], cta_begin[b + 1])
   int* status;
   int* unit_counter;         // units claimed dynamically (or null: round-robin / per-CTA lists)
+  const int* home;           // single problem, seeding pass: tile t's window starts at home[t]
   int n_items;               // batched, claimed: items in the list
   TcProblem one;             // single problem
 };
@@ -177,7 +178,7 @@ struct UnitCursor {
       const int s = w / p.m_tiles;
       x.pr = &p.one;
       x.t = w % p.m_tiles;
-      x.j0 = s * p.one.tiles_per_split;
+      x.j0 = p.home ? p.home[x.t] : s * p.one.tiles_per_split;
       x.j1 = min(x.j0 + p.one.tiles_per_split, p.one.n_tiles);
       x.slot = s;
     }
@@ -657,15 +658,17 @@ bool tc_lazy_sink(int k) { return k > 16; }
 int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
                      int exclude_self, int64_t q_offset, int S, const float* E, int sink_kind,
                      const SinkArgs& sa, int* status, cudaStream_t st, const int* perm,
-                     int* unit_counter, bool tf32) {
+                     int* unit_counter, bool tf32, const int* home, int home_tiles) {
   if (tf32 && sink_kind != kSinkKnn) return (int)cudaErrorInvalidValue;
+  if (home && (S != 1 || home_tiles <= 0)) return (int)cudaErrorInvalidValue;
   TcParams p{};
   p.unit_counter = unit_counter;
+  p.home = home;
   TcProblem& one = p.one;
   one.m = (int)m;
   one.KB = tf32 ? ix->dpt / kTcBKf : ix->dp / kTcBK;
   one.n_tiles = (int)(ix->n_pad_tc / kTcBN);
-  one.tiles_per_split = (one.n_tiles + S - 1) / S;
+  one.tiles_per_split = home ? home_tiles : (one.n_tiles + S - 1) / S;
   one.exclude_self = exclude_self;
   one.q_offset = q_offset;
   one.E = E;

@@ -329,15 +329,18 @@ def test_k_across_the_screen_limit(k, rng):
 
 
 @pytest.mark.parametrize("mode", ["bf16", "tf32"])
-@pytest.mark.parametrize("group", ["0", "1"])
-def test_row_grouping_both_ways(group, mode, monkeypatch):
+@pytest.mark.parametrize("group,seed", [("0", "1"), ("1", "0"), ("1", "1")])
+def test_row_grouping_both_ways(group, seed, mode, monkeypatch):
     """The bf16 operand's rows are grouped by nearest pivot (the screen's
     lists hold operand rows, certify maps them back to training rows, a
-    self-query excludes its row's operand column); both layouts give the
-    oracle's answer, ties between duplicated rows included."""
+    self-query excludes its row's operand column), and a seeding pass over
+    each query tile's home window starts the lists from published k-th
+    values; every combination gives the oracle's answer, ties between
+    duplicated rows and self-queries included."""
     import torch
 
     monkeypatch.setenv("B2K_GROUP_ROWS", group)
+    monkeypatch.setenv("B2K_SEED", seed)
     C = np.random.default_rng(15).uniform(-1, 1, (128, 48))
     X, _ = mixture(np.random.default_rng(16), 30000, C, 0.1)
     X[20000:20060] = X[:60]  # exact duplicates: ties resolved by training index
