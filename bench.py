@@ -51,9 +51,11 @@ sys.path.insert(0, os.path.join(REPO, "tests"))
 METRIC = ("exact kNN queries/s at 1M×128 k=10: BF16-screen+certified vs FP32; % TC peak")
 N_REF, N_QUERY, D, K = 1_000_000, 100_000, 128, 10
 WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
-# Our kernels per kNN call: assign, bin_scan, scatter, gather (query grouping),
-# prep_queries, screen_tc, certify, exact (fallback rows; no-op when none).
-LAUNCHES_PER_STEP = 8
+# Our kernels per kNN call (the ncu launch list of this workload): nonfinite
+# check; assign, bin_scan, scatter, gather (query grouping); prep_queries;
+# home_tiles and the seeding screen; the main screen; certify.  No exhaustive
+# or second-pass launch when every row certifies.
+LAUNCHES_PER_STEP = 10
 # DRAM bytes (read + write) of one screen launch at the headline size, from the
 # ncu capture summarised in profiles/screen_tc_knn_gauss1Mx128.txt (a 10k-query
 # capture scaled by the (query tile, reference tile) pairs)

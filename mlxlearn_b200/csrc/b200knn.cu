@@ -1028,8 +1028,11 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
     return B2K_OK;
   };
   if ((rc = screen(kSinkRadiusCount))) return rc;
+  int64_t* scan_scratch = nullptr;  // multi-block scans (count offsets, then indptr)
+  if ((rc = dalloc(&scan_scratch, (size_t)scan_scratch_len(m), st))) return rc;
+  fr.keep(scan_scratch);
   launch_scan_split_counts(sa.rcount, S_lists, m, m_pad, roff, roff + (size_t)S_lists * m_pad,
-                           st);
+                           scan_scratch, st);
   int64_t ncand = 0;
   int hstatus[8];
   B2K_CUDA(cudaMemcpyAsync(&ncand, roff + (size_t)S_lists * m_pad, sizeof(int64_t),
@@ -1071,7 +1074,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   launch_classify(ra, st);
   int64_t* indptr = nullptr;
   if ((rc = dalloc(&indptr, (size_t)m + 1, st))) return rc;
-  launch_scan_rows(ra.mcount, m, indptr, st);
+  launch_scan_rows(ra.mcount, m, indptr, scan_scratch, st);
   B2K_CUDA(cudaGetLastError());
   int64_t nnz = 0;
   unsigned long long hc[2];
@@ -1101,12 +1104,16 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
     // (distance, index) order when asked for, else ascending training index
     // (grouped operand rows list candidates out of index order)
     const bool by_dist = sort_results;
-    int* big = nullptr;
-    if ((rc = dalloc(&big, (size_t)m + 1, st))) return rc;
-    fr.keep(big);
+    // row lists for the longer rows: [m] rows + count, twice
+    int* lists = nullptr;
+    if ((rc = dalloc(&lists, 2 * (size_t)m + 2, st))) return rc;
+    fr.keep(lists);
+    int* mid = lists;
+    int* big = lists + m + 1;
+    B2K_CUDA(cudaMemsetAsync(mid + m, 0, sizeof(int), st));
     B2K_CUDA(cudaMemsetAsync(big + m, 0, sizeof(int), st));
-    launch_sort_rows(indptr, m, indices, dist, big, big + m, std::min<int64_t>(m, 4 * sms), st,
-                     by_dist);
+    launch_sort_rows(indptr, m, indices, dist, mid, mid + m, big, big + m,
+                     (int)std::min<int64_t>(m, 4 * sms), st, by_dist);
     int nbig = 0;
     B2K_CUDA(cudaMemcpyAsync(&nbig, big + m, sizeof(int), cudaMemcpyDeviceToHost, st));
     B2K_CUDA(cudaStreamSynchronize(st));

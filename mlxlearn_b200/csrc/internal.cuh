@@ -245,17 +245,21 @@ struct RadiusPlanArgs {
 };
 void launch_radius_threshold(const double* nq, const float* E, int64_t m, int64_t m_pad,
                              double R2, float* thr, cudaStream_t st);
+// Multi-block scans; `scratch` holds scan_scratch_len(m) int64 values.
+int64_t scan_scratch_len(int64_t m);
 void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad, int64_t* off,
-                              int64_t* total, cudaStream_t st);
-void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, cudaStream_t st);
+                              int64_t* total, int64_t* scratch, cudaStream_t st);
+void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, int64_t* scratch,
+                      cudaStream_t st);
 void launch_classify(const RadiusPlanArgs& r, cudaStream_t st);
 void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* indices,
                     double* dist, cudaStream_t st);
 // Per-row sort by (distance, index), or by index alone when !by_dist (dist,
 // if not null, then moves with its index).
+// mid_rows/big_rows: scratch lists of m rows each, their counts zeroed.
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
-                      int* big_rows, int* big_count, int grid, cudaStream_t st,
-                      bool by_dist = true);
+                      int* mid_rows, int* mid_count, int* big_rows, int* big_count, int grid,
+                      cudaStream_t st, bool by_dist = true);
 void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
                           double* dist, double* tmp_d, int64_t* tmp_i, int64_t tmp_stride,
                           int grid, cudaStream_t st, bool by_dist = true);

@@ -19,6 +19,7 @@
 // training index after step 4 when no distance order is asked for.
 // Replaces the reference's Metal screen + host finisher
 // (src/mlxlearn/_kernels/radius_metal_v1.py:257-611, src/mlxlearn_device/_radius.py:54-330).
+#include <algorithm>
 #include <cfloat>
 
 #include "common.cuh"
@@ -47,63 +48,108 @@ __global__ void radius_threshold_kernel(const double* __restrict__ nq, const flo
   thr[r] = __double2float_ru(t);
 }
 
-// Exclusive scan of per-(split, row) counts in row-major (row, split) order.
-// One CTA; each thread owns a contiguous block of rows.
-__global__ void scan_split_counts_kernel(const int* __restrict__ counts, int S, int64_t m,
-                                         int64_t m_pad, int64_t* __restrict__ off,
-                                         int64_t* __restrict__ total) {
-  __shared__ int64_t part[1024];
-  const int t = threadIdx.x;
-  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
-  const int64_t r0 = min(m, (int64_t)t * per), r1 = min(m, r0 + per);
-  int64_t sum = 0;
-  for (int64_t r = r0; r < r1; ++r)
-    for (int s = 0; s < S; ++s) sum += counts[(size_t)s * m_pad + r];
-  part[t] = sum;
-  __syncthreads();
-  if (t == 0) {
-    int64_t acc = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      const int64_t v = part[i];
-      part[i] = acc;
-      acc += v;
-    }
-    *total = acc;
+// Multi-block exclusive scan of int64 values (the radius path's offsets):
+// each block scans a tile of kScanTile values (four per thread, warp
+// shuffles, then the warp totals), writes the tile-local scan and the tile's
+// total; one block scans the tile totals; a last pass adds each tile's base.
+constexpr int kScanThreads = 1024;
+constexpr int kScanTile = 4 * kScanThreads;
+
+__device__ __forceinline__ int64_t warp_incl_scan(int64_t v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
   }
-  __syncthreads();
-  int64_t acc = part[t];
-  for (int64_t r = r0; r < r1; ++r)
-    for (int s = 0; s < S; ++s) {
-      off[(size_t)s * m_pad + r] = acc;
-      acc += counts[(size_t)s * m_pad + r];
-    }
+  return v;
 }
 
-// Exclusive scan of per-row counts into indptr[m+1].
-__global__ void scan_rows_kernel(const int64_t* __restrict__ counts, int64_t m,
-                                 int64_t* __restrict__ indptr) {
-  __shared__ int64_t part[1024];
-  const int t = threadIdx.x;
-  const int64_t per = (m + blockDim.x - 1) / blockDim.x;
-  const int64_t r0 = min(m, (int64_t)t * per), r1 = min(m, r0 + per);
-  int64_t sum = 0;
-  for (int64_t r = r0; r < r1; ++r) sum += counts[r];
-  part[t] = sum;
+// Exclusive scan of the block's kScanThreads values `v` (returned), the
+// block total in *total_out (all threads).
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* warp_sums,
+                                                   int64_t* total_out) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t incl = warp_incl_scan(v, lane);
+  if (lane == 31) warp_sums[w] = incl;
   __syncthreads();
-  if (t == 0) {
-    int64_t acc = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      const int64_t v = part[i];
-      part[i] = acc;
-      acc += v;
-    }
-    indptr[m] = acc;
+  if (w == 0) {
+    const int64_t ws = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+    const int64_t wi = warp_incl_scan(ws, lane);
+    warp_sums[lane] = wi - ws;  // exclusive
+    if (lane == 31) warp_sums[32] = wi;
   }
   __syncthreads();
-  int64_t acc = part[t];
-  for (int64_t r = r0; r < r1; ++r) {
-    indptr[r] = acc;
-    acc += counts[r];
+  const int64_t r = warp_sums[w] + incl - v;
+  *total_out = warp_sums[32];
+  __syncthreads();
+  return r;
+}
+
+// Tile-local exclusive scan of in[0..n) into out, tile totals into part.
+__global__ void __launch_bounds__(kScanThreads)
+    scan_tiles_kernel(const int64_t* __restrict__ in, int64_t n, int64_t* __restrict__ out,
+                      int64_t* __restrict__ part) {
+  __shared__ int64_t warp_sums[33];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + 4 * (int64_t)threadIdx.x;
+  int64_t x[4], sum = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    x[j] = base + j < n ? in[base + j] : 0;
+    sum += x[j];
+  }
+  int64_t tile_total;
+  int64_t acc = block_excl_scan(sum, warp_sums, &tile_total);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (base + j < n) out[base + j] = acc;
+    acc += x[j];
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = tile_total;
+}
+
+// Exclusive scan of the nt tile totals in place (one block, any nt); the
+// grand total into *total.
+__global__ void __launch_bounds__(kScanThreads)
+    scan_parts_kernel(int64_t* __restrict__ part, int64_t nt, int64_t* __restrict__ total) {
+  __shared__ int64_t warp_sums[33];
+  int64_t carry = 0;
+  for (int64_t b0 = 0; b0 < nt; b0 += kScanThreads) {
+    const int64_t i = b0 + threadIdx.x;
+    const int64_t v = i < nt ? part[i] : 0;
+    int64_t chunk;
+    const int64_t e = block_excl_scan(v, warp_sums, &chunk);
+    if (i < nt) part[i] = carry + e;
+    carry += chunk;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_add_kernel(int64_t* __restrict__ out, int64_t n, const int64_t* __restrict__ part) {
+  const int64_t i = (int64_t)blockIdx.x * kScanThreads + threadIdx.x;
+  if (i < n) out[i] += part[i / kScanTile];
+}
+
+// Per row: the total over its lists (a coalesced pass over rows).
+__global__ void row_totals_kernel(const int* __restrict__ counts, int S, int64_t m,
+                                  int64_t m_pad, int64_t* __restrict__ tot) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  int64_t sum = 0;
+  for (int s = 0; s < S; ++s) sum += counts[(size_t)s * m_pad + r];
+  tot[r] = sum;
+}
+
+// Per (list, row) offsets in row-major (row, list) order from the row offsets.
+__global__ void split_offsets_kernel(const int* __restrict__ counts, int S, int64_t m,
+                                     int64_t m_pad, const int64_t* __restrict__ row_off,
+                                     int64_t* __restrict__ off) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  int64_t acc = row_off[r];
+  for (int s = 0; s < S; ++s) {
+    off[(size_t)s * m_pad + r] = acc;
+    acc += counts[(size_t)s * m_pad + r];
   }
 }
 
@@ -233,21 +279,77 @@ __device__ __forceinline__ bool sort_after(double x, int64_t xi, double y, int64
   return xi > yi;
 }
 
-// Per-row sort, one CTA per row, rows of at most kRadiusSortCap; `dist` may
-// be null for an index sort.
+// Per-row sorts; `dist` may be null for an index sort.  Rows of at most
+// kWarpSortCap entries: one warp each, bitonic in the warp's shared memory;
+// longer rows go to a list for one CTA each (at most kRadiusSortCap entries),
+// and longer still to the global-memory sort.
+constexpr int kWarpSortCap = 256;
+constexpr int kWarpSortWarps = 8;
 constexpr int kRadiusSortCap = 4096;
 constexpr int kSortThreads = 512;
 
 template <bool BY_DIST>
-__global__ void sort_rows_kernel(const int64_t* __restrict__ indptr, int64_t m,
+__global__ void __launch_bounds__(kWarpSortWarps * 32)
+    sort_rows_warp_kernel(const int64_t* __restrict__ indptr, int64_t m,
+                          int64_t* __restrict__ indices, double* __restrict__ dist,
+                          int* __restrict__ mid_rows, int* __restrict__ mid_count) {
+  __shared__ double sd_all[kWarpSortWarps][kWarpSortCap];
+  __shared__ int64_t si_all[kWarpSortWarps][kWarpSortCap];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sd = sd_all[w];
+  int64_t* si = si_all[w];
+  const int64_t warps = (int64_t)gridDim.x * kWarpSortWarps;
+  for (int64_t row = (int64_t)blockIdx.x * kWarpSortWarps + w; row < m; row += warps) {
+    const int64_t a0 = indptr[row], len = indptr[row + 1] - a0;
+    if (len <= 1) continue;
+    if (len > kWarpSortCap) {
+      if (lane == 0) mid_rows[atomicAdd(mid_count, 1)] = (int)row;
+      continue;
+    }
+    int P = 2;
+    while (P < len) P <<= 1;
+    for (int i = lane; i < P; i += 32) {
+      sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
+      si[i] = i < len ? indices[a0 + i] : INT64_MAX;
+    }
+    __syncwarp();
+    for (int size = 2; size <= P; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = lane; t < P / 2; t += 32) {
+          const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+          const bool up = (i & size) == 0;
+          const double x = sd[i], y = sd[j];
+          const int64_t xi = si[i], yi = si[j];
+          if (sort_after<BY_DIST>(x, xi, y, yi) == up) {
+            sd[i] = y;
+            sd[j] = x;
+            si[i] = yi;
+            si[j] = xi;
+          }
+        }
+        __syncwarp();
+      }
+    for (int i = lane; i < len; i += 32) {
+      if (dist) dist[a0 + i] = sd[i];
+      indices[a0 + i] = si[i];
+    }
+    __syncwarp();
+  }
+}
+
+// Rows listed by the warp sort: one CTA per row.
+template <bool BY_DIST>
+__global__ void sort_rows_kernel(const int64_t* __restrict__ indptr,
+                                 const int* __restrict__ rows, const int* __restrict__ row_count,
                                  int64_t* __restrict__ indices, double* __restrict__ dist,
                                  int* __restrict__ big_rows, int* __restrict__ big_count) {
   extern __shared__ uint8_t smem[];
   double* sd = reinterpret_cast<double*>(smem);
   int64_t* si = reinterpret_cast<int64_t*>(sd + kRadiusSortCap);
-  for (int64_t row = blockIdx.x; row < m; row += gridDim.x) {
+  const int count = *row_count;
+  for (int it = blockIdx.x; it < count; it += gridDim.x) {
+    const int64_t row = rows[it];
     const int64_t a0 = indptr[row], len = indptr[row + 1] - a0;
-    if (len <= 1) continue;
     if (len > kRadiusSortCap) {
       if (threadIdx.x == 0) big_rows[atomicAdd(big_count, 1)] = (int)row;
       continue;
@@ -340,13 +442,40 @@ void launch_radius_threshold(const double* nq, const float* E, int64_t m, int64_
                                                                             thr);
 }
 
-void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad, int64_t* off,
-                              int64_t* total, cudaStream_t st) {
-  scan_split_counts_kernel<<<1, 1024, 0, st>>>(counts, S, m, m_pad, off, total);
+int64_t scan_scratch_len(int64_t n) { return 2 * n + (n + kScanTile - 1) / kScanTile + 2; }
+
+void launch_exclusive_scan(const int64_t* in, int64_t n, int64_t* out, int64_t* total,
+                           int64_t* part, cudaStream_t st) {
+  if (n <= 0) {
+    cudaMemsetAsync(total, 0, sizeof(int64_t), st);
+    return;
+  }
+  const int64_t nt = (n + kScanTile - 1) / kScanTile;
+  scan_tiles_kernel<<<(unsigned)nt, kScanThreads, 0, st>>>(in, n, out, part);
+  scan_parts_kernel<<<1, kScanThreads, 0, st>>>(part, nt, total);
+  if (nt > 1)
+    scan_add_kernel<<<(unsigned)((n + kScanThreads - 1) / kScanThreads), kScanThreads, 0, st>>>(
+        out, n, part);
 }
 
-void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, cudaStream_t st) {
-  scan_rows_kernel<<<1, 1024, 0, st>>>(counts, m, indptr);
+void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad, int64_t* off,
+                              int64_t* total, int64_t* scratch, cudaStream_t st) {
+  if (m <= 0) {
+    cudaMemsetAsync(total, 0, sizeof(int64_t), st);
+    return;
+  }
+  int64_t* tot = scratch;           // [m] row totals
+  int64_t* row_off = scratch + m;   // [m] row offsets
+  int64_t* part = scratch + 2 * m;  // tile totals
+  const unsigned blocks = (unsigned)((m + 255) / 256);
+  row_totals_kernel<<<blocks, 256, 0, st>>>(counts, S, m, m_pad, tot);
+  launch_exclusive_scan(tot, m, row_off, total, part, st);
+  split_offsets_kernel<<<blocks, 256, 0, st>>>(counts, S, m, m_pad, row_off, off);
+}
+
+void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, int64_t* scratch,
+                      cudaStream_t st) {
+  launch_exclusive_scan(counts, m, indptr, indptr + m, scratch, st);
 }
 
 // Thresholds of the float64 band (radius_contract.py:129-153) and the exact
@@ -437,12 +566,23 @@ void launch_translate_cols(int* cols, int64_t count, const int* xperm, const int
 }
 
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,
-                      int* big_rows, int* big_count, int grid, cudaStream_t st, bool by_dist) {
+                      int* mid_rows, int* mid_count, int* big_rows, int* big_count, int grid,
+                      cudaStream_t st, bool by_dist) {
   if (m <= 0) return;
+  const unsigned wgrid = (unsigned)std::min<int64_t>((m + kWarpSortWarps - 1) / kWarpSortWarps,
+                                                     (int64_t)grid * 4);
+  if (by_dist)
+    sort_rows_warp_kernel<true><<<wgrid, kWarpSortWarps * 32, 0, st>>>(indptr, m, indices, dist,
+                                                                        mid_rows, mid_count);
+  else
+    sort_rows_warp_kernel<false><<<wgrid, kWarpSortWarps * 32, 0, st>>>(indptr, m, indices,
+                                                                         dist, mid_rows,
+                                                                         mid_count);
   const size_t smem = (size_t)kRadiusSortCap * (sizeof(double) + sizeof(int64_t));
   auto kern = by_dist ? sort_rows_kernel<true> : sort_rows_kernel<false>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<grid, kSortThreads, smem, st>>>(indptr, m, indices, dist, big_rows, big_count);
+  kern<<<grid, kSortThreads, smem, st>>>(indptr, mid_rows, mid_count, indices, dist, big_rows,
+                                         big_count);
 }
 
 void launch_sort_big_rows(const int64_t* indptr, const int* rows, int count, int64_t* indices,
