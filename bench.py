@@ -56,10 +56,10 @@ WORKLOAD = "knn_gauss_mixture_1Mx128_100kq_k10"
 # home_tiles and the seeding screen; the main screen; certify.  No exhaustive
 # or second-pass launch when every row certifies.
 LAUNCHES_PER_STEP = 10
-# DRAM bytes (read + write) of one screen launch at the headline size, from the
-# ncu capture summarised in profiles/screen_tc_knn_gauss1Mx128.txt (a 10k-query
-# capture scaled by the (query tile, reference tile) pairs)
-SCREEN_TRAFFIC_BYTES = 5.77e9
+# DRAM bytes (read + write) of one screen launch at the headline size: an ncu
+# capture of the full 100,000-query launch (dram__bytes_read/write, one pass),
+# summarised in profiles/screen_tc_knn_gauss1Mx128.txt
+SCREEN_TRAFFIC_BYTES = 5.84e9
 # FP32 CUDA-core rate (no measured figure): 148 SMs x 128 lanes x 2 FLOP x 1.965 GHz
 FP32_NOMINAL_TFLOPS = 74.4
 L2_FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
