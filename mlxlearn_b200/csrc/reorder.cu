@@ -44,27 +44,40 @@ __global__ void pivot_rows_kernel(const float* __restrict__ X, int64_t n, int d,
   if (threadIdx.x == 0) pnorm[p] = (float)s;
 }
 
-// One thread per query: argmin_p ||p||^2 - 2 <y_q, p>.
+// 128 queries per block: argmin_p ||p||^2 - 2 <y_q, p>.  Per 32-pivot tile
+// warp w takes pivots [8w, 8w + 8) and lane l the queries l, l + 32, l + 64,
+// l + 96, so each feature step is 6 shared-memory loads (4 query values, two
+// 16-byte pivot loads) for 32 FMAs.  Each (query, pivot) sum runs over the
+// features in order, and ties go to the smaller pivot, so the keys do not
+// depend on this layout.
 __global__ void __launch_bounds__(kAssignThreads)
     assign_kernel(const float* __restrict__ Q, int64_t m, int d, const float* __restrict__ center,
                   const float* __restrict__ piv, const float* __restrict__ pnorm, int P,
                   int* __restrict__ key, int* __restrict__ hist) {
-  __shared__ float sp[kPivTile][kDChunk + 1];
-  __shared__ float sq[kDChunk][kAssignThreads + 1];  // query tile, transposed
+  __shared__ __align__(16) float sp[kDChunk][kPivTile];  // pivot tile, transposed
+  __shared__ float sq[kDChunk][kAssignThreads + 1];       // query tile, transposed
+  __shared__ float red_v[4][kAssignThreads];
+  __shared__ int red_p[4][kAssignThreads];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t q0 = (int64_t)blockIdx.x * kAssignThreads;
-  const int64_t q = q0 + threadIdx.x;
-  const bool valid = q < m;
-  float best = INFINITY;
-  int best_p = 0;
-  for (int p0 = 0; p0 < P; p0 += kPivTile) {
-    float acc[kPivTile];
+  float best[4];
+  int best_p[4];
 #pragma unroll
-    for (int j = 0; j < kPivTile; ++j) acc[j] = 0.0f;
+  for (int i = 0; i < 4; ++i) {
+    best[i] = INFINITY;
+    best_p[i] = 0;
+  }
+  for (int p0 = 0; p0 < P; p0 += kPivTile) {
+    float acc[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
     for (int k0 = 0; k0 < d; k0 += kDChunk) {
       __syncthreads();
       for (int i = threadIdx.x; i < kPivTile * kDChunk; i += kAssignThreads) {
-        const int j = i / kDChunk, k = i % kDChunk;
-        sp[j][k] = (p0 + j < P && k0 + k < d) ? piv[(size_t)(p0 + j) * d + k0 + k] : 0.0f;
+        const int j = i % kPivTile, k = i / kPivTile;
+        sp[k][j] = (p0 + j < P && k0 + k < d) ? piv[(size_t)(p0 + j) * d + k0 + k] : 0.0f;
       }
       // coalesced: consecutive threads read consecutive features of one query
       for (int i = threadIdx.x; i < kAssignThreads * kDChunk; i += kAssignThreads) {
@@ -73,31 +86,56 @@ __global__ void __launch_bounds__(kAssignThreads)
         sq[k][r] = (qr < m && k0 + k < d) ? Q[qr * d + k0 + k] - center[k0 + k] : 0.0f;
       }
       __syncthreads();
-      if (valid) {
-        const int kend = min(kDChunk, d - k0);
-        for (int k = 0; k < kend; ++k) {
-          const float y = sq[k][threadIdx.x];
+      const int kend = min(kDChunk, d - k0);
+      for (int k = 0; k < kend; ++k) {
+        const float4 pa = *reinterpret_cast<const float4*>(&sp[k][8 * w]);
+        const float4 pb = *reinterpret_cast<const float4*>(&sp[k][8 * w + 4]);
+        const float pv[8] = {pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, pb.z, pb.w};
 #pragma unroll
-          for (int j = 0; j < kPivTile; ++j) acc[j] = fmaf(y, sp[j][k], acc[j]);
+        for (int i = 0; i < 4; ++i) {
+          const float y = sq[k][lane + 32 * i];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(y, pv[j], acc[i][j]);
         }
       }
     }
-    if (valid) {
 #pragma unroll
-      for (int j = 0; j < kPivTile; ++j) {
-        if (p0 + j < P) {
-          const float v = fmaf(-2.0f, acc[j], pnorm[p0 + j]);
-          if (v < best) {
-            best = v;
-            best_p = p0 + j;
+    for (int j = 0; j < 8; ++j) {
+      const int pj = p0 + 8 * w + j;
+      if (pj < P) {
+        const float pn = pnorm[pj];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float v = fmaf(-2.0f, acc[i][j], pn);
+          if (v < best[i]) {
+            best[i] = v;
+            best_p[i] = pj;
           }
         }
       }
     }
   }
-  if (valid) {
-    key[q] = best_p;
-    atomicAdd(hist + best_p, 1);
+  // each warp's best per query, then the smallest (value, pivot) over warps
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    red_v[w][lane + 32 * i] = best[i];
+    red_p[w][lane + 32 * i] = best_p[i];
+  }
+  __syncthreads();
+  const int64_t q = q0 + threadIdx.x;
+  if (q < m) {
+    float bv = red_v[0][threadIdx.x];
+    int bp = red_p[0][threadIdx.x];
+    for (int ww = 1; ww < 4; ++ww) {
+      const float v = red_v[ww][threadIdx.x];
+      const int pp = red_p[ww][threadIdx.x];
+      if (v < bv || (v == bv && pp < bp)) {
+        bv = v;
+        bp = pp;
+      }
+    }
+    key[q] = bp;
+    atomicAdd(hist + bp, 1);
   }
 }
 
