@@ -650,9 +650,9 @@ def sec_radius(args):
     tf_burst, _, hbm, peak_kind = peaks()
     nnz = int(ip[-1])
     lengths = np.diff(ip)
-    # HBM roofline of the whole call: the index streamed twice by the two
-    # screen passes (bf16) plus 16 B per returned neighbour, over the call time
-    moved = 2 * X.shape[0] * 64 + 16 * nnz
+    # HBM roofline of the whole call: the bf16 index streamed once by the
+    # single screen pass plus 16 B per returned neighbour, over the call time
+    moved = X.shape[0] * 64 + 16 * nnz
     line = {
         "metric": "radius neighbourhoods (CSR) queries/s, 200000 x 32; e2e = "
                   "RadiusNeighborsClassifier.predict",
@@ -661,8 +661,9 @@ def sec_radius(args):
         "config": {"workload": "radius_200000x32_50000q", "radius": r,
                    "median_neighbours": float(np.median(lengths)),
                    "zero_neighbour_queries": int((lengths == 0).sum()), "nnz": nnz,
-                   "value_note": "query_radius_csr through the host C ABI (upload, two "
-                                 "screen passes, exact classify, CSR download)"},
+                   "value_note": "query_radius_csr through the host C ABI (upload, one "
+                                 "screen pass into capped lists, exact classify, CSR "
+                                 "download)"},
         "roofline": {"kernel": "whole radius call", "bound": "tensor",
                      "achieved": 2.0 * X.shape[0] * X.shape[1] * len(Q) / csr_s / 1e12,
                      "peak": tf_burst, "unit": "TFLOP/s",

@@ -960,11 +960,31 @@ struct b2k_radius_result {
 
 namespace b2k {
 
-// One block of queries: screen (count + fill), classify, compact, sort.
-// Appends device CSR pieces to `res` (which then owns them).
+// Entries per list of the single-pass radius screen: B2K_RADIUS_CAP when set
+// (0 = the counted two-pass form), else what a 512 MB budget for the block's
+// lists allows (B2K_RADIUS_LIST_MB), a multiple of 32 in [64, 1024], or 0 when
+// that budget holds fewer than 64 per list.
+static int radius_list_cap(int S_lists, int64_t m_pad) {
+  if (const char* e = getenv("B2K_RADIUS_CAP")) {
+    const long c = atol(e);
+    return c <= 0 ? 0 : (int)std::min<long>(c, 1 << 20);
+  }
+  const char* mb = getenv("B2K_RADIUS_LIST_MB");
+  const int64_t budget = (int64_t)(mb ? atoll(mb) : 512) << 20;
+  int64_t c = budget / ((int64_t)S_lists * m_pad * (int64_t)sizeof(int)) / 32 * 32;
+  return c < 64 ? 0 : (int)std::min<int64_t>(c, 1024);
+}
+
+// One block of queries: screen, classify, compact, sort.  The tcgen05 screen
+// runs once into fixed-capacity lists; rows that overflow a list are answered
+// by a counted sub-call (count pass, then fill at scanned offsets) on those
+// rows alone, the form the CUDA-core screen always uses (`counted`).
+// qrows: the block row of each query for self-exclusion (sub-calls), or null.
+// Stores device CSR pieces in `res` (which then owns them).
 static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int exclude_self,
                         int64_t q_offset, bool need_distance, bool sort_results, bool admit_all,
-                        cudaStream_t st, b2k_radius_result* res) {
+                        cudaStream_t st, b2k_radius_result* res, const int* qrows = nullptr,
+                        bool counted = false, bool sort_rows = true) {
   StreamFree fr{st, {}};
   int rc;
   int mode = (!admit_all && ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16 : B2K_MODE_FP32;
@@ -977,6 +997,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   const int S = choose_splits(m_pad / bm, n_tiles, tc ? sms : 2 * sms);
   // candidate lists per row: one per (split, column group of the screen)
   const int S_lists = S * (tc ? tc_radius_groups() : simt_column_groups(kSinkRadiusCount));
+  const int cap = (tc && !counted) ? radius_list_cap(S_lists, m_pad) : 0;
 
   int* status = nullptr;
   if ((rc = dalloc(&status, 8, st))) return rc;
@@ -1006,28 +1027,38 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   SinkArgs sa{};
   sa.thr = thr;
   sa.m_pad = (int)m_pad;
+  sa.rcap = cap;
   if ((rc = dalloc(&sa.rcount, (size_t)S_lists * m_pad, st))) return rc;
   fr.keep(sa.rcount);
   int64_t* roff = nullptr;
   if ((rc = dalloc(&roff, (size_t)S_lists * m_pad + 1, st))) return rc;
   fr.keep(roff);
   sa.roff = roff;
+  int* ovf = nullptr;  // single pass: overflowed rows [m] + their count
+  if (cap) {
+    if ((rc = dalloc(&sa.rcols, (size_t)S_lists * m_pad * cap, st))) return rc;
+    fr.keep(sa.rcols);
+    if ((rc = dalloc(&ovf, (size_t)m + 1, st))) return rc;
+    fr.keep(ovf);
+    B2K_CUDA(cudaMemsetAsync(ovf + m, 0, sizeof(int), st));
+  }
   CUtensorMap tmap_a;
   if (tc && !tensor_map_2d_bf16(&tmap_a, qp.Ah, (uint64_t)ix.dp, (uint64_t)m_pad, kTcBK, kTcBM))
     return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the query rows");
   auto screen = [&](int kind) -> int {
     if (tc) {
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E, kind,
-                                sa, status, st);
+                                sa, status, st, qrows);
       if (lr) return fail(B2K_ECUDA, "tcgen05 screen launch failed: %s",
                           cudaGetErrorString((cudaError_t)lr));
       return B2K_OK;
     }
-    launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, S, qp.E, kind, sa, st);
+    launch_screen_simt(&ix, dQ, m, m_pad, exclude_self, q_offset, S, qp.E, kind, sa, st, qrows);
     B2K_CUDA(cudaGetLastError());
     return B2K_OK;
   };
-  if ((rc = screen(kSinkRadiusCount))) return rc;
+  if ((rc = screen(cap ? kSinkRadiusList : kSinkRadiusCount))) return rc;
+  if (cap) launch_radius_overflow(sa.rcount, S_lists, m, m_pad, cap, ovf, st);
   int64_t* scan_scratch = nullptr;  // multi-block scans (count offsets, then indptr)
   if ((rc = dalloc(&scan_scratch, (size_t)scan_scratch_len(m), st))) return rc;
   fr.keep(scan_scratch);
@@ -1035,24 +1066,36 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
                            scan_scratch, st);
   int64_t ncand = 0;
   int hstatus[8];
+  int n_ovf = 0;
   B2K_CUDA(cudaMemcpyAsync(&ncand, roff + (size_t)S_lists * m_pad, sizeof(int64_t),
                            cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaMemcpyAsync(hstatus, status, sizeof(hstatus), cudaMemcpyDeviceToHost, st));
+  if (cap) B2K_CUDA(cudaMemcpyAsync(&n_ovf, ovf + m, sizeof(int), cudaMemcpyDeviceToHost, st));
   B2K_CUDA(cudaStreamSynchronize(st));
   if (hstatus[0] != DEV_OK)
     return fail(B2K_ETIMEOUT, "a bounded device wait gave up (code %d)", hstatus[0]);
   if ((hstatus[4] & 1) && !admit_all)
     return radius_block(ix, dQ, m, R2, exclude_self, q_offset, need_distance, sort_results, true,
-                        st, res);
-  if ((rc = dalloc(&sa.rcols, (size_t)ncand, st))) return rc;
-  fr.keep(sa.rcols);
-  if ((rc = screen(kSinkRadiusFill))) return rc;
-  // grouped operand rows: candidates to training rows; rows are re-sorted by
-  // index after the compaction when their lists are out of index order
-  // (grouped rows, or several lists per row, whose columns interleave)
+                        st, res, qrows, counted, sort_rows);
+  // the candidates in one array at their scanned offsets, as training rows
+  // (grouped operand rows are mapped); rows are re-sorted by index after the
+  // compaction when their lists are out of index order (grouped rows, or
+  // several lists per row, whose columns interleave)
   const bool grouped = tc && ix.xperm;
-  if (grouped) launch_translate_cols(sa.rcols, ncand, ix.xperm, status, st);
+  int* cand = nullptr;
+  if ((rc = dalloc(&cand, (size_t)ncand, st))) return rc;
+  fr.keep(cand);
+  if (cap) {
+    launch_radius_pack(sa.rcols, cap, sa.rcount, S_lists, m, m_pad, roff,
+                       grouped ? ix.xperm : nullptr, cand, status, st);
+  } else {
+    sa.rcols = cand;
+    if ((rc = screen(kSinkRadiusFill))) return rc;
+    if (grouped)
+      launch_radius_pack(cand, 0, sa.rcount, S_lists, m, m_pad, roff, ix.xperm, cand, status, st);
+  }
   const bool unordered = grouped || S_lists > S;
+  const bool keep_dist = need_distance || sort_results;
 
   RadiusPlanArgs ra{};
   ra.X = ix.X;
@@ -1063,7 +1106,7 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   ra.S = S_lists;
   ra.roff = roff;
   ra.rcount = sa.rcount;
-  ra.cols = sa.rcols;
+  ra.cols = cand;
   ra.R2 = R2;
   ra.exact_tests = counters;
   ra.status = status;
@@ -1072,6 +1115,34 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   if ((rc = dalloc(&ra.mcount, (size_t)m, st))) return rc;
   fr.keep(ra.mcount);
   launch_classify(ra, st);
+
+  // rows that overflowed their lists: the counted form over those rows alone
+  // (their own block; self-exclusion through their block rows)
+  b2k_radius_result* sub = nullptr;
+  struct SubFree {
+    b2k_radius_result*& r;
+    ~SubFree() {
+      if (r) b2k_radius_result_release(r);
+    }
+  } sub_free{sub};
+  if (n_ovf > 0) {
+    float* Qo = nullptr;
+    int* orow = nullptr;
+    if ((rc = dalloc(&Qo, (size_t)n_ovf * ix.d, st))) return rc;
+    fr.keep(Qo);
+    if ((rc = dalloc(&orow, (size_t)n_ovf, st))) return rc;
+    fr.keep(orow);
+    // sub-call row i answers block row ovf[i] (any order: the scatter places it)
+    launch_gather_fallback(dQ, ix.d, ovf, qrows, n_ovf, Qo, orow, st);
+    B2K_CUDA(cudaGetLastError());
+    sub = new b2k_radius_result();
+    sub->device = ix.device;
+    if ((rc = radius_block(ix, Qo, n_ovf, R2, exclude_self, q_offset, keep_dist, false, admit_all,
+                           st, sub, orow, true, false)))
+      return rc;
+    launch_radius_sub_counts(ovf, n_ovf, sub->indptr, ra.mcount, st);
+  }
+
   int64_t* indptr = nullptr;
   if ((rc = dalloc(&indptr, (size_t)m + 1, st))) return rc;
   launch_scan_rows(ra.mcount, m, indptr, scan_scratch, st);
@@ -1092,15 +1163,17 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
     cudaFreeAsync(indptr, st);
     return rc;
   }
-  const bool keep_dist = need_distance || sort_results;
   if (keep_dist && (rc = dalloc(&dist, (size_t)nnz, st))) {
     cudaFreeAsync(indptr, st);
     cudaFreeAsync(indices, st);
     return rc;
   }
   launch_compact(ra, indptr, indices, dist, st);
+  if (sub)
+    launch_radius_sub_scatter(ovf, n_ovf, sub->indptr, sub->indices, sub->dist, indptr, indices,
+                              dist, st);
   B2K_CUDA(cudaGetLastError());
-  if ((sort_results || unordered) && nnz > 1) {
+  if (sort_rows && (sort_results || unordered) && nnz > 1) {
     // (distance, index) order when asked for, else ascending training index
     // (grouped operand rows list candidates out of index order)
     const bool by_dist = sort_results;
@@ -1142,8 +1215,8 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   res->indptr = indptr;
   res->indices = indices;
   res->dist = dist;
-  res->exact_tests = (int64_t)hc[0];
-  res->candidates = ncand;
+  res->exact_tests = (int64_t)hc[0] + (sub ? sub->exact_tests : 0);
+  res->candidates = ncand + (sub ? sub->candidates : 0);
   return B2K_OK;
 }
 

@@ -131,7 +131,7 @@ void launch_prep_queries_batch(const PrepProblem* tab, const int64_t* row_start,
                                int64_t total_rows, cudaStream_t st);
 
 // ---------------------------------------------------------- screen kernels
-constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2;
+constexpr int kSinkKnn = 0, kSinkRadiusCount = 1, kSinkRadiusFill = 2, kSinkRadiusList = 3;
 struct SinkArgs;
 // tf32: the kind::tf32 form over the index's tf32 operand (kNN sinks only).
 // home (with S = 1): query tile t scans only reference tiles
@@ -224,10 +224,6 @@ void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, c
                         cudaStream_t st);
 
 // ------------------------------------------------------------------ radius
-// cols[i] = xperm[cols[i]]: candidate columns of a grouped operand to training
-// rows (nothing when *status records an error: the fill pass may be unfinished)
-void launch_translate_cols(int* cols, int64_t count, const int* xperm, const int* status,
-                           cudaStream_t st);
 struct RadiusPlanArgs {
   const float* X;
   const float* Q;
@@ -236,7 +232,7 @@ struct RadiusPlanArgs {
   int S;
   const int64_t* roff;   // [S][m_pad] candidate offsets
   const int* rcount;     // [S][m_pad] candidate counts
-  const int* cols;       // candidate columns
+  const int* cols;       // candidates (training rows) at roff
   double* cdist;         // [ncand] member distance or -1
   int64_t* mcount;       // [m] members per query
   double R2;
@@ -252,6 +248,27 @@ void launch_scan_split_counts(const int* counts, int S, int64_t m, int64_t m_pad
 void launch_scan_rows(const int64_t* counts, int64_t m, int64_t* indptr, int64_t* scratch,
                       cudaStream_t st);
 void launch_classify(const RadiusPlanArgs& r, cudaStream_t st);
+// Single-pass screen: rows whose count passed `cap` in any of their S lists
+// are appended to rows[] (rows[m] = how many) and their counts zeroed, so
+// classify and compact skip them.
+void launch_radius_overflow(int* rcount, int S, int64_t m, int64_t m_pad, int cap, int* rows,
+                            cudaStream_t st);
+// Candidates to one array at their scanned offsets roff, as training rows
+// (xperm: grouped operand rows, else null).  src: lists of `cap` entries at
+// slot * cap (single pass), or cap = 0 and src == dst (counted form: the
+// fill's candidates translated in place).  Nothing when *status is an error.
+void launch_radius_pack(const int* src, int cap, const int* rcount, int S, int64_t m,
+                        int64_t m_pad, const int64_t* roff, const int* xperm, int* dst,
+                        const int* status, cudaStream_t st);
+// mcount[rows[i]] = sub_indptr[i + 1] - sub_indptr[i]: members of the rows a
+// counted sub-call answered
+void launch_radius_sub_counts(const int* rows, int count, const int64_t* sub_indptr,
+                              int64_t* mcount, cudaStream_t st);
+// the sub-call's rows into the CSR at indptr[rows[i]] (dist, sub_dist may be null)
+void launch_radius_sub_scatter(const int* rows, int count, const int64_t* sub_indptr,
+                               const int64_t* sub_indices, const double* sub_dist,
+                               const int64_t* indptr, int64_t* indices, double* dist,
+                               cudaStream_t st);
 void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* indices,
                     double* dist, cudaStream_t st);
 // Per-row sort by (distance, index), or by index alone when !by_dist (dist,

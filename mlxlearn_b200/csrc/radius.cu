@@ -3,9 +3,15 @@
 // Pipeline (host side in b200knn.cu, b2k_radius):
 //   1. threshold : T = R2 - ||y_q||^2 + E per query (rounded up): a column with
 //                  v > T has S > R2 and is certainly not a neighbour.
-//   2. screen    : the kNN screen kernels with RadiusCountSink, then
-//                  RadiusFillSink at scanned offsets -> candidate columns per
-//                  query in ascending index order (sinks.cuh).
+//   2. screen    : the tcgen05 screen with RadiusListSink in one pass: each
+//                  (split, column group, query) list keeps up to `cap`
+//                  columns in ascending order and counts them all; rows whose
+//                  count passed `cap` are answered again by a counted
+//                  sub-call (RadiusCountSink, then RadiusFillSink at scanned
+//                  offsets) -- the form the CUDA-core screen always uses.
+//   2b. pack     : the lists (or, in the counted form, the fill) to one
+//                  contiguous candidate array at the scanned offsets, operand
+//                  rows mapped to training rows when the rows are grouped.
 //   3. classify  : canonical float64 value s of every candidate; member iff
 //                  s <= f64_in, non-member iff s > f64_out, otherwise the exact
 //                  integer test key(S) <= floor(R2 * 2^298) (exact.cuh) --
@@ -14,9 +20,9 @@
 //                  distances sqrt(min(s, R2)), rows in ascending index order.
 //   5. sort      : optional per-row (distance, index) order
 //                  (src/mlxlearn/_kernels/radius_result.py:160-187).
-// With grouped operand rows (reorder.cu) the fill pass yields operand rows:
-// they are translated to training rows before step 3, and rows are sorted by
-// training index after step 4 when no distance order is asked for.
+// With grouped operand rows (reorder.cu) the screen yields operand rows:
+// step 2b maps them to training rows, and rows are sorted by training index
+// after step 4 when no distance order is asked for.
 // Replaces the reference's Metal screen + host finisher
 // (src/mlxlearn/_kernels/radius_metal_v1.py:257-611, src/mlxlearn_device/_radius.py:54-330).
 #include <algorithm>
@@ -162,7 +168,7 @@ struct ClassifyArgs {
   int64_t m_pad;
   const int64_t* roff;   // [S][m_pad] candidate offsets
   const int* rcount;     // [S][m_pad]
-  const int* cols;       // candidates
+  const int* cols;       // candidates (training rows)
   double* cdist;         // [ncand]: distance of members, -1 for non-members
   int64_t* mcount;       // [m]
   double R2, f_in, f_out;
@@ -264,12 +270,67 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
   }
 }
 
-__global__ void translate_cols_kernel(int* __restrict__ cols, int64_t count,
-                                      const int* __restrict__ xperm,
-                                      const int* __restrict__ status) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (*reinterpret_cast<volatile const int*>(status) != DEV_OK) return;
-  if (i < count) cols[i] = __ldg(xperm + cols[i]);
+// One thread per row: a row whose count passed the list capacity in any of
+// its lists lost candidates; list it for the counted sub-call and zero its
+// counts (classify then gives it no members and compact writes nothing).
+__global__ void radius_overflow_kernel(int* __restrict__ rcount, int S, int64_t m, int64_t m_pad,
+                                       int cap, int* __restrict__ rows) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  bool over = false;
+  for (int s = 0; s < S; ++s) over |= rcount[(size_t)s * m_pad + r] > cap;
+  if (!over) return;
+  for (int s = 0; s < S; ++s) rcount[(size_t)s * m_pad + r] = 0;
+  rows[atomicAdd(rows + m, 1)] = (int)r;
+}
+
+// One warp per row: the candidates of the row's S lists to their scanned
+// offsets, as training rows.  src holds lists of `cap` entries at slot * cap,
+// or (cap = 0) the candidates already at their offsets, translated in place
+// (each entry is read and written by the same lane).
+__global__ void radius_pack_kernel(const int* src, int cap, const int* __restrict__ rcount,
+                                   int S, int64_t m, int64_t m_pad,
+                                   const int64_t* __restrict__ roff,
+                                   const int* __restrict__ xperm, int* dst,
+                                   const int* __restrict__ status) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= m || call_failed(status, lane)) return;
+  for (int s = 0; s < S; ++s) {
+    const size_t slot = (size_t)s * m_pad + row;
+    const int cnt = rcount[slot];
+    const int64_t o = roff[slot];
+    const int* in = cap ? src + slot * (size_t)cap : src + o;
+    for (int i = lane; i < cnt; i += 32) {
+      const int c = in[i];
+      dst[o + i] = xperm ? __ldg(xperm + c) : c;
+    }
+  }
+}
+
+__global__ void radius_sub_counts_kernel(const int* __restrict__ rows, int count,
+                                         const int64_t* __restrict__ sub_indptr,
+                                         int64_t* __restrict__ mcount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) mcount[rows[i]] = sub_indptr[i + 1] - sub_indptr[i];
+}
+
+// One warp per sub-call row.
+__global__ void radius_sub_scatter_kernel(const int* __restrict__ rows, int count,
+                                          const int64_t* __restrict__ sub_indptr,
+                                          const int64_t* __restrict__ sub_indices,
+                                          const double* __restrict__ sub_dist,
+                                          const int64_t* __restrict__ indptr,
+                                          int64_t* __restrict__ indices,
+                                          double* __restrict__ dist) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= count) return;
+  const int64_t b = sub_indptr[w], e = sub_indptr[w + 1], o = indptr[rows[w]] - b;
+  for (int64_t i = b + lane; i < e; i += 32) {
+    indices[o + i] = sub_indices[i];
+    if (dist) dist[o + i] = sub_dist[i];
+  }
 }
 
 // Sort order of the per-row sorts: (distance, index), or index alone.
@@ -558,11 +619,34 @@ void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* ind
                                                                                  indices, dist);
 }
 
-void launch_translate_cols(int* cols, int64_t count, const int* xperm, const int* status,
-                           cudaStream_t st) {
+void launch_radius_overflow(int* rcount, int S, int64_t m, int64_t m_pad, int cap, int* rows,
+                            cudaStream_t st) {
+  if (m <= 0) return;
+  radius_overflow_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(rcount, S, m, m_pad, cap,
+                                                                      rows);
+}
+
+void launch_radius_pack(const int* src, int cap, const int* rcount, int S, int64_t m,
+                        int64_t m_pad, const int64_t* roff, const int* xperm, int* dst,
+                        const int* status, cudaStream_t st) {
+  if (m <= 0) return;
+  radius_pack_kernel<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(src, cap, rcount, S, m, m_pad,
+                                                             roff, xperm, dst, status);
+}
+
+void launch_radius_sub_counts(const int* rows, int count, const int64_t* sub_indptr,
+                              int64_t* mcount, cudaStream_t st) {
   if (count <= 0) return;
-  translate_cols_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(cols, count, xperm,
-                                                                          status);
+  radius_sub_counts_kernel<<<(count + 255) / 256, 256, 0, st>>>(rows, count, sub_indptr, mcount);
+}
+
+void launch_radius_sub_scatter(const int* rows, int count, const int64_t* sub_indptr,
+                               const int64_t* sub_indices, const double* sub_dist,
+                               const int64_t* indptr, int64_t* indices, double* dist,
+                               cudaStream_t st) {
+  if (count <= 0) return;
+  radius_sub_scatter_kernel<<<(unsigned)((count + 7) / 8), 256, 0, st>>>(
+      rows, count, sub_indptr, sub_indices, sub_dist, indptr, indices, dist);
 }
 
 void launch_sort_rows(const int64_t* indptr, int64_t m, int64_t* indices, double* dist,

@@ -708,6 +708,7 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
             : launch_tc_variant<SINK, false, EW, false>(maps, p, KB, grid, st))
   if (sink_kind == kSinkRadiusCount) return B2K_TC_LAUNCH(RadiusCountSink, kRadiusEW);
   if (sink_kind == kSinkRadiusFill) return B2K_TC_LAUNCH(RadiusFillSink, kRadiusEW);
+  if (sink_kind == kSinkRadiusList) return B2K_TC_LAUNCH(RadiusListSink, kRadiusEW);
   if (tc_knn_ew(sa.k) == 16) {
     if (sa.k <= 8) return B2K_TC_LAUNCH(KnnSink<8>, 16);
     if (sa.k <= 12) return B2K_TC_LAUNCH(KnnSink<12>, 16);

@@ -6,6 +6,7 @@
 //   KnnSink        : the running k-smallest tracker + candidate list (tracker.cuh)
 //   RadiusCountSink: counts columns with v <= T (T fixed per row: R2 - ||y_q||^2 + E)
 //   RadiusFillSink : writes those columns, in ascending order, at a precomputed offset
+//   RadiusListSink : writes them into a fixed-capacity list per (split, row), counting all
 #pragma once
 #include "internal.cuh"
 #include "tracker.cuh"
@@ -21,8 +22,9 @@ struct SinkArgs {
   const float* thr;      // [m_pad] admission threshold per row
   int* rcount;           // [S][m_pad]
   const int64_t* roff;   // [S][m_pad]
-  int* rcols;            // candidate columns
+  int* rcols;            // candidate columns (RadiusListSink: [S][m_pad][rcap] lists)
   int m_pad;
+  int rcap;              // RadiusListSink: entries kept per list
 };
 
 // Shared 32-column prefilter: the 3-input-min tree over the chunk.
@@ -108,6 +110,44 @@ struct RadiusFillSink {
   B2K_DEV uint32_t tile_fetch() const { return 0; }
   B2K_DEV void tile_apply(uint32_t) {}
   B2K_DEV void finish(const SinkArgs&) {}
+};
+
+// Single-pass radius: the admitted columns of (split, row), ascending, into a
+// list of rcap entries at slot * rcap; the count goes on past rcap, so a
+// count above it marks a row whose list lost columns (the caller answers that
+// row again with the counted two-pass form).
+struct RadiusListSink {
+  static constexpr bool kWarpWide = false;
+  float T;
+  int self, cnt, cap;
+  int* out;
+  size_t slot;
+  B2K_DEV void init(const SinkArgs& a, int row, int split, float /*E*/, int self_col) {
+    slot = (size_t)split * a.m_pad + row;
+    T = a.thr[row];
+    self = self_col;
+    cnt = 0;
+    cap = a.rcap;
+    out = a.rcols + slot * (size_t)a.rcap;
+  }
+  B2K_DEV void put(int col) {
+    if (cnt < cap) out[cnt] = col;
+    ++cnt;
+  }
+  B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
+    if (min32(v) <= T) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (v[i] <= T && col0 + i != self) put(col0 + i);
+    }
+  }
+  B2K_DEV void offer1(float x, int col) {
+    if (x <= T && col != self) put(col);
+  }
+  B2K_DEV void tile_sync() {}
+  B2K_DEV uint32_t tile_fetch() const { return 0; }
+  B2K_DEV void tile_apply(uint32_t) {}
+  B2K_DEV void finish(const SinkArgs& a) { a.rcount[slot] = cnt; }
 };
 
 // kNN sink for large k on the lazy tracker (tracker.cuh).  Warp-collective:

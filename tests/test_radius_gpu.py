@@ -141,3 +141,37 @@ def test_radius_row_grouping_both_ways(group, monkeypatch):
     np.testing.assert_array_equal(ip, op)
     np.testing.assert_array_equal(ix, oix)
     np.testing.assert_array_equal(dd, od)
+
+
+@pytest.mark.parametrize("cap", ["0", "4", "40"])
+def test_radius_single_pass_overflow_and_counted_form(cap, monkeypatch):
+    """The tcgen05 radius screen runs once into lists of a fixed capacity; a
+    row whose count passes it in any list is answered again by the counted
+    two-pass form on those rows alone and scattered into the CSR.  Capacity 0
+    is the counted form for every row; 4 sends most rows (and every row past
+    4 x 4 x 64 entries) through the sub-call, self-queries included (their
+    excluded column follows the row into the sub-call); 40 only the long
+    rows."""
+    monkeypatch.setenv("B2K_RADIUS_CAP", cap)
+    C = np.random.default_rng(21).normal(0, 2.0, (12, 24))
+    X, _ = mixture(np.random.default_rng(22), 24000, C, 1.0)
+    Q, _ = mixture(np.random.default_rng(23), 600, C, 1.0)
+    Q[:3] += 30.0  # no neighbours
+    index = make_index(X)
+    for r, sort in ((5.0, False), (5.0, True), (12.0, False), (12.0, True)):
+        op, oix, od = oracle.radius(X, Q, r, sort_results=sort)
+        ip, ix, dd = csr(index.query_radius_csr(Q, r, sort_results=sort))
+        np.testing.assert_array_equal(ip, op)
+        np.testing.assert_array_equal(ix, oix)
+        np.testing.assert_array_equal(dd, od)
+    assert np.diff(op).max() > 4 * 4 * 64  # overflows any list layout at capacity 4
+    ip, ix, dd = csr(index.query_radius_csr(Q, 12.0, need_distance=False))
+    op, oix, _ = oracle.radius(X, Q, 12.0)
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    assert dd is None
+    op, oix, od = oracle.radius(X, X, 4.0, exclude_self=True)
+    ip, ix, dd = csr(index.query_radius_csr(X, 4.0, exclude_self=True))
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    np.testing.assert_array_equal(dd, od)
