@@ -51,6 +51,10 @@ extern "C" {
 #define B2K_MODE_EXACT 3       /* float64 exhaustive scan + exact ties (slow) */
 #define B2K_MODE_TF32 4        /* plain form on the tensor cores: tf32 tcgen05
                                   screen + the same certified re-rank         */
+#define B2K_MODE_U8 5          /* integer pixels: exact u8 tcgen05 (kind::i8)
+                                  screen, used by AUTO when the index and the
+                                  queries are integers in [0, 255] and k <= 16;
+                                  on other data the certified screens run      */
 /* Flag ORed into the mode of b2k_knn / b2k_knn_device: distances are returned
  * as the canonical float64 squared distance instead of its square root (the
  * `_squared` option of DeviceNeighborIndex.query,

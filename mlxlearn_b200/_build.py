@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libb200knn.so")
-SOURCES = ["b200knn.cu", "prep.cu", "screen_tc.cu", "screen_simt.cu", "certify.cu", "radius.cu", "noalloc.cu", "reorder.cu", "backward.cu", "votes.cu", "batch.cu", "segments.cu", "shards.cu"]
+SOURCES = ["b200knn.cu", "prep.cu", "screen_tc.cu", "screen_simt.cu", "certify.cu", "radius.cu", "noalloc.cu", "reorder.cu", "backward.cu", "votes.cu", "batch.cu", "segments.cu", "shards.cu", "exact_u8.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]

@@ -30,9 +30,10 @@ MODE_FP32 = 1
 MODE_BF16 = 2
 MODE_EXACT = 3
 MODE_TF32 = 4
+MODE_U8 = 5
 MODE_SQUARED = 16  # flag: squared distances (B2K_MODE_SQUARED)
 MODES = {"auto": MODE_AUTO, "fp32": MODE_FP32, "bf16": MODE_BF16, "exact": MODE_EXACT,
-         "tf32": MODE_TF32}
+         "tf32": MODE_TF32, "u8": MODE_U8}
 
 
 class Stats(ctypes.Structure):

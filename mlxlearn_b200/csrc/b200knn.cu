@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdarg>
 #include <cmath>
 #include <cstdio>
@@ -345,6 +346,90 @@ static int ensure_tf32(Index& ix) {
   return B2K_OK;
 }
 
+// The exact u8 screen's operand, when every training coordinate is an
+// integer in [0, 255] (checked once); *ok tells whether the index qualifies.
+static int ensure_u8(Index& ix, bool* ok) {
+  std::lock_guard<std::mutex> lock(ix.mu);
+  *ok = false;
+  if (ix.d > kU8MaxD) return B2K_OK;
+  cudaStream_t st = ix.stream;
+  if (ix.u8_state == 0) {
+    int* flag = nullptr;
+    B2K_CUDA(cudaMalloc(&flag, sizeof(int)));
+    B2K_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+    launch_u8_check(ix.X, ix.n * (int64_t)ix.d, flag, st);
+    int h = 1;
+    B2K_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    B2K_CUDA(cudaStreamSynchronize(st));
+    cudaFree(flag);
+    ix.u8_state = h ? -1 : 1;
+  }
+  if (ix.u8_state < 0) return B2K_OK;
+  if (!ix.u8_ready) {
+    ix.dpu = (int32_t)round_up(ix.d, kTcBKu);
+    ix.n_pad_tc = round_up(ix.n, kTcBN);
+    B2K_CUDA(cudaMalloc(&ix.Xu, (size_t)ix.n_pad_tc * ix.dpu));
+    B2K_CUDA(cudaMalloc(&ix.nxu, (size_t)ix.n_pad_tc * sizeof(int)));
+    // padding rows: v = INT_MAX, never admitted
+    launch_prep_u8(ix.X, ix.n, ix.d, ix.n_pad_tc, ix.dpu, ix.Xu, ix.nxu, nullptr, INT_MAX, st);
+    B2K_CUDA(cudaGetLastError());
+    B2K_CUDA(cudaStreamSynchronize(st));
+    if (!tensor_map_2d(&ix.tmap_bu, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix.Xu, (uint64_t)ix.dpu,
+                       (uint64_t)ix.n_pad_tc, kTcBKu, kTcBN, 128))
+      return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the u8 operand");
+    ix.u8_ready = true;
+  }
+  *ok = true;
+  return B2K_OK;
+}
+
+static int choose_splits(int64_t m_tiles, int64_t n_tiles, int64_t slots);
+
+// Exact kNN of integer queries on a u8 index (exact_u8.cu): prep, the
+// kind::i8 screen, the merge of the lists.  dQ's rows are integers in [0, 255].
+static int run_u8(Index& ix, const float* dQ, int64_t m, int k, int exclude_self,
+                  int64_t q_offset, double* d_dist, int64_t* d_idx, int squared, int* status,
+                  cudaStream_t st, StreamFree& fr, int* splits_out) {
+  int rc;
+  const int64_t m_pad = round_up(m, kTcBM);
+  const int64_t n_tiles = ix.n_pad_tc / kTcBN;
+  const int S = choose_splits(m_pad / kTcBM, n_tiles, num_sms(ix.device));
+  const int S_lists = S * tc_u8_column_groups(k);
+  *splits_out = S;
+  uint8_t* Qu = nullptr;
+  int64_t* nq = nullptr;
+  uint32_t* shared_kth = nullptr;
+  if ((rc = dalloc(&Qu, (size_t)m_pad * ix.dpu, st))) return rc;
+  fr.keep(Qu);
+  if ((rc = dalloc(&nq, (size_t)m_pad, st))) return rc;
+  fr.keep(nq);
+  if ((rc = dalloc(&shared_kth, (size_t)m_pad, st))) return rc;
+  fr.keep(shared_kth);
+  B2K_CUDA(cudaMemsetAsync(shared_kth, 0xff, (size_t)m_pad * sizeof(uint32_t), st));
+  launch_prep_u8(dQ, m, ix.d, m_pad, ix.dpu, Qu, nullptr, nq, 0, st);
+  ScreenOut so{};
+  so.cap = k;
+  so.m_pad = (int)m_pad;
+  if ((rc = dalloc(&so.lists, (size_t)S_lists * m_pad * k, st))) return rc;
+  fr.keep(so.lists);
+  SinkArgs sa{};
+  sa.out = so;
+  sa.k = k;
+  sa.shared_kth = shared_kth;
+  CUtensorMap tmap_a;
+  if (!tensor_map_2d(&tmap_a, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, Qu, (uint64_t)ix.dpu,
+                     (uint64_t)m_pad, kTcBKu, kTcBM, 128))
+    return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the u8 query rows");
+  // status[6] (zeroed by the caller) counts the claimed work units
+  const int lr = launch_screen_tc_u8(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, sa,
+                                     status, st, status + 6);
+  if (lr) return fail(B2K_ECUDA, "u8 tcgen05 screen launch failed: %s",
+                      cudaGetErrorString((cudaError_t)lr));
+  launch_u8_merge(so.lists, S_lists, m, m_pad, k, nq, squared, d_dist, d_idx, status, st);
+  B2K_CUDA(cudaGetLastError());
+  return B2K_OK;
+}
+
 static int ensure_pivots(Index& ix) {
   std::lock_guard<std::mutex> lock(ix.mu);
   return make_pivots(ix);
@@ -433,11 +518,36 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   const int squared = (mode & B2K_MODE_SQUARED) ? 1 : 0;
   const int sq_flag = squared ? B2K_MODE_SQUARED : 0;
   mode &= ~B2K_MODE_SQUARED;
+  int rc;
+  bool u8 = false;
+  // Integer pixels: the exact u8 screen, when the index and every query
+  // coordinate are integers in [0, 255] (AUTO in the bf16 screen's size range,
+  // or asked for); otherwise the certified screens.
+  if (m > 0 && k <= kU8MaxK && ix.range_ok &&
+      (mode == B2K_MODE_U8 || (mode == B2K_MODE_AUTO && ix.d >= 16 && ix.n >= 2048))) {
+    bool ok = false;
+    if ((rc = ensure_u8(ix, &ok))) return rc;
+    if (ok) {
+      cudaSetDevice(ix.device);
+      int* flag = nullptr;
+      if ((rc = dalloc(&flag, 1, st))) return rc;
+      B2K_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+      launch_u8_check(dQ, m * (int64_t)ix.d, flag, st);
+      int h = 1;
+      B2K_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+      B2K_CUDA(cudaStreamSynchronize(st));
+      cudaFreeAsync(flag, st);
+      ok = h == 0;
+    }
+    u8 = ok;
+  }
+  if (mode == B2K_MODE_U8) mode = B2K_MODE_AUTO;  // not integer pixels: the certified screens
+  if (u8) mode = B2K_MODE_U8;
   if (mode == B2K_MODE_AUTO)
     mode = (!ix.range_ok || k > kMaxK) ? B2K_MODE_EXACT
            : (ix.d >= 16 && ix.n >= 2048) ? B2K_MODE_BF16
                                          : B2K_MODE_FP32;
-  if (mode != B2K_MODE_EXACT && (!ix.range_ok || k > kMaxK)) mode = B2K_MODE_EXACT;
+  if (mode != B2K_MODE_EXACT && !u8 && (!ix.range_ok || k > kMaxK)) mode = B2K_MODE_EXACT;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->mode_used = mode;
@@ -452,7 +562,6 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
 
   int* status = nullptr;
   unsigned long long* counters = nullptr;
-  int rc;
   if ((rc = dalloc(&status, 8, st))) return rc;
   fr.keep(status);
   if ((rc = dalloc(&counters, 8, st))) return rc;
@@ -469,6 +578,11 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     rc = run_exact(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, nullptr, nullptr,
                    counters, status, st, fr, true, ext_perm, squared);
     if (rc) return rc;
+  } else if (mode == B2K_MODE_U8) {
+    if (stats) cudaEventRecord(ev[1], st);
+    rc = run_u8(ix, dQ, m, k, exclude_self, q_offset, d_dist, d_idx, squared, status, st, fr, &S);
+    if (rc) return rc;
+    if (stats) cudaEventRecord(ev[2], st);
   } else {
     if (mode == B2K_MODE_BF16 && (rc = ensure_bf16(ix))) return rc;
     if (mode == B2K_MODE_TF32 && (rc = ensure_tf32(ix))) return rc;
@@ -701,7 +815,7 @@ static int validate_knn(const Index& ix, int64_t m, int32_t k, int32_t exclude_s
                 "query rows at offset %lld and %lld training rows.",
                 (long long)m, (long long)q_offset, (long long)ix.n);
   const int32_t base = mode & ~B2K_MODE_SQUARED;
-  if (base < B2K_MODE_AUTO || base > B2K_MODE_TF32) return fail(B2K_EINVAL, "unknown mode %d", mode);
+  if (base < B2K_MODE_AUTO || base > B2K_MODE_U8) return fail(B2K_EINVAL, "unknown mode %d", mode);
   return B2K_OK;
 }
 
@@ -871,6 +985,8 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.Xt);
   cudaFree(ix.Xtaug);
   cudaFree(ix.taug_ones);
+  cudaFree(ix.Xu);
+  cudaFree(ix.nxu);
   if (ix.stream) cudaStreamDestroy(ix.stream);
   delete h;
   return B2K_OK;

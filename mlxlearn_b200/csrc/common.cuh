@@ -143,6 +143,19 @@ B2K_DEV void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::i8 (8-bit integer operands, s32
+// accumulation: every product and sum is exact while it fits 32 bits).
+B2K_DEV void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                    uint32_t accumulate) {
+  asm volatile(
+      "{\n"
+      ".reg .pred p;\n"
+      "setp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n"
+      "}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // Arrive on `bar` when all previously issued tcgen05.mma of this thread complete.
 B2K_DEV void mma_commit(uint64_t* bar) {
   asm volatile(
@@ -209,6 +222,13 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_bf16) {
 // K-major, shape M x N.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(N >> 3) << 17) |
+         (uint32_t(M >> 4) << 24);
+}
+
+// Instruction descriptor, kind::i8: D s32 (format 2), A and B unsigned 8-bit
+// (format 0), both K-major, shape M x N.
+__host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
+  return (2u << 4) | (0u << 7) | (0u << 10) | (uint32_t(N >> 3) << 17) |
          (uint32_t(M >> 4) << 24);
 }
 

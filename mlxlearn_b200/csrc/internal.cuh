@@ -16,6 +16,9 @@ constexpr int kTcBK = 64;    // 16-bit elements per 128-byte swizzle row
 constexpr int kTcAug = 16;   // norm columns appended to every operand row (one K=16 step)
 constexpr int kTcBKf = 32;   // fp32 (tf32) elements per 128-byte swizzle row
 constexpr int kTcAugF = 8;   // tf32 norm columns (one K=8 step, 32 bytes like kTcAug)
+constexpr int kTcBKu = 128;  // u8 elements per 128-byte swizzle row
+constexpr int kU8MaxK = 16;  // largest k of the exact u8 screen
+constexpr int kU8MaxD = 16384;  // ||x||^2 and -2<q, x> of u8 rows fit int32
 constexpr int kSimtBM = 128; // query rows per CUDA-core tile
 constexpr int kSimtBN = 64;  // reference rows per CUDA-core tile
 constexpr int kListCap = 512;      // screen list entries per (split, query)
@@ -70,6 +73,14 @@ struct Index {
   float* taug_ones = nullptr;    // [128, 8] [1, 1, 1, 0...] (query side)
   float xt_max = 0, ext_max = 0; // max ||tf32 operand||, max ||(x - c) - tf32 operand||
   CUtensorMap tmap_bt, tmap_btaug, tmap_ataug;
+  // u8 copy for the exact integer screen (lazy; training row order), when
+  // every coordinate is an integer in [0, 255]
+  int u8_state = 0;              // 0 not checked, 1 integer pixels, -1 not
+  bool u8_ready = false;
+  int32_t dpu = 0;               // d padded to a multiple of kTcBKu
+  uint8_t* Xu = nullptr;         // [n_pad_tc, dpu]
+  int* nxu = nullptr;            // [n_pad_tc] ||x||^2 exactly; INT_MAX on padding rows
+  CUtensorMap tmap_bu;           // over Xu, box 128 x 256, 128-byte swizzle
   // Row grouping of the bf16 operand (reorder.cu): operand row i holds
   // training row xperm[i]; rows sharing a nearest pivot are consecutive, so a
   // query tile's candidates fall in few reference tiles.  Null: identity.
@@ -102,6 +113,21 @@ void launch_prep_aug(const Index* ix, uint16_t* Xaug, uint16_t* ones, cudaStream
 void launch_prep_index_tf32(const Index* ix, float* Xt, cudaStream_t st, const int* rows);
 void launch_prep_aug_tf32(const Index* ix, float* Xtaug, float* ones, cudaStream_t st,
                           const int* rows);
+// ------------------------------------------------- exact u8 screen (exact_u8.cu)
+// flag |= 1 when some value is not an integer in [0, 255]
+void launch_u8_check(const float* v, int64_t count, int* flag, cudaStream_t st);
+// rows [rows_pad, dpu] u8 of v [rows, d] (zero padding) and their squared norms
+// (exact; `pad_norm` on padding rows)
+void launch_prep_u8(const float* v, int64_t rows, int d, int64_t rows_pad, int dpu, uint8_t* out,
+                    int* norms, int64_t* norms64, int pad_norm, cudaStream_t st);
+// Per query: the k smallest (v, column) over the S lists of k entries each
+// (v = ||x||^2 - 2<q, x>, INT_MAX = empty), then squared distance ||q||^2 + v
+// (exact) or its square root, and the column as index.  rows: the query's
+// output row (null: its own).
+void launch_u8_merge(const int2* lists, int S, int64_t m, int64_t m_pad, int k,
+                     const int64_t* nq, int squared, double* dist, int64_t* idx,
+                     const int* status, cudaStream_t st);
+
 // Query preparation: per-row fp32/bf16 error bounds and the bf16 operand.
 struct QueryPrep {
   float* E;        // [m_pad] screen error bound (fp32, rounded up)
@@ -141,7 +167,14 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
                      const SinkArgs& sa, int* status, cudaStream_t st,
                      const int* perm = nullptr, int* unit_counter = nullptr, bool tf32 = false,
                      const int* home = nullptr, int home_tiles = 0);
+// The exact u8 screen (kind::i8; index and queries integers in [0, 255]):
+// per (split, column group, query) the k smallest (||x||^2 - 2<q, x>, column)
+// into sa.out.lists (cap = k), columns in training order; E unused.
+int launch_screen_tc_u8(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
+                        int exclude_self, int64_t q_offset, int S, const SinkArgs& sa,
+                        int* status, cudaStream_t st, int* unit_counter);
 int tc_column_groups(int k);
+int tc_u8_column_groups(int k);  // lists per (split, row) of the u8 screen
 int tc_radius_groups();  // candidate lists per (split, row) of the tcgen05 radius screens
 bool tc_lazy_sink(int k);  // the tcgen05 kNN screen's lazy tracker (no k-th output)
 // noalloc: one scanner per row (half the list memory of the default two)

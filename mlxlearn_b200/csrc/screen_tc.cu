@@ -231,11 +231,16 @@ B2K_DEV uint64_t smem_desc_sw32(const void* smem_tile) {
 // Threads per CTA: producer warp, MMA warp, EW epilogue warps, gate warp.
 __host__ __device__ constexpr int tc_block_threads(int ew) { return 96 + 32 * ew; }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32>
+// Operand kinds of the screen kernel.
+constexpr int kKindBf16 = 0, kKindTf32 = 1, kKindU8 = 2;
+
+template <class Sink, bool A_STREAM, int EW, bool BATCH, int KIND>
 __global__ void __launch_bounds__(tc_block_threads(EW), 1)
     screen_tc_kernel(const __grid_constant__ TcMapSet<BATCH ? kBatchGroups : 1> maps,
                      const __grid_constant__ TcParams p) {
   constexpr int G = BATCH ? kBatchGroups : 1;
+  constexpr bool TF32 = KIND == kKindTf32;
+  constexpr bool U8 = KIND == kKindU8;  // exact integer products, no norm columns
   constexpr int kEpiThreads = 32 * EW;
   constexpr int kHalves = EW / 4;                 // column groups per tile
   constexpr int kChunks = kTcBN / 32 / kHalves;   // 32-column chunks per epilogue warp
@@ -282,8 +287,10 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
     mbar_init(a_empty, 2);
     mbar_init(&acc_full[0], 1);
     mbar_init(&acc_full[1], 1);
-    mbar_init(&acc_empty[0], kEpiThreads);
-    mbar_init(&acc_empty[1], kEpiThreads);
+    // one arrival per epilogue warp: 512 per-thread arrivals on one barrier
+    // serialise in shared memory and delayed every release by ~700 cycles
+    mbar_init(&acc_empty[0], EW);
+    mbar_init(&acc_empty[1], EW);
     mbar_init(aaug_full, 1);
     mbar_init(mma_drain, 1);
     for (int g = 0; g < kGoRing; ++g) mbar_init(&go[g], 1);
@@ -309,12 +316,16 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       for (int g = 0; g < G; ++g) {
         prefetch_tmap(&maps.a[g]);
         prefetch_tmap(&maps.b[g]);
-        prefetch_tmap(&maps.baug[g]);
+        if (!U8) prefetch_tmap(&maps.baug[g]);
       }
-      prefetch_tmap(&maps.aaug);
-      // the query-side norm columns are the same for every tile: load once
-      mbar_arrive_expect_tx(aaug_full, kAAugBytes);
-      tma_load_2d(aaug_smem, &maps.aaug, aaug_full, 0, 0);
+      if (U8) {
+        mbar_arrive(aaug_full);  // no norm columns: the epilogue adds ||x||^2
+      } else {
+        prefetch_tmap(&maps.aaug);
+        // the query-side norm columns are the same for every tile: load once
+        mbar_arrive_expect_tx(aaug_full, kAAugBytes);
+        tma_load_2d(aaug_smem, &maps.aaug, aaug_full, 0, 0);
+      }
       uint32_t stage = 0, phase = 0, a_phase = 0;
       // copies issued, for the exit path: per stage the parity of the full
       // phase its latest load completes, and the same for the query tile
@@ -324,8 +335,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       while (cur.next(p, x)) {
         const int KB = x.pr->KB;
         // TMA coordinates count elements of the map's type: a 128-byte block
-        // is 64 bf16 or 32 fp32 columns
-        constexpr int kx = TF32 ? kTcBKf : kTcBK;
+        // is 64 bf16, 32 fp32 or 128 u8 columns
+        constexpr int kx = TF32 ? kTcBKf : (U8 ? kTcBKu : kTcBK);
         const int g = G == 1 ? 0 : x.pr->group;
         const int a_row = x.pr->a_row0 + x.t * kTcBM;
         const int b_row0 = x.pr->b_row0;
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
             pend |= 1u << stage;
             pend_par = (pend_par & ~(1u << stage)) | (phase << stage);
             uint8_t* st = b_smem + (size_t)stage * stage_bytes;
-            const bool last = kb == KB - 1;
+            const bool last = !U8 && kb == KB - 1;  // with the norm columns
             mbar_arrive_expect_tx(&full[stage], (A_STREAM ? kATileBytes : 0) + kBTileBytes +
                                                     (last ? kBAugBytes : 0));
             if (A_STREAM) tma_load_2d(st, tmA, &full[stage], kb * kx, a_row);
@@ -384,11 +395,15 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   } else if (warp == 1) {
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      constexpr uint32_t idesc = TF32 ? idesc_tf32(kTcBM, kTcBN) : idesc_f16(kTcBM, kTcBN, 1);
-      // one MMA of the screen's kind: 32 bytes of K (16 bf16 or 8 tf32)
+      constexpr uint32_t idesc = TF32 ? idesc_tf32(kTcBM, kTcBN)
+                                 : U8 ? idesc_u8(kTcBM, kTcBN)
+                                      : idesc_f16(kTcBM, kTcBN, 1);
+      // one MMA of the screen's kind: 32 bytes of K (16 bf16, 8 tf32 or 32 u8)
       auto mma = [&](uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
         if constexpr (TF32)
           mma_tf32(d_tmem, a, b, idesc, acc);
+        else if constexpr (U8)
+          mma_i8(d_tmem, a, b, idesc, acc);
         else
           mma_f16(d_tmem, a, b, idesc, acc);
       };
@@ -424,7 +439,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
                 // advance 32 bytes inside the 128-byte swizzle atom: +2 in 16-byte units
                 mma(d_tmem, adesc + 2 * kk, bdesc + 2 * kk, (kb | kk) != 0);
               }
-              if (kb == KB - 1)  // + ||y_x||^2 through the norm columns
+              if (!U8 && kb == KB - 1)  // + ||y_x||^2 through the norm columns
                 mma(d_tmem, aaug_desc, smem_desc_sw32(st + baug_off), 1);
               mma_commit(&empty[stage]);
               if (++stage == (uint32_t)nst) stage = 0;
@@ -492,6 +507,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
     const int row_in_tile = g * 32 + lane;
     const int et = threadIdx.x - 64;        // 0 .. kEpiThreads-1
     float* spill = spill_all + et * kSpillStride;
+    // u8: the warp's ||x||^2 values of the current tile (its spill rows are unused)
+    int* nx_warp = reinterpret_cast<int*>(spill_all + (size_t)ew * 32 * kSpillStride);
     uint32_t acc_it = 0;
     UnitCursor<BATCH> cur(p, ring, false);
     TcUnit x;
@@ -513,12 +530,12 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
       };
       if constexpr (Sink::kWarpWide) {
         const int orig = valid ? (pr.perm ? pr.perm[row] : row) : 0;
-        sink.init_warp(pr.sink, row, x.slot * kHalves + half, valid ? pr.E[row] : 0.0f,
+        sink.init_warp(pr.sink, row, x.slot * kHalves + half, (valid && pr.E) ? pr.E[row] : 0.0f,
                        (valid && pr.exclude_self) ? self_column(orig) : -1, valid,
                        reinterpret_cast<unsigned*>(spill_all + (size_t)ew * 32 * kSpillStride));
       } else if (valid) {
         const int orig = pr.perm ? pr.perm[row] : row;
-        sink.init(pr.sink, row, x.slot * kHalves + half, pr.E[row],
+        sink.init(pr.sink, row, x.slot * kHalves + half, pr.E ? pr.E[row] : 0.0f,
                   pr.exclude_self ? self_column(orig) : -1);
       }
       uint32_t pending_key = kNoKey;
@@ -528,17 +545,47 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
         const uint32_t shared_key = pending_key;
         pending_key = live ? sink.tile_fetch() : 0u;
         const uint32_t buf = acc_it & 1, apar = (acc_it >> 1) & 1;
+        // u8: ||x||^2 of this warp's columns, fetched before the wait
+        int nxr[kChunks];
+        if constexpr (U8) {
+          const int* g_nx = pr.nxu + (size_t)j * kTcBN + c0 * 32 + lane;
+#pragma unroll
+          for (int c = 0; c < kChunks; ++c) nxr[c] = __ldg(g_nx + c * 32);
+        }
         // warp-uniform outcome, so collective sinks never run on a partial warp
         if (!__all_sync(0xffffffffu,
                         mbar_wait(&acc_full[buf], apar, status, DEV_TIMEOUT_ACC, lim)))
           goto epi_done;
         tc_fence_after();
+        if constexpr (U8) {
+          // into the warp's scratch, read back as broadcasts (the previous
+          // tile's reads are done first)
+          __syncwarp();
+#pragma unroll
+          for (int c = 0; c < kChunks; ++c) nx_warp[c * 32 + lane] = nxr[c];
+          __syncwarp();
+        }
         const uint32_t tbase = tmem_base + ((uint32_t)(g * 32) << 16) + buf * kTcBN + c0 * 32;
         auto process = [&](const uint32_t(&r)[32], int c) {
-          float v[32];
+          if constexpr (U8) {
+            // v = ||x||^2 - 2<q, x>, exact in int32
+            const int4* nx4 = reinterpret_cast<const int4*>(nx_warp + c * 32);
+            int v[32];
 #pragma unroll
-          for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-          if (live) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
+            for (int i = 0; i < 8; ++i) {
+              const int4 t = nx4[i];
+              v[4 * i] = t.x - 2 * (int)r[4 * i];
+              v[4 * i + 1] = t.y - 2 * (int)r[4 * i + 1];
+              v[4 * i + 2] = t.z - 2 * (int)r[4 * i + 2];
+              v[4 * i + 3] = t.w - 2 * (int)r[4 * i + 3];
+            }
+            if (live) sink.offer32i(v, j * kTcBN + (c0 + c) * 32);
+          } else {
+            float v[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+            if (live) sink.offer32(v, j * kTcBN + (c0 + c) * 32, spill);
+          }
         };
         if constexpr (EW == 16) {
           // four warps per lane group: one 32-column buffer each (register budget);
@@ -549,8 +596,10 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
             tmem_ld_32x32b_x32(tbase + c * 32, ra);
             tmem_ld_wait_regs(ra);
             if (c == kChunks - 1) {
+              // every lane's loads are complete (wait::ld) before the warp's arrival
               tc_fence_before();
-              mbar_arrive(&acc_empty[buf]);
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&acc_empty[buf]);
             }
             process(ra, c);
           }
@@ -571,7 +620,8 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
           } else {
             // all of this warp's columns are in registers: hand the buffer back
             tc_fence_before();
-            mbar_arrive(&acc_empty[buf]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);
             process(rb, c + 1);
           }
         }
@@ -598,7 +648,7 @@ __global__ void __launch_bounds__(tc_block_threads(EW), 1)
   }
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, int KIND = kKindBf16>
 size_t tc_variant_smem(int KB_max, int* stages_out) {
   const size_t budget = 227 * 1024;
   int stages = 8;
@@ -608,14 +658,14 @@ size_t tc_variant_smem(int KB_max, int* stages_out) {
   return smem < kMinCtaSmem ? kMinCtaSmem : smem;
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, int KIND = kKindBf16>
 int prepare_tc_variant(int KB_max) {
   const size_t smem = tc_variant_smem<Sink, A_STREAM, EW, BATCH>(KB_max, nullptr);
-  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, TF32>;
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, KIND>;
   return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-template <class Sink, bool A_STREAM, int EW, bool BATCH, bool TF32 = false>
+template <class Sink, bool A_STREAM, int EW, bool BATCH, int KIND = kKindBf16>
 int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcParams& p, int KB_max,
                       int grid, cudaStream_t st) {
   int stages = 0;
@@ -624,7 +674,7 @@ int launch_tc_variant(const TcMapSet<BATCH ? kBatchGroups : 1>& maps, const TcPa
   q.stages = stages;
   q.a_blocks = KB_max;
   q.spin_limit = device_spin_limit();
-  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, TF32>;
+  auto kern = screen_tc_kernel<Sink, A_STREAM, EW, BATCH, KIND>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;
@@ -690,8 +740,8 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   maps.aaug = tf32 ? ix->tmap_ataug : ix->tmap_aaug;
   if (tf32) {
 #define B2K_TC_LAUNCH_TF32(SINK, EW)                                                 \
-  (a_stream ? launch_tc_variant<SINK, true, EW, false, true>(maps, p, KB, grid, st) \
-            : launch_tc_variant<SINK, false, EW, false, true>(maps, p, KB, grid, st))
+  (a_stream ? launch_tc_variant<SINK, true, EW, false, kKindTf32>(maps, p, KB, grid, st) \
+            : launch_tc_variant<SINK, false, EW, false, kKindTf32>(maps, p, KB, grid, st))
     if (tc_knn_ew(sa.k) == 16) {
       if (sa.k <= 8) return B2K_TC_LAUNCH_TF32(KnnSink<8>, 16);
       if (sa.k <= 12) return B2K_TC_LAUNCH_TF32(KnnSink<12>, 16);
@@ -720,6 +770,42 @@ int launch_screen_tc(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_
   return B2K_TC_LAUNCH(LazyKnnSink, 8);
 #undef B2K_TC_LAUNCH
 }
+
+int launch_screen_tc_u8(Index* ix, const CUtensorMap* tmap_a, int64_t m, int64_t m_pad,
+                        int exclude_self, int64_t q_offset, int S, const SinkArgs& sa,
+                        int* status, cudaStream_t st, int* unit_counter) {
+  if (sa.k < 1 || sa.k > kU8MaxK || !ix->u8_ready) return (int)cudaErrorInvalidValue;
+  TcParams p{};
+  p.unit_counter = unit_counter;
+  TcProblem& one = p.one;
+  one.m = (int)m;
+  one.KB = ix->dpu / kTcBKu;
+  one.n_tiles = (int)(ix->n_pad_tc / kTcBN);
+  one.tiles_per_split = (one.n_tiles + S - 1) / S;
+  one.exclude_self = exclude_self;
+  one.q_offset = q_offset;
+  one.nxu = ix->nxu;  // training order: the self column is the training row
+  one.sink = sa;
+  p.S = S;
+  p.m_tiles = (int)(m_pad / kTcBM);
+  p.status = status;
+  const int KB = one.KB;
+  const bool a_stream = KB > 4;
+  const int units = p.m_tiles * S;
+  const int grid = units < num_sms(ix->device) ? units : num_sms(ix->device);
+  if (grid <= 0) return 0;
+  TcMapSet<1> maps{};  // no norm-column maps: the epilogue adds ||x||^2
+  maps.a[0] = *tmap_a;
+  maps.b[0] = ix->tmap_bu;
+#define B2K_TC_LAUNCH_U8(SINK, EW)                                                 \
+  (a_stream ? launch_tc_variant<SINK, true, EW, false, kKindU8>(maps, p, KB, grid, st) \
+            : launch_tc_variant<SINK, false, EW, false, kKindU8>(maps, p, KB, grid, st))
+  return sa.k <= 8 ? B2K_TC_LAUNCH_U8(ExactU8Sink<8>, 16) : B2K_TC_LAUNCH_U8(ExactU8Sink<16>, 8);
+#undef B2K_TC_LAUNCH_U8
+}
+// u8 screen: 16 epilogue warps while the 8-wide heap fits their registers,
+// 8 warps (two TMEM loads in flight each) for k = 9..16
+int tc_u8_column_groups(int k) { return k <= 8 ? 4 : 2; }
 
 // Batched launches: kNN sinks only, with 4 or 8 epilogue warps.  Heap width
 // class 64 stands for the lazy tracker (every k > 16).

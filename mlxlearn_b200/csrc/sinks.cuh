@@ -150,6 +150,103 @@ struct RadiusListSink {
   B2K_DEV void finish(const SinkArgs& a) { a.rcount[slot] = cnt; }
 };
 
+// Exact kNN sink of the u8 screen: values are exact integers
+// v = ||x||^2 - 2<q, x>, so the list keeps just the k smallest (v, column)
+// in registers, ascending, equal values in column order.  Columns reach a
+// list in ascending order, so a value equal to the current k-th is never
+// better (a larger index); one equal to a k-th published by another list may
+// be (ties across lists are resolved by the merge), so the shared bound is
+// inclusive.  The padding rows' v is INT_MAX and never admitted.
+template <int KMAX>
+struct ExactU8Sink {
+  static constexpr bool kWarpWide = false;
+  int kv[KMAX], kc[KMAX];
+  int bound;          // admit v <= bound: min(k-th - 1, shared k-th)
+  int shared_v;       // smallest k-th published for this query (INT_MAX: none)
+  int self;
+  bool dirty;
+  uint32_t* shared;
+  size_t slot;
+  B2K_DEV static uint32_t key_of(int v) { return (uint32_t)v ^ 0x80000000u; }
+  B2K_DEV static int value_of(uint32_t key) { return (int)(key ^ 0x80000000u); }
+  B2K_DEV void init(const SinkArgs& a, int row, int split, float /*E*/, int self_col) {
+    slot = (size_t)split * a.out.m_pad + row;
+#pragma unroll
+    for (int i = 0; i < KMAX; ++i) {
+      // KMAX - k sentinels below every value, then k empty places
+      kv[i] = i < KMAX - a.k ? INT_MIN : INT_MAX;
+      kc[i] = -1;
+    }
+    shared_v = INT_MAX;
+    self = self_col;
+    dirty = false;
+    shared = a.shared_kth ? a.shared_kth + row : nullptr;
+    set_bound();
+    sync_shared();
+  }
+  B2K_DEV void set_bound() {
+    const int own = kv[KMAX - 1] == INT_MAX ? INT_MAX - 1 : kv[KMAX - 1] - 1;
+    bound = min(own, shared_v);
+  }
+  // x < kv[KMAX - 1]: insert after the values <= x
+  B2K_DEV void insert(int x, int c) {
+#pragma unroll
+    for (int i = KMAX - 1; i > 0; --i) {
+      const bool shift = kv[i - 1] > x, here = kv[i] > x;
+      const int nv = shift ? kv[i - 1] : (here ? x : kv[i]);
+      const int nc = shift ? kc[i - 1] : (here ? c : kc[i]);
+      kv[i] = nv;
+      kc[i] = nc;
+    }
+    if (kv[0] > x) {
+      kv[0] = x;
+      kc[0] = c;
+    }
+    dirty = true;
+    set_bound();
+  }
+  B2K_DEV void offer32i(const int (&v)[32], int col0) {
+    int a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = min(v[2 * i], v[2 * i + 1]);
+#pragma unroll
+    for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+      for (int i = 0; i < w; ++i) a[i] = min(a[i], a[i + w]);
+    if (a[0] <= bound) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (v[i] <= bound && col0 + i != self) insert(v[i], col0 + i);
+    }
+  }
+  B2K_DEV uint32_t fetch_shared() const {
+    uint32_t key = kNoKey;
+    if (shared) asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(key) : "l"(shared));
+    return key;
+  }
+  B2K_DEV void apply_shared(uint32_t key) {
+    if (!shared) return;
+    if (dirty && kv[KMAX - 1] != INT_MAX) {
+      atomicMin(shared, key_of(kv[KMAX - 1]));
+      dirty = false;
+    }
+    if (key != kNoKey && value_of(key) < shared_v) {
+      shared_v = value_of(key);
+      set_bound();
+    }
+  }
+  B2K_DEV void sync_shared() { apply_shared(fetch_shared()); }
+  B2K_DEV void tile_sync() { sync_shared(); }
+  B2K_DEV uint32_t tile_fetch() const { return fetch_shared(); }
+  B2K_DEV void tile_apply(uint32_t key) { apply_shared(key); }
+  B2K_DEV void finish(const SinkArgs& a) {
+    int2* out = a.out.lists + slot * a.out.cap;
+#pragma unroll
+    for (int i = 0; i < KMAX; ++i)
+      if (i >= KMAX - a.k) out[i - (KMAX - a.k)] = make_int2(kv[i], kc[i]);
+  }
+};
+
 // kNN sink for large k on the lazy tracker (tracker.cuh).  Warp-collective:
 // every lane of the warp calls every method, `active` false for rows past the
 // end of the query block; `hist` is the warp's 256-word shared scratch.

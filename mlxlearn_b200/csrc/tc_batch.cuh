@@ -28,6 +28,7 @@ struct TcProblem {
   const float* E;       // [m_pad] screen error bound per query row
   const int* perm;      // tile row -> original query row (or null)
   const int* self_col;  // training row -> its reference column (grouped operand), or null
+  const int* nxu;       // u8 screen: ||x||^2 per reference row (exact), else null
   SinkArgs sink;
 };
 
