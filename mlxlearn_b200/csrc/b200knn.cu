@@ -217,6 +217,9 @@ static int make_pivots(Index& ix) {
   ix.n_pivots = pivot_count(ix.n);
   B2K_CUDA(cudaMalloc(&ix.pivots, (size_t)ix.n_pivots * ix.d * sizeof(float)));
   B2K_CUDA(cudaMalloc(&ix.pivot_norms, (size_t)ix.n_pivots * sizeof(float)));
+  ix.pivot_dpa = pivot_dims_padded(ix.d);
+  B2K_CUDA(cudaMalloc(&ix.pivots_h,
+                      (size_t)pivot_rows_padded(ix.n_pivots) * ix.pivot_dpa * sizeof(uint16_t)));
   launch_pivots(&ix, ix.stream);
   B2K_CUDA(cudaGetLastError());
   B2K_CUDA(cudaStreamSynchronize(ix.stream));
@@ -977,6 +980,7 @@ int b2k_index_destroy(b2k_index* h) {
   cudaFree(ix.Xh);
   cudaFree(ix.pivots);
   cudaFree(ix.pivot_norms);
+  cudaFree(ix.pivots_h);
   cudaFree(ix.Xaug);
   cudaFree(ix.aug_ones);
   cudaFree(ix.xperm);

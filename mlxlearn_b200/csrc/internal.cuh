@@ -91,6 +91,8 @@ struct Index {
   int n_pivots = 0;
   float* pivots = nullptr;       // [n_pivots, d] centred rows
   float* pivot_norms = nullptr;  // [n_pivots]
+  uint16_t* pivots_h = nullptr;  // bf16 pivots for the assignment, zero padded:
+  int pivot_dpa = 0;             // [pivot_rows_padded(n_pivots), pivot_dpa]
   cudaStream_t stream = nullptr;
   std::mutex mu;
 };
@@ -187,6 +189,8 @@ int simt_column_groups(int sink_kind, bool noalloc = false);
 
 // ----------------------------------------------------------- query order
 int pivot_count(int64_t n);
+int pivot_rows_padded(int P);  // pivots padded to the assignment's tile
+int pivot_dims_padded(int d);  // features padded to its chunk
 void launch_pivots(Index* ix, cudaStream_t st);
 // perm[i] = original row of sorted position i; Qp = Q[perm]
 void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,

@@ -8,7 +8,8 @@
 // are close to each other makes their admissions coincide.
 //
 // Method: P pivots (every (n/P)-th training row), each query goes to its
-// nearest pivot (fp32 Gram form, the assignment only affects speed), then a
+// nearest pivot (bf16 Gram form on the tensor cores: the assignment only
+// affects speed, a near tie may go either way), then a
 // counting sort by pivot gives the permutation `perm` (sorted position ->
 // original query row) and the permuted query matrix.  Results are written
 // back to the original rows by the certify / exact kernels, so the answer
@@ -17,6 +18,8 @@
 // The same assignment groups the rows of the index's bf16 operand by pivot
 // (b200knn.cu): a tile of grouped queries then finds its candidates in a few
 // consecutive reference tiles, and the other tiles' chunks skip admission.
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -24,9 +27,10 @@ namespace b2k {
 
 namespace {
 
-constexpr int kPivTile = 32;     // pivots per shared-memory tile
-constexpr int kDChunk = 64;      // features per shared-memory chunk
-constexpr int kAssignThreads = 128;
+constexpr int kAssignThreads = 128;  // 4 warps x 32 queries
+constexpr int kMmaP = 64;            // pivots per shared-memory tile
+constexpr int kMmaK = 64;            // features per shared-memory chunk
+constexpr int kMmaLd = kMmaK + 8;    // padded row: conflict-free fragment loads
 
 __global__ void pivot_rows_kernel(const float* __restrict__ X, int64_t n, int d, int P,
                                   const float* __restrict__ center, float* __restrict__ piv,
@@ -44,98 +48,133 @@ __global__ void pivot_rows_kernel(const float* __restrict__ X, int64_t n, int d,
   if (threadIdx.x == 0) pnorm[p] = (float)s;
 }
 
-// 128 queries per block: argmin_p ||p||^2 - 2 <y_q, p>.  Per 32-pivot tile
-// warp w takes pivots [8w, 8w + 8) and lane l the queries l, l + 32, l + 64,
-// l + 96, so each feature step is 6 shared-memory loads (4 query values, two
-// 16-byte pivot loads) for 32 FMAs.  Each (query, pivot) sum runs over the
-// features in order, and ties go to the smaller pivot, so the keys do not
-// depend on this layout.
+// The bf16 copy of the pivots, [P_pad, dpa] (multiples of 64), zero padded.
+__global__ void pivots_bf16_kernel(const float* __restrict__ piv, int P, int d, int P_pad, int dpa,
+                                   uint16_t* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)P_pad * dpa) return;
+  const int p = (int)(i / dpa), f = (int)(i % dpa);
+  const float v = (p < P && f < d) ? piv[(size_t)p * d + f] : 0.0f;
+  out[i] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
+// D (16 x 8, fp32) += A (16 x 16, bf16, row major) * B (16 x 8, bf16, column major)
+__device__ __forceinline__ void mma_16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                          uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, "
+      "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// 128 queries per block: argmin_p ||p||^2 - 2 <y_q, p> with bf16 operands and
+// fp32 accumulation.  Warp w takes queries [32w, 32w + 32) (two 16-row
+// fragments) against each 64-pivot tile (eight 8-column fragments), the
+// features streamed through shared memory 64 at a time.  In a fragment of D,
+// lane (g = lane / 4, t = lane % 4) holds rows g and g + 8, columns 2t and
+// 2t + 1; it sees its pivots in ascending order and the quad's reduction
+// prefers the smaller pivot on equal values, so keys are deterministic.
 __global__ void __launch_bounds__(kAssignThreads)
     assign_kernel(const float* __restrict__ Q, int64_t m, int d, const float* __restrict__ center,
-                  const float* __restrict__ piv, const float* __restrict__ pnorm, int P,
-                  int* __restrict__ key, int* __restrict__ hist) {
-  __shared__ __align__(16) float sp[kDChunk][kPivTile];  // pivot tile, transposed
-  __shared__ float sq[kDChunk][kAssignThreads + 1];       // query tile, transposed
-  __shared__ float red_v[4][kAssignThreads];
-  __shared__ int red_p[4][kAssignThreads];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                  const uint16_t* __restrict__ piv_h, int dpa, const float* __restrict__ pnorm,
+                  int P, int* __restrict__ key, int* __restrict__ hist) {
+  __shared__ __align__(16) uint16_t sq[kAssignThreads][kMmaLd];
+  __shared__ __align__(16) uint16_t sp[kMmaP][kMmaLd];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int64_t q0 = (int64_t)blockIdx.x * kAssignThreads;
-  float best[4];
+  const int P_pad = (P + kMmaP - 1) / kMmaP * kMmaP;
+  float best[4];  // rows 32w + 16 (i / 2) + g + 8 (i % 2)
   int best_p[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     best[i] = INFINITY;
     best_p[i] = 0;
   }
-  for (int p0 = 0; p0 < P; p0 += kPivTile) {
-    float acc[4][8];
+  for (int p0 = 0; p0 < P_pad; p0 += kMmaP) {
+    float acc[2][8][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-    for (int k0 = 0; k0 < d; k0 += kDChunk) {
+      for (int b = 0; b < 8; ++b)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    for (int k0 = 0; k0 < dpa; k0 += kMmaK) {
       __syncthreads();
-      for (int i = threadIdx.x; i < kPivTile * kDChunk; i += kAssignThreads) {
-        const int j = i % kPivTile, k = i / kPivTile;
-        sp[k][j] = (p0 + j < P && k0 + k < d) ? piv[(size_t)(p0 + j) * d + k0 + k] : 0.0f;
-      }
       // coalesced: consecutive threads read consecutive features of one query
-      for (int i = threadIdx.x; i < kAssignThreads * kDChunk; i += kAssignThreads) {
-        const int r = i / kDChunk, k = i % kDChunk;
+      for (int i = threadIdx.x; i < kAssignThreads * kMmaK; i += kAssignThreads) {
+        const int r = i / kMmaK, k = i % kMmaK;
         const int64_t qr = q0 + r;
-        sq[k][r] = (qr < m && k0 + k < d) ? Q[qr * d + k0 + k] - center[k0 + k] : 0.0f;
+        const int f = k0 + k;
+        const float y = (qr < m && f < d) ? Q[qr * d + f] - center[f] : 0.0f;
+        sq[r][k] = __bfloat16_as_ushort(__float2bfloat16_rn(y));
+      }
+      for (int i = threadIdx.x; i < kMmaP * (kMmaK / 8); i += kAssignThreads) {
+        const int r = i / (kMmaK / 8), c8 = i % (kMmaK / 8);
+        *reinterpret_cast<uint4*>(&sp[r][c8 * 8]) =
+            *reinterpret_cast<const uint4*>(piv_h + (size_t)(p0 + r) * dpa + k0 + c8 * 8);
       }
       __syncthreads();
-      const int kend = min(kDChunk, d - k0);
-      for (int k = 0; k < kend; ++k) {
-        const float4 pa = *reinterpret_cast<const float4*>(&sp[k][8 * w]);
-        const float4 pb = *reinterpret_cast<const float4*>(&sp[k][8 * w + 4]);
-        const float pv[8] = {pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, pb.z, pb.w};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float y = sq[k][lane + 32 * i];
+      for (int kk = 0; kk < kMmaK; kk += 16) {
+        uint32_t a[2][4];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(y, pv[j], acc[i][j]);
+        for (int mt = 0; mt < 2; ++mt) {
+          const int r = 32 * w + 16 * mt + g;
+          a[mt][0] = *reinterpret_cast<const uint32_t*>(&sq[r][kk + 2 * t]);
+          a[mt][1] = *reinterpret_cast<const uint32_t*>(&sq[r + 8][kk + 2 * t]);
+          a[mt][2] = *reinterpret_cast<const uint32_t*>(&sq[r][kk + 2 * t + 8]);
+          a[mt][3] = *reinterpret_cast<const uint32_t*>(&sq[r + 8][kk + 2 * t + 8]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&sp[8 * nt + g][kk + 2 * t]);
+          const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&sp[8 * nt + g][kk + 2 * t + 8]);
+          mma_16816(acc[0][nt], a[0], b0, b1);
+          mma_16816(acc[1][nt], a[1], b0, b1);
         }
       }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int pj = p0 + 8 * w + j;
-      if (pj < P) {
-        const float pn = pnorm[pj];
+    for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float v = fmaf(-2.0f, acc[i][j], pn);
-          if (v < best[i]) {
-            best[i] = v;
-            best_p[i] = pj;
+      for (int e = 0; e < 4; ++e) {
+        const int pj = p0 + 8 * nt + 2 * t + (e & 1);
+        if (pj < P) {
+          const float pn = pnorm[pj];
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            const int i = 2 * mt + (e >> 1);
+            const float v = fmaf(-2.0f, acc[mt][nt][e], pn);
+            if (v < best[i]) {
+              best[i] = v;
+              best_p[i] = pj;
+            }
           }
         }
       }
-    }
   }
-  // each warp's best per query, then the smallest (value, pivot) over warps
+  // the quad's four lanes hold different pivots of the same rows
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    red_v[w][lane + 32 * i] = best[i];
-    red_p[w][lane + 32 * i] = best_p[i];
-  }
-  __syncthreads();
-  const int64_t q = q0 + threadIdx.x;
-  if (q < m) {
-    float bv = red_v[0][threadIdx.x];
-    int bp = red_p[0][threadIdx.x];
-    for (int ww = 1; ww < 4; ++ww) {
-      const float v = red_v[ww][threadIdx.x];
-      const int pp = red_p[ww][threadIdx.x];
-      if (v < bv || (v == bv && pp < bp)) {
-        bv = v;
-        bp = pp;
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, best[i], o);
+      const int op = __shfl_xor_sync(0xffffffffu, best_p[i], o);
+      if (ov < best[i] || (ov == best[i] && op < best_p[i])) {
+        best[i] = ov;
+        best_p[i] = op;
       }
     }
-    key[q] = bp;
-    atomicAdd(hist + bp, 1);
+  if (t == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t q = q0 + 32 * w + 16 * (i >> 1) + g + 8 * (i & 1);
+      if (q < m) {
+        key[q] = best_p[i];
+        atomicAdd(hist + best_p[i], 1);
+      }
+    }
   }
 }
 
@@ -217,16 +256,24 @@ int pivot_count(int64_t n) {
   return P;
 }
 
+int pivot_rows_padded(int P) { return (P + kMmaP - 1) / kMmaP * kMmaP; }
+int pivot_dims_padded(int d) { return (d + kMmaK - 1) / kMmaK * kMmaK; }
+
 void launch_pivots(Index* ix, cudaStream_t st) {
   pivot_rows_kernel<<<ix->n_pivots, 32, 0, st>>>(ix->X, ix->n, ix->d, ix->n_pivots, ix->center,
                                                  ix->pivots, ix->pivot_norms);
+  const int64_t total = (int64_t)pivot_rows_padded(ix->n_pivots) * ix->pivot_dpa;
+  pivots_bf16_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+      ix->pivots, ix->n_pivots, ix->d, pivot_rows_padded(ix->n_pivots), ix->pivot_dpa,
+      ix->pivots_h);
 }
 
 void launch_assign_rows(const Index* ix, const float* X, int64_t n, int* key, int* hist,
                         cudaStream_t st) {
   cudaMemsetAsync(hist, 0, (size_t)ix->n_pivots * sizeof(int), st);
   assign_kernel<<<(unsigned)((n + kAssignThreads - 1) / kAssignThreads), kAssignThreads, 0, st>>>(
-      X, n, ix->d, ix->center, ix->pivots, ix->pivot_norms, ix->n_pivots, key, hist);
+      X, n, ix->d, ix->center, ix->pivots_h, ix->pivot_dpa, ix->pivot_norms, ix->n_pivots, key,
+      hist);
 }
 
 void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, int* hist,
@@ -234,7 +281,7 @@ void launch_query_order(const Index* ix, const float* Q, int64_t m, int* key, in
   const int P = ix->n_pivots;
   cudaMemsetAsync(hist, 0, (size_t)P * sizeof(int), st);
   assign_kernel<<<(unsigned)((m + kAssignThreads - 1) / kAssignThreads), kAssignThreads, 0, st>>>(
-      Q, m, ix->d, ix->center, ix->pivots, ix->pivot_norms, P, key, hist);
+      Q, m, ix->d, ix->center, ix->pivots_h, ix->pivot_dpa, ix->pivot_norms, P, key, hist);
   bin_scan_kernel<<<1, 32, 0, st>>>(hist, P);
   scatter_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(key, m, hist, perm);
   gather_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(Q, perm, m, ix->d, Qp);
