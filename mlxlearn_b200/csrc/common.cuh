@@ -298,4 +298,39 @@ B2K_DEV double canonical_d2(const float* __restrict__ q, const float* __restrict
   return s;
 }
 
+// canonical_d2 of two rows against one query, the two sequential chains
+// interleaved so each covers the other's latency; each result is bit-identical
+// to canonical_d2(q, x, d).
+B2K_DEV void canonical_d2_pair(const float* __restrict__ q, const float* __restrict__ x0,
+                               const float* __restrict__ x1, int d, double& s0, double& s1) {
+  s0 = 0.0;
+  s1 = 0.0;
+  if ((d & 3) == 0 &&
+      ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(x0) |
+        reinterpret_cast<uintptr_t>(x1)) & 15) == 0) {
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* a4 = reinterpret_cast<const float4*>(x0);
+    const float4* b4 = reinterpret_cast<const float4*>(x1);
+    for (int i = 0; i < d / 4; ++i) {
+      const float4 c = q4[i], a = __ldg(a4 + i), b = __ldg(b4 + i);
+      const float cq[4] = {c.x, c.y, c.z, c.w}, xa[4] = {a.x, a.y, a.z, a.w},
+                  xb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double ta = __dsub_rn((double)cq[e], (double)xa[e]);
+        const double tb = __dsub_rn((double)cq[e], (double)xb[e]);
+        s0 = __dadd_rn(s0, __dmul_rn(ta, ta));
+        s1 = __dadd_rn(s1, __dmul_rn(tb, tb));
+      }
+    }
+    return;
+  }
+  for (int i = 0; i < d; ++i) {
+    const double ta = __dsub_rn((double)q[i], (double)x0[i]);
+    const double tb = __dsub_rn((double)q[i], (double)x1[i]);
+    s0 = __dadd_rn(s0, __dmul_rn(ta, ta));
+    s1 = __dadd_rn(s1, __dmul_rn(tb, tb));
+  }
+}
+
 }  // namespace b2k

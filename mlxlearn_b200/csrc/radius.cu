@@ -190,6 +190,18 @@ __device__ __forceinline__ bool key_le(const ExactKey& a, const ExactKey& b) {
 }
 
 // One warp per query row.
+// A row's candidates are contiguous across its lists (offsets in (row, list)
+// order): [roff[row], roff[row] + its total).
+__device__ __forceinline__ int64_t row_candidates(const ClassifyArgs& a, int64_t row,
+                                                  int64_t* base) {
+  *base = a.roff[row];
+  int64_t total = 0;
+  for (int s = 0; s < a.S; ++s) total += a.rcount[(size_t)s * a.m_pad + row];
+  return total;
+}
+
+// One warp per query row; each lane takes candidates i and i + 32 of every 64
+// together (two interleaved canonical chains).
 __global__ void classify_kernel(const ClassifyArgs a) {
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -199,34 +211,38 @@ __global__ void classify_kernel(const ClassifyArgs a) {
     return;
   }
   const float* q = a.Q + (size_t)row * a.d;
+  int64_t base;
+  const int64_t total = row_candidates(a, row, &base);
   int64_t members = 0;
   unsigned exact = 0;
-  for (int s = 0; s < a.S; ++s) {
-    const size_t slot = (size_t)s * a.m_pad + row;
-    const int64_t base = a.roff[slot];
-    const int cnt = a.rcount[slot];
-    for (int i = lane; i < cnt; i += 32) {
-      const int col = a.cols[base + i];
-      const float* x = a.X + (size_t)col * a.d;
-      double dist = -1.0;
-      if (a.all) {
-        dist = sqrt(canonical_d2(q, x, a.d));  // min(s, inf) = s
-      } else {
-        const double sv = canonical_d2(q, x, a.d);
-        bool in;
-        if (sv <= a.f_in) in = true;
-        else if (!(sv <= a.f_out)) in = false;
-        else if (a.r2_huge) in = true;
-        else {
-          ExactKey k;
-          exact_key(q, x, a.d, k);
-          in = key_le(k, a.r2key);
-          ++exact;
-        }
-        if (in) dist = sqrt(sv < a.R2 ? sv : a.R2);
-      }
-      a.cdist[base + i] = dist;
-      members += dist >= 0.0;
+  // member distance sqrt(min(s, R2)), or -1
+  auto classify = [&](const float* x, double sv) -> double {
+    if (a.all) return sqrt(sv);  // min(s, inf) = s
+    bool in;
+    if (sv <= a.f_in) in = true;
+    else if (!(sv <= a.f_out)) in = false;
+    else if (a.r2_huge) in = true;
+    else {
+      ExactKey k;
+      exact_key(q, x, a.d, k);
+      in = key_le(k, a.r2key);
+      ++exact;
+    }
+    return in ? sqrt(sv < a.R2 ? sv : a.R2) : -1.0;
+  };
+  for (int64_t i = lane; i < total; i += 64) {
+    const bool two = i + 32 < total;
+    const float* x0 = a.X + (size_t)a.cols[base + i] * a.d;
+    const float* x1 = two ? a.X + (size_t)a.cols[base + i + 32] * a.d : x0;
+    double s0, s1;
+    canonical_d2_pair(q, x0, x1, a.d, s0, s1);
+    const double d0 = classify(x0, s0);
+    a.cdist[base + i] = d0;
+    members += d0 >= 0.0;
+    if (two) {
+      const double d1 = classify(x1, s1);
+      a.cdist[base + i + 32] = d1;
+      members += d1 >= 0.0;
     }
   }
   for (int o = 16; o; o >>= 1) {
@@ -245,28 +261,25 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= a.m || call_failed(a.status, lane)) return;
+  int64_t base;
+  const int64_t total = row_candidates(a, row, &base);
   int64_t out = indptr[row];
-  for (int s = 0; s < a.S; ++s) {
-    const size_t slot = (size_t)s * a.m_pad + row;
-    const int64_t base = a.roff[slot];
-    const int cnt = a.rcount[slot];
-    for (int i0 = 0; i0 < cnt; i0 += 32) {
-      const int i = i0 + lane;
-      double dv = -1.0;
-      int col = 0;
-      if (i < cnt) {
-        dv = a.cdist[base + i];
-        col = a.cols[base + i];
-      }
-      const bool keep = dv >= 0.0;
-      const unsigned bal = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const int64_t pos = out + __popc(bal & ((1u << lane) - 1));
-        indices[pos] = col;
-        if (dist) dist[pos] = dv;
-      }
-      out += __popc(bal);
+  for (int64_t i0 = 0; i0 < total; i0 += 32) {
+    const int64_t i = i0 + lane;
+    double dv = -1.0;
+    int col = 0;
+    if (i < total) {
+      dv = a.cdist[base + i];
+      col = a.cols[base + i];
     }
+    const bool keep = dv >= 0.0;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int64_t pos = out + __popc(bal & ((1u << lane) - 1));
+      indices[pos] = col;
+      if (dist) dist[pos] = dv;
+    }
+    out += __popc(bal);
   }
 }
 

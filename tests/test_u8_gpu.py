@@ -59,6 +59,25 @@ def test_u8_ties_duplicates_and_self_query():
     check_u8(index, X, X, 7, exclude_self=True)
 
 
+def test_u8_self_query_with_offset_on_the_device():
+    """A slice of the training rows as queries: q_offset places each query's
+    own row, which the u8 screen excludes."""
+    import torch
+
+    rng = np.random.default_rng(34)
+    X = ints(rng, (12000, 40), hi=8)
+    X[6000:6040] = X[5000:5040]  # duplicates across the slice boundary
+    index = make_index(X)
+    Xd = torch.from_numpy(X).cuda()
+    for lo in (0, 4990, 9000):
+        dd, di = index.query_device(Xd[lo:lo + 3000], 9, exclude_self=True, q_offset=lo,
+                                    stats=True)
+        assert index.last_stats["mode_used"] == MODE_U8
+        od, oi = oracle.knn(X, X[lo:lo + 3000], 9, exclude_self=True, q_offset=lo)
+        np.testing.assert_array_equal(di.cpu().numpy(), oi)
+        np.testing.assert_array_equal(dd.cpu().numpy(), od)
+
+
 def test_u8_squared_distances_on_the_device():
     import torch
 
