@@ -641,9 +641,11 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     launch_prep_queries(&ix, Qs, m, m_pad, mode, qp, st);
     B2K_CUDA(cudaGetLastError());
     ScreenOut so{};
-    so.cap = kListCap;
+    // the register trackers' lists hold 4 x kListCap entries per (split, query)
+    // whatever the column groups (the lazy tracker's select is sized for kListCap)
+    so.cap = (tc && !tc_lazy_sink(k)) ? kListCap * 4 / tc_column_groups(k) : kListCap;
     so.m_pad = (int)m_pad;
-    if ((rc = dalloc(&so.lists, (size_t)S_lists * m_pad * kListCap, st))) return rc;
+    if ((rc = dalloc(&so.lists, (size_t)S_lists * m_pad * so.cap, st))) return rc;
     fr.keep(so.lists);
     if ((rc = dalloc(&so.counts, (size_t)S_lists * m_pad, st))) return rc;
     fr.keep(so.counts);
