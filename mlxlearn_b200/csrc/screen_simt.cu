@@ -125,11 +125,22 @@ __global__ void __launch_bounds__(kThreads, (sizeof(Sink) <= 160 ? 2 : 1))
         const float4 b0 = *reinterpret_cast<const float4*>(Bs + (buf * BK + kk) * LDB + tx * 4);
         const float4 a0 = ap[0], a1 = ap[1];
         const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-        const float bv[4] = {b0.x, b0.y, b0.z, b0.w};
+        // packed fp32 pairs: one fma.rn.f32x2 per two accumulators (each lane
+        // result is the same rounded FMA as fmaf), half the FMA instructions
+        uint64_t b01, b23;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(b01) : "f"(b0.x), "f"(b0.y));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(b23) : "f"(b0.z), "f"(b0.w));
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+        for (int a = 0; a < 8; ++a) {
+          uint64_t aa, c01, c23;
+          asm("mov.b64 %0, {%1, %1};" : "=l"(aa) : "f"(av[a]));
+          asm("mov.b64 %0, {%1, %2};" : "=l"(c01) : "f"(acc[a][0]), "f"(acc[a][1]));
+          asm("mov.b64 %0, {%1, %2};" : "=l"(c23) : "f"(acc[a][2]), "f"(acc[a][3]));
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(c01) : "l"(aa), "l"(b01));
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(c23) : "l"(aa), "l"(b23));
+          asm("mov.b64 {%0, %1}, %2;" : "=f"(acc[a][0]), "=f"(acc[a][1]) : "l"(c01));
+          asm("mov.b64 {%0, %1}, %2;" : "=f"(acc[a][2]), "=f"(acc[a][3]) : "l"(c23));
+        }
       }
       if (kc + 1 < nk) store_regs(buf ^ 1);
       __syncthreads();
