@@ -161,6 +161,7 @@ struct b2k_batch {
   unsigned long long* counters = nullptr;  // [4]
   uint32_t* skth = nullptr;   // [total_pad]
   float* E = nullptr;         // [total_pad]
+  double* nq = nullptr;       // [total_pad] ||q - c||^2 (certify's two-stage refinement)
   uint16_t* ones = nullptr;   // [128, 16]
   CUtensorMap m_ones;
   int64_t* pad_start = nullptr;  // [n_graph + 1]
@@ -275,6 +276,7 @@ int build_fixed(b2k_batch* b, cudaStream_t st) {
   if ((rc = o.alloc(&b->counters, 4))) return rc;
   if ((rc = o.alloc(&b->skth, (size_t)b->total_pad))) return rc;
   if ((rc = o.alloc(&b->E, (size_t)b->total_pad))) return rc;
+  if ((rc = o.alloc(&b->nq, (size_t)b->total_pad))) return rc;
   if ((rc = o.alloc(&b->pad_start, (size_t)P + 1))) return rc;
   if ((rc = o.alloc(&b->row_start, (size_t)P + 1))) return rc;
   if ((rc = o.alloc(&b->prep_tab, (size_t)P))) return rc;
@@ -305,7 +307,7 @@ int build_fixed(b2k_batch* b, cudaStream_t st) {
     q.ex_max = p.ex_max;
     q.E = b->E + p.pad0;
     q.Ah = g.A + (size_t)p.a_row0 * g.dp;
-    q.nq = nullptr;
+    q.nq = b->nq + p.pad0;
     q.flags = b->zero_block + 8 + p.gi;
     ExactArgs& e = ex[p.gi];
     e = ExactArgs{};
@@ -447,6 +449,7 @@ int build_tuned(b2k_batch* b, const std::map<TuneKey, Tuning>& tune, int gran,
       c.S = p.S_lists;
       c.scr = so;
       c.E = b->E + p.pad0;
+      c.nq = b->nq + p.pad0;  // two-stage refinement (certify.cu)
       c.dist = p.dist;
       c.idx = p.idx;
       c.fallback_list = b->fb_list;
