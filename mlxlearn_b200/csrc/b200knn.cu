@@ -349,6 +349,27 @@ static int ensure_tf32(Index& ix) {
   return B2K_OK;
 }
 
+// Whether every one of `count` values is an integer in [0, 255]: one check
+// kernel and a 4-byte read (the flag is freed on every path).
+static int all_u8(const float* v, int64_t count, cudaStream_t st, bool* yes) {
+  *yes = false;
+  int* flag = nullptr;
+  int rc = dalloc(&flag, 1, st);
+  if (rc) return rc;
+  int h = 1;
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    launch_u8_check(v, count, flag, st);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFreeAsync(flag, st);
+  if (e != cudaSuccess) return fail(B2K_ECUDA, "u8 check: %s", cudaGetErrorString(e));
+  *yes = h == 0;
+  return B2K_OK;
+}
+
 // The exact u8 screen's operand, when every training coordinate is an
 // integer in [0, 255] (checked once); *ok tells whether the index qualifies.
 static int ensure_u8(Index& ix, bool* ok) {
@@ -356,19 +377,26 @@ static int ensure_u8(Index& ix, bool* ok) {
   *ok = false;
   if (ix.d > kU8MaxD) return B2K_OK;
   cudaStream_t st = ix.stream;
+  int rc;
   if (ix.u8_state == 0) {
-    int* flag = nullptr;
-    B2K_CUDA(cudaMalloc(&flag, sizeof(int)));
-    B2K_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
-    launch_u8_check(ix.X, ix.n * (int64_t)ix.d, flag, st);
-    int h = 1;
-    B2K_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-    B2K_CUDA(cudaStreamSynchronize(st));
-    cudaFree(flag);
-    ix.u8_state = h ? -1 : 1;
+    bool yes = false;
+    if ((rc = all_u8(ix.X, ix.n * (int64_t)ix.d, st, &yes))) return rc;
+    ix.u8_state = yes ? 1 : -1;
   }
   if (ix.u8_state < 0) return B2K_OK;
   if (!ix.u8_ready) {
+    // a failed build leaves nothing allocated, so a later call starts over
+    struct Partial {
+      Index& ix;
+      bool done = false;
+      ~Partial() {
+        if (done) return;
+        cudaFree(ix.Xu);
+        cudaFree(ix.nxu);
+        ix.Xu = nullptr;
+        ix.nxu = nullptr;
+      }
+    } partial{ix};
     ix.dpu = (int32_t)round_up(ix.d, kTcBKu);
     ix.n_pad_tc = round_up(ix.n, kTcBN);
     B2K_CUDA(cudaMalloc(&ix.Xu, (size_t)ix.n_pad_tc * ix.dpu));
@@ -380,6 +408,7 @@ static int ensure_u8(Index& ix, bool* ok) {
     if (!tensor_map_2d(&ix.tmap_bu, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix.Xu, (uint64_t)ix.dpu,
                        (uint64_t)ix.n_pad_tc, kTcBKu, kTcBN, 128))
       return fail(B2K_ECUDA, "cuTensorMapEncodeTiled failed for the u8 operand");
+    partial.done = true;
     ix.u8_ready = true;
   }
   *ok = true;
@@ -532,15 +561,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if ((rc = ensure_u8(ix, &ok))) return rc;
     if (ok) {
       cudaSetDevice(ix.device);
-      int* flag = nullptr;
-      if ((rc = dalloc(&flag, 1, st))) return rc;
-      B2K_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
-      launch_u8_check(dQ, m * (int64_t)ix.d, flag, st);
-      int h = 1;
-      B2K_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-      B2K_CUDA(cudaStreamSynchronize(st));
-      cudaFreeAsync(flag, st);
-      ok = h == 0;
+      if ((rc = all_u8(dQ, m * (int64_t)ix.d, st, &ok))) return rc;
     }
     u8 = ok;
   }
