@@ -1230,12 +1230,13 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   fr.keep(cand);
   if (cap) {
     launch_radius_pack(sa.rcols, cap, sa.rcount, S_lists, m, m_pad, roff,
-                       grouped ? ix.xperm : nullptr, cand, status, st);
+                       grouped ? ix.xperm : nullptr, cand, ncand, status, st);
   } else {
     sa.rcols = cand;
     if ((rc = screen(kSinkRadiusFill))) return rc;
     if (grouped)
-      launch_radius_pack(cand, 0, sa.rcount, S_lists, m, m_pad, roff, ix.xperm, cand, status, st);
+      launch_radius_pack(cand, 0, sa.rcount, S_lists, m, m_pad, roff, ix.xperm, cand, ncand,
+                         status, st);
   }
   const bool unordered = grouped || S_lists > S;
   const bool keep_dist = need_distance || sort_results;
@@ -1250,6 +1251,8 @@ static int radius_block(Index& ix, const float* dQ, int64_t m, double R2, int ex
   ra.roff = roff;
   ra.rcount = sa.rcount;
   ra.cols = cand;
+  // long rows (an overflow sub-call's) take a CTA each in classify and compact
+  ra.wide = ncand >= (int64_t)kWideRowCandidates * m;
   ra.R2 = R2;
   ra.exact_tests = counters;
   ra.status = status;

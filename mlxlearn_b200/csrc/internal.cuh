@@ -261,6 +261,9 @@ void launch_exact_batch(const ExactArgs* tab, const int64_t* row_start, int P, c
                         cudaStream_t st);
 
 // ------------------------------------------------------------------ radius
+// Average candidates per row from which classify and compact take one CTA
+// per row instead of one warp.
+constexpr int kWideRowCandidates = 512;
 struct RadiusPlanArgs {
   const float* X;
   const float* Q;
@@ -270,6 +273,7 @@ struct RadiusPlanArgs {
   const int64_t* roff;   // [S][m_pad] candidate offsets
   const int* rcount;     // [S][m_pad] candidate counts
   const int* cols;       // candidates (training rows) at roff
+  bool wide;             // one CTA per row (long rows), else one warp per row
   double* cdist;         // [ncand] member distance or -1
   int64_t* mcount;       // [m] members per query
   double R2;
@@ -293,10 +297,11 @@ void launch_radius_overflow(int* rcount, int S, int64_t m, int64_t m_pad, int ca
 // Candidates to one array at their scanned offsets roff, as training rows
 // (xperm: grouped operand rows, else null).  src: lists of `cap` entries at
 // slot * cap (single pass), or cap = 0 and src == dst (counted form: the
-// fill's candidates translated in place).  Nothing when *status is an error.
+// fill's `count` candidates translated in place).  Nothing when *status is an
+// error.
 void launch_radius_pack(const int* src, int cap, const int* rcount, int S, int64_t m,
                         int64_t m_pad, const int64_t* roff, const int* xperm, int* dst,
-                        const int* status, cudaStream_t st);
+                        int64_t count, const int* status, cudaStream_t st);
 // mcount[rows[i]] = sub_indptr[i + 1] - sub_indptr[i]: members of the rows a
 // counted sub-call answered
 void launch_radius_sub_counts(const int* rows, int count, const int64_t* sub_indptr,

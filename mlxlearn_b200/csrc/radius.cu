@@ -200,6 +200,48 @@ __device__ __forceinline__ int64_t row_candidates(const ClassifyArgs& a, int64_t
   return total;
 }
 
+// Member distance sqrt(min(s, R2)) of candidate row x with canonical value
+// sv, or -1 for a non-member; band cases take the exact key (counted).
+__device__ __forceinline__ double classify_one(const ClassifyArgs& a, const float* q,
+                                               const float* x, double sv, unsigned& exact) {
+  if (a.all) return sqrt(sv);  // min(s, inf) = s
+  bool in;
+  if (sv <= a.f_in) in = true;
+  else if (!(sv <= a.f_out)) in = false;
+  else if (a.r2_huge) in = true;
+  else {
+    ExactKey k;
+    exact_key(q, x, a.d, k);
+    in = key_le(k, a.r2key);
+    ++exact;
+  }
+  return in ? sqrt(sv < a.R2 ? sv : a.R2) : -1.0;
+}
+
+// Candidates [i0, total) of a row with step `stride`, two per thread at a
+// time (i and i + stride, interleaved canonical chains); returns the members.
+__device__ __forceinline__ int64_t classify_range(const ClassifyArgs& a, const float* q,
+                                                  int64_t base, int64_t i0, int64_t total,
+                                                  int stride, unsigned& exact) {
+  int64_t members = 0;
+  for (int64_t i = i0; i < total; i += 2 * (int64_t)stride) {
+    const bool two = i + stride < total;
+    const float* x0 = a.X + (size_t)a.cols[base + i] * a.d;
+    const float* x1 = two ? a.X + (size_t)a.cols[base + i + stride] * a.d : x0;
+    double s0, s1;
+    canonical_d2_pair(q, x0, x1, a.d, s0, s1);
+    const double d0 = classify_one(a, q, x0, s0, exact);
+    a.cdist[base + i] = d0;
+    members += d0 >= 0.0;
+    if (two) {
+      const double d1 = classify_one(a, q, x1, s1, exact);
+      a.cdist[base + i + stride] = d1;
+      members += d1 >= 0.0;
+    }
+  }
+  return members;
+}
+
 // One warp per query row; each lane takes candidates i and i + 32 of every 64
 // together (two interleaved canonical chains).
 __global__ void classify_kernel(const ClassifyArgs a) {
@@ -213,38 +255,8 @@ __global__ void classify_kernel(const ClassifyArgs a) {
   const float* q = a.Q + (size_t)row * a.d;
   int64_t base;
   const int64_t total = row_candidates(a, row, &base);
-  int64_t members = 0;
   unsigned exact = 0;
-  // member distance sqrt(min(s, R2)), or -1
-  auto classify = [&](const float* x, double sv) -> double {
-    if (a.all) return sqrt(sv);  // min(s, inf) = s
-    bool in;
-    if (sv <= a.f_in) in = true;
-    else if (!(sv <= a.f_out)) in = false;
-    else if (a.r2_huge) in = true;
-    else {
-      ExactKey k;
-      exact_key(q, x, a.d, k);
-      in = key_le(k, a.r2key);
-      ++exact;
-    }
-    return in ? sqrt(sv < a.R2 ? sv : a.R2) : -1.0;
-  };
-  for (int64_t i = lane; i < total; i += 64) {
-    const bool two = i + 32 < total;
-    const float* x0 = a.X + (size_t)a.cols[base + i] * a.d;
-    const float* x1 = two ? a.X + (size_t)a.cols[base + i + 32] * a.d : x0;
-    double s0, s1;
-    canonical_d2_pair(q, x0, x1, a.d, s0, s1);
-    const double d0 = classify(x0, s0);
-    a.cdist[base + i] = d0;
-    members += d0 >= 0.0;
-    if (two) {
-      const double d1 = classify(x1, s1);
-      a.cdist[base + i + 32] = d1;
-      members += d1 >= 0.0;
-    }
-  }
+  int64_t members = classify_range(a, q, base, lane, total, 32, exact);
   for (int o = 16; o; o >>= 1) {
     members += __shfl_xor_sync(0xffffffffu, members, o);
     exact += __shfl_xor_sync(0xffffffffu, exact, o);
@@ -281,6 +293,105 @@ __global__ void compact_kernel(const ClassifyArgs a, const int64_t* __restrict__
     }
     out += __popc(bal);
   }
+}
+
+// Long rows (the overflow sub-call's rows hold thousands of candidates):
+// one CTA per row, so a few rows still spread over the whole GPU.
+constexpr int kWideThreads = 256;
+
+// The call's error word, read once by thread 0 and shared with the block.
+__device__ __forceinline__ bool block_failed(const int* status, int* s_flag) {
+  if (threadIdx.x == 0) *s_flag = *reinterpret_cast<volatile const int*>(status);
+  __syncthreads();
+  return *s_flag != DEV_OK;
+}
+
+__global__ void __launch_bounds__(kWideThreads) classify_wide_kernel(const ClassifyArgs a) {
+  __shared__ int s_flag;
+  __shared__ long long s_members[kWideThreads / 32];
+  __shared__ unsigned s_exact[kWideThreads / 32];
+  const int64_t row = blockIdx.x;  // grid = m: every thread of the block has a row
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (block_failed(a.status, &s_flag)) {
+    if (threadIdx.x == 0) a.mcount[row] = 0;
+    return;
+  }
+  const float* q = a.Q + (size_t)row * a.d;
+  int64_t base;
+  const int64_t total = row_candidates(a, row, &base);
+  unsigned exact = 0;
+  int64_t members = classify_range(a, q, base, threadIdx.x, total, kWideThreads, exact);
+  for (int o = 16; o; o >>= 1) {
+    members += __shfl_xor_sync(0xffffffffu, members, o);
+    exact += __shfl_xor_sync(0xffffffffu, exact, o);
+  }
+  if (lane == 0) {
+    s_members[w] = members;
+    s_exact[w] = exact;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long mm = 0;
+    unsigned ee = 0;
+    for (int i = 0; i < kWideThreads / 32; ++i) {
+      mm += s_members[i];
+      ee += s_exact[i];
+    }
+    a.mcount[row] = mm;
+    if (ee) atomicAdd(a.exact_tests, (unsigned long long)ee);
+  }
+}
+
+// One CTA per row, order preserved: warp w compacts the w-th contiguous chunk
+// of the row's candidates at the members counted before it.
+__global__ void __launch_bounds__(kWideThreads)
+    compact_wide_kernel(const ClassifyArgs a, const int64_t* __restrict__ indptr,
+                        int64_t* __restrict__ indices, double* __restrict__ dist) {
+  constexpr int kWarps = kWideThreads / 32;
+  __shared__ int s_flag;
+  __shared__ long long s_cnt[kWarps];
+  const int64_t row = blockIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (block_failed(a.status, &s_flag)) return;
+  int64_t base;
+  const int64_t total = row_candidates(a, row, &base);
+  const int64_t chunk = ((total + kWarps - 1) / kWarps + 31) / 32 * 32;
+  const int64_t lo = min(total, w * chunk), hi = min(total, lo + chunk);
+  long long cnt = 0;
+  for (int64_t i0 = lo; i0 < hi; i0 += 32) {
+    const int64_t i = i0 + lane;
+    cnt += __popc(__ballot_sync(0xffffffffu, i < hi && a.cdist[base + i] >= 0.0));
+  }
+  if (lane == 0) s_cnt[w] = cnt;
+  __syncthreads();
+  int64_t out = indptr[row];
+  for (int i = 0; i < w; ++i) out += s_cnt[i];
+  for (int64_t i0 = lo; i0 < hi; i0 += 32) {
+    const int64_t i = i0 + lane;
+    double dv = -1.0;
+    int col = 0;
+    if (i < hi) {
+      dv = a.cdist[base + i];
+      col = a.cols[base + i];
+    }
+    const bool keep = dv >= 0.0;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int64_t pos = out + __popc(bal & ((1u << lane) - 1));
+      indices[pos] = col;
+      if (dist) dist[pos] = dv;
+    }
+    out += __popc(bal);
+  }
+}
+
+// Candidates already at their offsets to training rows, in place, one thread
+// per entry (the counted form's fill pass on grouped operand rows).
+__global__ void translate_kernel(int* cand, int64_t count, const int* __restrict__ xperm,
+                                 const int* __restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (*reinterpret_cast<volatile const int*>(status) != DEV_OK) return;
+  if (i < count) cand[i] = __ldg(xperm + cand[i]);
 }
 
 // One thread per row: a row whose count passed the list capacity in any of
@@ -611,6 +722,10 @@ void launch_classify(const RadiusPlanArgs& r, cudaStream_t st) {
   a.status = r.status;
   radius_band(r.d, r.R2, &a.f_in, &a.f_out, &a.all, &a.r2_huge, a.r2key.w);
   if (r.m <= 0) return;
+  if (r.wide) {
+    classify_wide_kernel<<<(unsigned)r.m, kWideThreads, 0, st>>>(a);
+    return;
+  }
   const int warps = 8;
   classify_kernel<<<(unsigned)((r.m + warps - 1) / warps), warps * 32, 0, st>>>(a);
 }
@@ -627,6 +742,10 @@ void launch_compact(const RadiusPlanArgs& r, const int64_t* indptr, int64_t* ind
   a.cdist = r.cdist;
   a.status = r.status;
   if (r.m <= 0) return;
+  if (r.wide) {
+    compact_wide_kernel<<<(unsigned)r.m, kWideThreads, 0, st>>>(a, indptr, indices, dist);
+    return;
+  }
   const int warps = 8;
   compact_kernel<<<(unsigned)((r.m + warps - 1) / warps), warps * 32, 0, st>>>(a, indptr,
                                                                                  indices, dist);
@@ -641,8 +760,15 @@ void launch_radius_overflow(int* rcount, int S, int64_t m, int64_t m_pad, int ca
 
 void launch_radius_pack(const int* src, int cap, const int* rcount, int S, int64_t m,
                         int64_t m_pad, const int64_t* roff, const int* xperm, int* dst,
-                        const int* status, cudaStream_t st) {
+                        int64_t count, const int* status, cudaStream_t st) {
   if (m <= 0) return;
+  if (cap == 0) {  // in place: one thread per entry
+    if (src != dst || !xperm) return;
+    if (count > 0)
+      translate_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(dst, count, xperm,
+                                                                         status);
+    return;
+  }
   radius_pack_kernel<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(src, cap, rcount, S, m, m_pad,
                                                              roff, xperm, dst, status);
 }
