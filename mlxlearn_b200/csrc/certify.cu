@@ -179,6 +179,20 @@ __device__ uint32_t warp_radix_select(Visit visit, int k, unsigned* hist, int la
   return prefix;
 }
 
+// k-th smallest (1-based, k <= n) of n <= 32 keys, lane l holding key l
+// (lanes >= n hold anything): every lane counts the keys below its own (ties
+// by lane), and the lane of rank k - 1 holds the answer.
+__device__ __forceinline__ uint32_t warp_kth_32(uint32_t key, int n, int k, int lane) {
+  int rank = 0;
+#pragma unroll 8
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t o = __shfl_sync(0xffffffffu, key, j);
+    rank += (j < n && (o < key || (o == key && j < lane))) ? 1 : 0;
+  }
+  const unsigned hit = __ballot_sync(0xffffffffu, lane < n && rank == k - 1);
+  return __shfl_sync(0xffffffffu, key, __ffs(hit) - 1);
+}
+
 template <class KeyFn>
 __device__ uint32_t warp_radix_kth(KeyFn key_of, int count, int k, unsigned* hist, int lane) {
   return warp_radix_select(
@@ -292,15 +306,19 @@ __device__ __forceinline__ void refine_fp32(const float* __restrict__ q,
 // certified lower bound above the k-th smallest upper bound of the refined
 // ones, so it could not have survived.  `sa` / `av` are scratch for at most
 // kSurvivorCap stage-one candidates.
+// U0 (out): the k-th smallest fp32 upper bound of the stage-one candidates,
+// INFINITY when the refinement ran in one stage.
 __device__ __forceinline__ int refine_candidates(const CertifyArgs& a, int64_t row,
                                                  const float* q, int* ci, float* cv, int* sa,
                                                  float* av, unsigned* hist, int C, float up_f,
-                                                 float abs32, int lane) {
+                                                 float abs32, float Vk, float* U0out, int lane) {
   const int k = a.k;
+  *U0out = INFINITY;
   if (a.nq && C >= 4 * k) {
-    // stage one: the candidates whose screen value is at most the k-th smallest
-    const float Vsel =
-        key_float(warp_radix_kth([&](int c) { return float_key(cv[c]); }, C, k, hist, lane));
+    // stage one: the candidates whose screen value is at most the k-th
+    // smallest, which is V_k itself: the k smallest screen values of the query
+    // are in its lists' k smallest (and all of them are <= Tf, so listed here)
+    const float Vsel = Vk;
     int nA = 0;
     for (int base = 0; base < C; base += 32) {
       const int c = base + lane;
@@ -314,9 +332,11 @@ __device__ __forceinline__ int refine_candidates(const CertifyArgs& a, int64_t r
       __syncwarp();
       refine_fp32(q, a.X, a.d, sa, av, nA, lane);
       __syncwarp();
-      const float U0 = key_float(warp_radix_kth(
-          [&](int j) { return float_key(__fadd_ru(__fmul_ru(av[j], up_f), abs32)); }, nA, k,
-          hist, lane));
+      auto upper_key = [&](int j) { return float_key(__fadd_ru(__fmul_ru(av[j], up_f), abs32)); };
+      const float U0 = key_float(
+          nA <= 32 ? warp_kth_32(lane < nA ? upper_key(lane) : 0u, nA, k, lane)
+                   : warp_radix_kth(upper_key, nA, k, hist, lane));
+      *U0out = U0;
       // stage two: the other candidates whose screen lower bound
       // ||y_q||^2 + v - E (rounded down) reaches U0, compacted in place
       const double nq = a.nq[row], E = (double)a.E[row];
@@ -412,7 +432,30 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
       keys[i] = float_key(so.kth[((size_t)s * so.m_pad + row) * k + t]);
     }
     __syncwarp();
-    Vk = key_float(warp_radix_kth([&](int i) { return keys[i]; }, total, k, hist, lane));
+    if (S <= 32) {
+      // each list's k values ascend: k rounds of a warp minimum over the
+      // lists' heads (lane s walks list s), the k-th winner is V_k
+      int p = 0;
+      uint32_t head = lane < S ? keys[lane * k] : 0xffffffffu, kth_key = 0;
+      for (int t = 0; t < k; ++t) {
+        uint32_t mv = head;
+        int ml = lane;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          const uint32_t ov = __shfl_xor_sync(0xffffffffu, mv, o);
+          const int ol = __shfl_xor_sync(0xffffffffu, ml, o);
+          if (ov < mv || (ov == mv && ol < ml)) {
+            mv = ov;
+            ml = ol;
+          }
+        }
+        kth_key = mv;
+        if (lane == ml) head = ++p < k ? keys[lane * k + p] : 0xffffffffu;
+      }
+      Vk = key_float(kth_key);
+    } else {
+      Vk = key_float(warp_radix_kth([&](int i) { return keys[i]; }, total, k, hist, lane));
+    }
     __syncwarp();
   } else {
     Vk = key_float(warp_radix_kth(
@@ -424,38 +467,44 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   }
   const float Tf = __fadd_ru(Vk, __fmul_ru(2.0f, a.E[row]));
 
-  // 3. gather candidates v <= Tf
+  // 3. gather candidates v <= Tf.  Each lane keeps four list entries in
+  // flight (the loop is bound by their latency), and the columns of grouped
+  // operand rows are mapped to training rows afterwards, all at once.
   int C = 0;
   bool too_many = false;
+  constexpr int kAhead = 4;
   for (int s = 0; s < S && !too_many; ++s) {
     const size_t slot = (size_t)s * so.m_pad + row;
     const int cnt = so.counts[slot];
     const int2* lst = so.lists + slot * so.cap;
-    for (int base = 0; base < cnt; base += 32) {
-      const int i = base + lane;
-      bool pass = false;
-      int col = 0;
-      float v = 0.0f;
-      if (i < cnt) {
-        const int2 e = lst[i];
-        v = __int_as_float(e.x);
-        pass = v <= Tf;
-        col = e.y;
+    for (int base = 0; base < cnt && !too_many; base += 32 * kAhead) {
+      int2 e[kAhead];
+#pragma unroll
+      for (int u = 0; u < kAhead; ++u) {
+        const int i = base + 32 * u + lane;
+        e[u] = i < cnt ? lst[i] : make_int2(0, 0);
       }
-      const unsigned bal = __ballot_sync(0xffffffffu, pass);
-      const int pos = C + __popc(bal & ((1u << lane) - 1));
-      // grouped operand rows: the list holds operand rows, the answer training rows
-      if (pass && a.cols) col = __ldg(a.cols + col);
-      if (pass && pos < kCertifyCap) {
-        ci[pos] = col;
-        cv[pos] = v;  // the screen value until the refinement overwrites it
+#pragma unroll
+      for (int u = 0; u < kAhead; ++u) {
+        const int i = base + 32 * u + lane;
+        const float v = __int_as_float(e[u].x);
+        const bool pass = i < cnt && v <= Tf;
+        const unsigned bal = __ballot_sync(0xffffffffu, pass);
+        const int pos = C + __popc(bal & ((1u << lane) - 1));
+        if (pass && pos < kCertifyCap) {
+          ci[pos] = e[u].y;
+          cv[pos] = v;  // the screen value until the refinement overwrites it
+        }
+        C += __popc(bal);
       }
-      C += __popc(bal);
-      if (C > kCertifyCap) {
-        too_many = true;
-        break;
-      }
+      too_many = C > kCertifyCap;
     }
+  }
+  // grouped operand rows: the lists hold operand rows, the answer training rows
+  if (!too_many && a.cols) {
+    __syncwarp();
+#pragma unroll 4
+    for (int c = lane; c < C; c += 32) ci[c] = __ldg(a.cols + ci[c]);
   }
   if (too_many || C < k) {
     if (lane == 0) a.fallback_list[atomicAdd(a.fallback_count, 1)] = (int)(a.row_base + row);
@@ -467,12 +516,39 @@ __device__ __forceinline__ void certify_row(const CertifyArgs& a, int64_t row, u
   const float g32 = (float)((double)(a.d + 5) * 0x1p-24 * 1.01);
   const float abs32 = (float)a.d * 0x1p-126f;
   const float up_f = 1.0f + g32, lo_f = 1.0f - g32;
+  float U0;
   const int Cr = refine_candidates(a, row, q, ci, cv, si, reinterpret_cast<float*>(cs), hist, C,
-                                   up_f, abs32, lane);
-  // 5. U = k-th smallest upper bound (radix select over ordered keys)
-  const float U = key_float(warp_radix_kth(
-      [&](int c) { return float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)); }, Cr, k, hist,
-      lane));
+                                   up_f, abs32, Vk, &U0, lane);
+  // 5. U = k-th smallest upper bound.  After a two-stage refinement the
+  // stage-one candidates (among the refined) put k upper bounds at or below
+  // U0, so only those bounds can be the k-th smallest: when at most 32, a
+  // rank select among them; otherwise a radix select over all.
+  auto upper_key = [&](int c) { return float_key(__fadd_ru(__fmul_ru(cv[c], up_f), abs32)); };
+  uint32_t Ukey = 0;
+  bool small = false;
+  if (U0 < INFINITY) {
+    // the keys <= U0, gathered through the survivor scratch (free until step 6)
+    uint32_t* tmp = reinterpret_cast<uint32_t*>(si);
+    const uint32_t u0 = float_key(U0);
+    int n = 0;
+    for (int base = 0; base < Cr && n <= 32; base += 32) {
+      const int c = base + lane;
+      const uint32_t key = c < Cr ? upper_key(c) : 0xffffffffu;
+      const bool le = c < Cr && key <= u0;
+      const unsigned bal = __ballot_sync(0xffffffffu, le);
+      const int pos = n + __popc(bal & ((1u << lane) - 1));
+      if (le && pos < 32) tmp[pos] = key;
+      n += __popc(bal);
+    }
+    __syncwarp();
+    if (n <= 32 && n >= k) {
+      Ukey = warp_kth_32(lane < n ? tmp[lane] : 0u, n, k, lane);
+      small = true;
+    }
+    __syncwarp();
+  }
+  if (!small) Ukey = warp_radix_kth(upper_key, Cr, k, hist, lane);
+  const float U = key_float(Ukey);
   // 6. survivors: lower bound <= U (everything that can still be in the top k)
   int Cs = 0;
   for (int base = 0; base < Cr; base += 32) {
