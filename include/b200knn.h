@@ -75,6 +75,8 @@ typedef struct b2k_stats {
   double screen_ms;         /* device time of the screen kernel (if timed)     */
   double total_ms;          /* device time of the whole call (if timed)        */
   int64_t refined;          /* candidates refined in fp32 by the certify pass  */
+  double seed_ms;           /* device time of the screen's seeding pass, which
+                               screen_ms includes (0: no seeding pass)        */
 } b2k_stats;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -48,6 +48,7 @@ class Stats(ctypes.Structure):
         ("screen_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
         ("refined", ctypes.c_int64),
+        ("seed_ms", ctypes.c_double),
     ]
 
     def as_dict(self):

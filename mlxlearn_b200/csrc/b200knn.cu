@@ -579,7 +579,9 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
   if (m == 0) return B2K_OK;
   cudaSetDevice(ix.device);
   StreamFree fr{st, {}};
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // call start, screen start, screen end, call end, seeding pass end
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool seeded = false;
   if (stats)
     for (auto& e : ev) cudaEventCreate(&e);
   if (stats) cudaEventRecord(ev[0], st);
@@ -720,6 +722,8 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
                                   kSeedTiles);
         if (lr) return fail(B2K_ECUDA, "tcgen05 seeding screen launch failed: %s",
                             cudaGetErrorString((cudaError_t)lr));
+        if (stats) cudaEventRecord(ev[4], st);
+        seeded = true;
       }
       // status[6] (zeroed above) counts the claimed work units
       int lr = launch_screen_tc(&ix, &tmap_a, m, m_pad, exclude_self, q_offset, S, qp.E,
@@ -823,6 +827,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
     if (mode != B2K_MODE_EXACT && cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess)
       stats->screen_ms = ms;
     if (cudaEventElapsedTime(&ms, ev[0], ev[3]) == cudaSuccess) stats->total_ms = ms;
+    if (seeded && cudaEventElapsedTime(&ms, ev[1], ev[4]) == cudaSuccess) stats->seed_ms = ms;
     for (auto& e : ev) cudaEventDestroy(e);
   }
   return B2K_OK;
