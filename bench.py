@@ -75,32 +75,51 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region.
+
+    Samples are stamped with the host clock as they arrive (every 50 ms);
+    `begin()` / `end()` mark the timed region and `summary()` keeps the
+    samples inside it (all samples when the region caught none)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
         self.lines = []
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the sampler is live before the caller's work starts
+            deadline = time.perf_counter() + 3.0
+            while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def begin(self):
+        self.window = [time.perf_counter(), None]
+
+    def end(self):
+        if self.window is not None:
+            # one more interval: the sample taken while the last step ran
+            time.sleep(self.INTERVAL_MS / 1000.0)
+            self.window[1] = time.perf_counter()
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -111,9 +130,16 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        lines = self.lines
+        in_window = False
+        if self.window is not None and self.window[1] is not None:
+            t0, t1 = self.window
+            inside = [(t, ln) for t, ln in lines if t0 <= t <= t1]
+            if inside:
+                lines, in_window = inside, True
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for _, line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -128,7 +154,8 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "timed_region_only": in_window, "interval_ms": self.INTERVAL_MS}
 
 
 def dist_env():
@@ -358,25 +385,29 @@ def run_ours(args):
             pg.barrier()
         torch.cuda.synchronize()
 
-    def timed(mode, steps, warmup):
+    def timed(mode, steps, warmup, clk=None):
         stats = []
         for _ in range(warmup):
             index.query_device(Qd, K, mode=mode)
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if clk is not None:
+            clk.begin()
         ev0.record(stream)
         for _ in range(steps):
             index.query_device(Qd, K, mode=mode, stats=True)
             stats.append(index.last_stats)
         ev1.record(stream)
         barrier()
+        if clk is not None:
+            clk.end()
         ms = ev0.elapsed_time(ev1) / steps
         if pg is not None:
             ms = max_over_ranks(ms)
         return ms, stats
 
     with ClockSampler(local) as clk:
-        ms_bf16, st_bf16 = timed("bf16", args.steps, args.warmup)
+        ms_bf16, st_bf16 = timed("bf16", args.steps, args.warmup, clk)
     clocks = clk.summary()
     ms_fp32, st_fp32 = timed("fp32", max(1, min(2, args.steps)), 1)
     ms_tf32, st_tf32 = timed("tf32", max(1, min(5, args.steps)), 2)
@@ -775,11 +806,14 @@ def sec_batch(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         torch.cuda.synchronize()
+        clk.begin()
         ev0.record(stream)
         for _ in range(steps):
             batch.run()
         ev1.record(stream)
         stats = batch.finish()
+        torch.cuda.synchronize()
+        clk.end()
     ms = ev0.elapsed_time(ev1) / steps
     # one call per problem through the single-problem device API
     for ix, q, (_, _, k) in zip(indexes, Qd, problems):
