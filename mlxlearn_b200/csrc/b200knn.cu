@@ -475,7 +475,15 @@ static bool reorder_enabled() {
 
 // Seeding pass over each query tile's home window (grouped rows): on unless
 // B2K_SEED=0 (tests run both ways).
-constexpr int kSeedTiles = 16;
+// Reference tiles per query tile of the seeding pass's home window
+// (B2K_SEED_TILES overrides).  16 was the fastest of 8, 16 and 32 on 100k
+// queries of the 1M x 128 mixture, k = 10: 8 tiles admit 4% more list
+// entries in the main pass, 32 spend 0.22 ms more seeding than they save.
+static int seed_tiles() {
+  const char* e = getenv("B2K_SEED_TILES");
+  const int t = e ? atoi(e) : 16;
+  return t < 1 ? 1 : (t > 256 ? 256 : t);
+}
 static bool seed_enabled() {
   const char* e = getenv("B2K_SEED");
   return !(e && e[0] == '0');
@@ -698,6 +706,7 @@ static int knn_device_impl(Index& ix, const float* dQ, int64_t m, int k, int exc
       // from.  A published value is the k-th smallest of real screen values
       // of the query, so it is >= the final V_k and the certificate holds.
       const int64_t m_tiles = m_pad / kTcBM;
+      const int kSeedTiles = seed_tiles();
       if (key && ix.group_start && !tc_lazy_sink(k) && n_tiles >= 2 * kSeedTiles &&
           seed_enabled()) {
         const int G = tc_column_groups(k);

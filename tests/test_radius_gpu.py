@@ -114,6 +114,28 @@ def test_radius_big_rows_sort(rng):
     np.testing.assert_array_equal(dd, od)
 
 
+@pytest.mark.parametrize("sort", [True, False])
+def test_radius_every_sort_stage_in_one_call(sort):
+    """Row lengths from 3 to 7,330 in one call: rows of up to 256 entries
+    are sorted by one warp each, up to 4,096 by one CTA each and longer rows
+    by the global-memory sort; every stage runs, with rows on both sides of
+    1,024 inside the CTA stage."""
+    rng = np.random.default_rng(31)
+    X = rng.normal(size=(9000, 4)).astype(np.float32)
+    dirs = rng.normal(size=(48, 4))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    Q = (dirs * np.linspace(0, 5.5, 48)[:, None]).astype(np.float32)
+    op, oix, od = oracle.radius(X, Q, 2.5, sort_results=sort)
+    lens = np.diff(op)
+    for lo, hi in ((2, 256), (257, 1024), (1025, 4096), (4097, 1 << 30)):
+        assert ((lens >= lo) & (lens <= hi)).sum() >= 5
+    index = make_index(X)
+    ip, ix, dd = csr(index.query_radius_csr(Q, 2.5, sort_results=sort))
+    np.testing.assert_array_equal(ip, op)
+    np.testing.assert_array_equal(ix, oix)
+    np.testing.assert_array_equal(dd, od)
+
+
 @pytest.mark.parametrize("group", ["0", "1"])
 def test_radius_row_grouping_both_ways(group, monkeypatch):
     """With grouped operand rows the fill pass lists operand rows; they are
