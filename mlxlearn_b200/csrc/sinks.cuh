@@ -38,6 +38,18 @@ __device__ __forceinline__ float min32(const float (&v)[32]) {
   return fminf(min3f(b0, b1, b2), b3);
 }
 
+// Admitted columns of a 32-column chunk as a bit mask (bit i: v[i] <= T),
+// the excluded column (self, when it lies in the chunk) cleared.
+__device__ __forceinline__ uint32_t admit_mask32(const float (&v)[32], float T, int col0,
+                                                 int self) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) m |= (v[i] <= T) ? (1u << i) : 0u;
+  const unsigned s = (unsigned)(self - col0);
+  if (s < 32u) m &= ~(1u << s);
+  return m;
+}
+
 template <int KMAX>
 struct KnnSink {
   static constexpr bool kWarpWide = false;
@@ -73,10 +85,7 @@ struct RadiusCountSink {
     cnt = 0;
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
-    if (min32(v) <= T) {
-#pragma unroll
-      for (int i = 0; i < 32; ++i) cnt += (v[i] <= T && col0 + i != self) ? 1 : 0;
-    }
+    if (min32(v) <= T) cnt += __popc(admit_mask32(v, T, col0, self));
   }
   B2K_DEV void offer1(float x, int col) { cnt += (x <= T && col != self) ? 1 : 0; }
   B2K_DEV void tile_sync() {}
@@ -98,9 +107,9 @@ struct RadiusFillSink {
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
     if (min32(v) <= T) {
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        if (v[i] <= T && col0 + i != self) *out++ = col0 + i;
+      // ascending columns: lowest set bit first
+      for (uint32_t m = admit_mask32(v, T, col0, self); m; m &= m - 1)
+        *out++ = col0 + __ffs(m) - 1;
     }
   }
   B2K_DEV void offer1(float x, int col) {
@@ -136,9 +145,12 @@ struct RadiusListSink {
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
     if (min32(v) <= T) {
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        if (v[i] <= T && col0 + i != self) put(col0 + i);
+      const uint32_t m = admit_mask32(v, T, col0, self);
+      // the entries that still fit, ascending (lowest set bit first); the
+      // count goes on past the capacity
+      int c = cnt;
+      for (uint32_t f = m; f && c < cap; f &= f - 1) out[c++] = col0 + __ffs(f) - 1;
+      cnt += __popc(m);
     }
   }
   B2K_DEV void offer1(float x, int col) {
