@@ -473,6 +473,16 @@ constexpr int kWarpSortWarps = 8;
 constexpr int kRadiusSortCap = 4096;
 constexpr int kSortThreads = 512;
 
+// Index-order sorts move one 64-bit key per entry, (training index << 16) |
+// position in the row: training indices are distinct within a row and below
+// 2^31, positions below kRadiusSortCap <= 2^16, so the keys are distinct and
+// ascend with the index; the distances follow by position afterwards.
+constexpr int kKeyPosBits = 16;
+static_assert(kRadiusSortCap <= (1 << kKeyPosBits), "row positions fit the key");
+__device__ __forceinline__ int64_t index_key(int64_t idx, int pos) {
+  return (idx << kKeyPosBits) | pos;
+}
+
 template <bool BY_DIST>
 __global__ void __launch_bounds__(kWarpSortWarps * 32)
     sort_rows_warp_kernel(const int64_t* __restrict__ indptr, int64_t m,
@@ -493,30 +503,56 @@ __global__ void __launch_bounds__(kWarpSortWarps * 32)
     }
     int P = 2;
     while (P < len) P <<= 1;
-    for (int i = lane; i < P; i += 32) {
-      sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
-      si[i] = i < len ? indices[a0 + i] : INT64_MAX;
-    }
-    __syncwarp();
-    for (int size = 2; size <= P; size <<= 1)
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int t = lane; t < P / 2; t += 32) {
-          const int i = 2 * t - (t & (stride - 1)), j = i + stride;
-          const bool up = (i & size) == 0;
-          const double x = sd[i], y = sd[j];
-          const int64_t xi = si[i], yi = si[j];
-          if (sort_after<BY_DIST>(x, xi, y, yi) == up) {
-            sd[i] = y;
-            sd[j] = x;
-            si[i] = yi;
-            si[j] = xi;
-          }
-        }
-        __syncwarp();
+    if constexpr (BY_DIST) {
+      for (int i = lane; i < P; i += 32) {
+        sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
+        si[i] = i < len ? indices[a0 + i] : INT64_MAX;
       }
-    for (int i = lane; i < len; i += 32) {
-      if (dist) dist[a0 + i] = sd[i];
-      indices[a0 + i] = si[i];
+      __syncwarp();
+      for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int t = lane; t < P / 2; t += 32) {
+            const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+            const bool up = (i & size) == 0;
+            const double x = sd[i], y = sd[j];
+            const int64_t xi = si[i], yi = si[j];
+            if (sort_after<BY_DIST>(x, xi, y, yi) == up) {
+              sd[i] = y;
+              sd[j] = x;
+              si[i] = yi;
+              si[j] = xi;
+            }
+          }
+          __syncwarp();
+        }
+      for (int i = lane; i < len; i += 32) {
+        if (dist) dist[a0 + i] = sd[i];
+        indices[a0 + i] = si[i];
+      }
+    } else {
+      // index order: one key per entry, the distance gathered by position
+      for (int i = lane; i < P; i += 32) {
+        if (i < len && dist) sd[i] = dist[a0 + i];
+        si[i] = i < len ? index_key(indices[a0 + i], i) : INT64_MAX;
+      }
+      __syncwarp();
+      for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int t = lane; t < P / 2; t += 32) {
+            const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+            const int64_t x = si[i], y = si[j];
+            if ((x > y) == ((i & size) == 0)) {
+              si[i] = y;
+              si[j] = x;
+            }
+          }
+          __syncwarp();
+        }
+      for (int i = lane; i < len; i += 32) {
+        const int64_t key = si[i];
+        indices[a0 + i] = key >> kKeyPosBits;
+        if (dist) dist[a0 + i] = sd[key & ((1 << kKeyPosBits) - 1)];
+      }
     }
     __syncwarp();
   }
@@ -541,31 +577,57 @@ __global__ void sort_rows_kernel(const int64_t* __restrict__ indptr,
     }
     int P = 2;
     while (P < len) P <<= 1;
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-      sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
-      si[i] = i < len ? indices[a0 + i] : INT64_MAX;
-    }
-    __syncthreads();
-    for (int size = 2; size <= P; size <<= 1)
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-          const int i = 2 * t - (t & (stride - 1)), j = i + stride;
-          const bool up = (i & size) == 0;
-          const double x = sd[i], y = sd[j];
-          const int64_t xi = si[i], yi = si[j];
-          const bool gt = sort_after<BY_DIST>(x, xi, y, yi);
-          if (gt == up) {
-            sd[i] = y;
-            sd[j] = x;
-            si[i] = yi;
-            si[j] = xi;
-          }
-        }
-        __syncthreads();
+    if constexpr (BY_DIST) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        sd[i] = (i < len && dist) ? dist[a0 + i] : DBL_MAX;
+        si[i] = i < len ? indices[a0 + i] : INT64_MAX;
       }
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
-      if (dist) dist[a0 + i] = sd[i];
-      indices[a0 + i] = si[i];
+      __syncthreads();
+      for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+            const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+            const bool up = (i & size) == 0;
+            const double x = sd[i], y = sd[j];
+            const int64_t xi = si[i], yi = si[j];
+            const bool gt = sort_after<BY_DIST>(x, xi, y, yi);
+            if (gt == up) {
+              sd[i] = y;
+              sd[j] = x;
+              si[i] = yi;
+              si[j] = xi;
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        if (dist) dist[a0 + i] = sd[i];
+        indices[a0 + i] = si[i];
+      }
+    } else {
+      // index order: one key per entry, the distance gathered by position
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        if (i < len && dist) sd[i] = dist[a0 + i];
+        si[i] = i < len ? index_key(indices[a0 + i], i) : INT64_MAX;
+      }
+      __syncthreads();
+      for (int size = 2; size <= P; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+            const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+            const int64_t x = si[i], y = si[j];
+            if ((x > y) == ((i & size) == 0)) {
+              si[i] = y;
+              si[j] = x;
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const int64_t key = si[i];
+        indices[a0 + i] = key >> kKeyPosBits;
+        if (dist) dist[a0 + i] = sd[key & ((1 << kKeyPosBits) - 1)];
+      }
     }
     __syncthreads();
   }

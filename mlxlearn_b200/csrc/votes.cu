@@ -49,59 +49,98 @@ __global__ void votes_kernel(const int64_t* __restrict__ idx, const double* __re
   if (pred) pred[i] = best;
 }
 
-// Radius neighbourhoods (CSR rows, ascending training index): one thread per
-// query sums its row in entry order -- the order numpy's bincount uses in the
-// reference's reductions (src/mlxlearn/_kernels/radius_reduce.py:19-94), so
-// the float64 sums are identical.  Weights: 1, or 1/d with the zero-distance
-// rule of a row.
-__device__ __forceinline__ bool radius_zero_row(const double* dist, int64_t a, int64_t b) {
-  for (int64_t e = a; e < b; ++e)
-    if (dist[e] == 0.0) return true;
-  return false;
-}
+// Radius neighbourhoods (CSR rows, ascending training index): every class's
+// float64 sum runs over the row in entry order -- the order numpy's bincount
+// uses in the reference's reductions (src/mlxlearn/_kernels/radius_reduce.py:19-94),
+// so the sums are identical.  Weights: 1, or 1/d with the zero-distance rule
+// of a row.
+// One warp per row: the lanes load 32 entries at a time (class code and
+// weight), then each lane walks them in entry order through shuffles and
+// adds the weights of its own class, 32 classes per pass over the row.  A
+// long row is no longer one thread's chain of dependent global updates.
+constexpr int kVoteWarps = 8;
 
-__global__ void radius_votes_kernel(const int64_t* __restrict__ indptr,
-                                    const int64_t* __restrict__ indices,
-                                    const double* __restrict__ dist, int64_t m,
-                                    const int* __restrict__ codes, int n_classes, int weighted,
-                                    double* __restrict__ votes, int64_t* __restrict__ counts) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+__global__ void __launch_bounds__(kVoteWarps * 32)
+    radius_votes_kernel(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
+                        const double* __restrict__ dist, int64_t m,
+                        const int* __restrict__ codes, int n_classes, int weighted,
+                        double* __restrict__ votes, int64_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (int64_t)blockIdx.x * kVoteWarps + (threadIdx.x >> 5);
+  if (i >= m) return;  // warp-uniform
   const int64_t a = indptr[i], b = indptr[i + 1];
-  double* v = votes + i * n_classes;
-  for (int c = 0; c < n_classes; ++c) v[c] = 0.0;
-  const bool zero_row = weighted && radius_zero_row(dist, a, b);
-  for (int64_t e = a; e < b; ++e) {
-    double w = 1.0;
-    if (weighted) w = zero_row ? (dist[e] == 0.0 ? 1.0 : 0.0) : 1.0 / dist[e];
-    v[codes[indices[e]]] += w;
+  bool zero_row = false;
+  if (weighted)
+    for (int64_t e0 = a; e0 < b && !zero_row; e0 += 32) {
+      const int64_t e = e0 + lane;
+      zero_row = __any_sync(0xffffffffu, e < b && dist[e] == 0.0);
+    }
+  for (int c0 = 0; c0 < n_classes; c0 += 32) {
+    const int mine = c0 + lane;
+    double acc = 0.0;
+    for (int64_t e0 = a; e0 < b; e0 += 32) {
+      const int64_t e = e0 + lane;
+      int cls = -1;
+      double w = 1.0;
+      if (e < b) {
+        cls = codes[indices[e]];
+        if (weighted) w = zero_row ? (dist[e] == 0.0 ? 1.0 : 0.0) : 1.0 / dist[e];
+      }
+      const int n = b - e0 < 32 ? (int)(b - e0) : 32;
+      for (int t = 0; t < n; ++t) {
+        const int ct = __shfl_sync(0xffffffffu, cls, t);
+        const double wt = __shfl_sync(0xffffffffu, w, t);
+        if (ct == mine) acc += wt;
+      }
+    }
+    if (mine < n_classes) votes[i * n_classes + mine] = acc;
   }
-  counts[i] = b - a;
+  if (lane == 0) counts[i] = b - a;
 }
 
-__global__ void radius_means_kernel(const int64_t* __restrict__ indptr,
-                                    const int64_t* __restrict__ indices,
-                                    const double* __restrict__ dist, int64_t m,
-                                    const double* __restrict__ targets, int weighted,
-                                    double* __restrict__ means, int64_t* __restrict__ counts) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+// Weighted or plain mean of the row's targets, one warp per row: entries are
+// loaded 32 at a time and every lane forms the same sums in entry order
+// (product first, then the sum, no FMA), as the reference's host reduction.
+__global__ void __launch_bounds__(kVoteWarps * 32)
+    radius_means_kernel(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
+                        const double* __restrict__ dist, int64_t m,
+                        const double* __restrict__ targets, int weighted,
+                        double* __restrict__ means, int64_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (int64_t)blockIdx.x * kVoteWarps + (threadIdx.x >> 5);
+  if (i >= m) return;  // warp-uniform
   const int64_t a = indptr[i], b = indptr[i + 1];
-  const bool zero_row = weighted && radius_zero_row(dist, a, b);
+  bool zero_row = false;
+  if (weighted)
+    for (int64_t e0 = a; e0 < b && !zero_row; e0 += 32) {
+      const int64_t e = e0 + lane;
+      zero_row = __any_sync(0xffffffffu, e < b && dist[e] == 0.0);
+    }
   double num = 0.0, den = 0.0;
-  for (int64_t e = a; e < b; ++e) {
-    const double y = targets[indices[e]];
-    if (weighted) {
-      const double w = zero_row ? (dist[e] == 0.0 ? 1.0 : 0.0) : 1.0 / dist[e];
-      num = __dadd_rn(num, __dmul_rn(y, w));  // product first, then the sum (no FMA)
-      den = __dadd_rn(den, w);
-    } else {
-      num = __dadd_rn(num, y);
+  for (int64_t e0 = a; e0 < b; e0 += 32) {
+    const int64_t e = e0 + lane;
+    double y = 0.0, w = 1.0;
+    if (e < b) {
+      y = targets[indices[e]];
+      if (weighted) w = zero_row ? (dist[e] == 0.0 ? 1.0 : 0.0) : 1.0 / dist[e];
+    }
+    const int n = b - e0 < 32 ? (int)(b - e0) : 32;
+    for (int t = 0; t < n; ++t) {
+      const double yt = __shfl_sync(0xffffffffu, y, t);
+      if (weighted) {
+        const double wt = __shfl_sync(0xffffffffu, w, t);
+        num = __dadd_rn(num, __dmul_rn(yt, wt));
+        den = __dadd_rn(den, wt);
+      } else {
+        num = __dadd_rn(num, yt);
+      }
     }
   }
-  if (!weighted) den = (double)(b - a);
-  means[i] = b > a ? num / den : __longlong_as_double(0x7ff8000000000000ll);
-  counts[i] = b - a;
+  if (lane == 0) {
+    if (!weighted) den = (double)(b - a);
+    means[i] = b > a ? num / den : __longlong_as_double(0x7ff8000000000000ll);
+    counts[i] = b - a;
+  }
 }
 
 }  // namespace
@@ -110,7 +149,7 @@ void launch_radius_votes(const int64_t* indptr, const int64_t* indices, const do
                          int64_t m, const int* codes, int n_classes, int weighted, double* votes,
                          int64_t* counts, cudaStream_t st) {
   if (m <= 0) return;
-  radius_votes_kernel<<<(unsigned)((m + 127) / 128), 128, 0, st>>>(
+  radius_votes_kernel<<<(unsigned)((m + kVoteWarps - 1) / kVoteWarps), kVoteWarps * 32, 0, st>>>(
       indptr, indices, dist, m, codes, n_classes, weighted, votes, counts);
 }
 
@@ -118,7 +157,7 @@ void launch_radius_means(const int64_t* indptr, const int64_t* indices, const do
                          int64_t m, const double* targets, int weighted, double* means,
                          int64_t* counts, cudaStream_t st) {
   if (m <= 0) return;
-  radius_means_kernel<<<(unsigned)((m + 127) / 128), 128, 0, st>>>(
+  radius_means_kernel<<<(unsigned)((m + kVoteWarps - 1) / kVoteWarps), kVoteWarps * 32, 0, st>>>(
       indptr, indices, dist, m, targets, weighted, means, counts);
 }
 

@@ -207,6 +207,55 @@ def test_device_radius_reductions_equal_reference_reductions(weighted):
 
 
 @gpu
+@pytest.mark.parametrize("weighted", [False, True])
+def test_device_radius_reductions_many_classes_and_long_rows(weighted):
+    # 40 classes (two 32-class passes of the device reduction) and rows of up
+    # to a few hundred entries; each class's float64 sum in entry order is
+    # np.bincount's, each mean's numerator and denominator a sequential
+    # (cumulative) sum; queries equal to training rows take the zero rule
+    import torch
+
+    from mlxlearn_b200.index import build_index
+    from mlxlearn_b200.radius_result import join_batches
+
+    rng = np.random.default_rng(37)
+    X = rng.normal(size=(5000, 4)).astype(np.float32)
+    Q = np.concatenate([X[:30], rng.normal(size=(300, 4)).astype(np.float32)])
+    labels = rng.integers(0, 40, size=5000)
+    targets = rng.normal(size=5000)
+    ix = build_index(X)
+    r = 0.9
+    ip, ii, dd = join_batches(ix.query_radius_csr(Q, r, need_distance=True))
+    lens = np.diff(ip)
+    assert lens.max() > 200 and (lens == 0).any()
+    hv = np.zeros((len(Q), 40))
+    hm = np.full(len(Q), np.nan)
+    for q in range(len(Q)):
+        a, b = ip[q], ip[q + 1]
+        if b == a:
+            continue
+        d = dd[a:b]
+        if weighted:
+            w = (d == 0).astype(np.float64) if (d == 0).any() else 1.0 / d
+        else:
+            w = np.ones(b - a)
+        hv[q] = np.bincount(labels[ii[a:b]], weights=w, minlength=40)
+        y = targets[ii[a:b]]
+        num = np.cumsum(y * w)[-1] if weighted else np.cumsum(y)[-1]
+        den = np.cumsum(w)[-1] if weighted else float(b - a)
+        hm[q] = num / den
+    dev = torch.device("cuda", 0)
+    dv, dc = ix.query_radius_reduce(Q, r, codes=torch.from_numpy(labels.astype(np.int32)).to(dev),
+                                    n_classes=40, weighted=weighted)
+    dm, _ = ix.query_radius_reduce(Q, r, targets=torch.from_numpy(targets).to(dev),
+                                   weighted=weighted)
+    np.testing.assert_array_equal(dc, lens)
+    np.testing.assert_array_equal(dv, hv)
+    np.testing.assert_array_equal(np.isnan(dm), np.isnan(hm))
+    np.testing.assert_array_equal(dm[~np.isnan(dm)], hm[~np.isnan(hm)])
+
+
+@gpu
 def test_radius_estimators_pickle(rng):
     X, y, Q = radius_data()
     clf = RadiusNeighborsClassifier(radius=6.25, outlier_label="most_frequent").fit(X, y)
