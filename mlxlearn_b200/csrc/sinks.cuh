@@ -27,24 +27,30 @@ struct SinkArgs {
   int rcap;              // RadiusListSink: entries kept per list
 };
 
-// Shared 32-column prefilter: the 3-input-min tree over the chunk.
-__device__ __forceinline__ float min32(const float (&v)[32]) {
-  float a[11];
-#pragma unroll
-  for (int i = 0; i < 10; ++i) a[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
-  a[10] = fminf(v[30], v[31]);
-  const float b0 = min3f(a[0], a[1], a[2]), b1 = min3f(a[3], a[4], a[5]);
-  const float b2 = min3f(a[6], a[7], a[8]), b3 = fminf(a[9], a[10]);
-  return fminf(min3f(b0, b1, b2), b3);
-}
-
 // Admitted columns of a 32-column chunk as a bit mask (bit i: v[i] <= T),
-// the excluded column (self, when it lies in the chunk) cleared.
+// the excluded column (self, when it lies in the chunk) cleared.  The four
+// 8-column group minima come first (3-input minima); only groups
+// whose minimum passes build their bits, so a warp pays for a group only
+// where one of its rows admits.  NaN values (padding rows) never pass.
 __device__ __forceinline__ uint32_t admit_mask32(const float (&v)[32], float T, int col0,
                                                  int self) {
+  float g[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float a = min3f(v[8 * q], v[8 * q + 1], v[8 * q + 2]);
+    const float b = min3f(v[8 * q + 3], v[8 * q + 4], v[8 * q + 5]);
+    g[q] = min3f(a, b, fminf(v[8 * q + 6], v[8 * q + 7]));
+  }
+  if (!(fminf(min3f(g[0], g[1], g[2]), g[3]) <= T)) return 0u;
   uint32_t m = 0;
 #pragma unroll
-  for (int i = 0; i < 32; ++i) m |= (v[i] <= T) ? (1u << i) : 0u;
+  for (int q = 0; q < 4; ++q)
+    if (g[q] <= T) {
+      uint32_t bits = 0;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) bits |= (v[8 * q + e] <= T) ? (1u << e) : 0u;
+      m |= bits << (8 * q);
+    }
   const unsigned s = (unsigned)(self - col0);
   if (s < 32u) m &= ~(1u << s);
   return m;
@@ -85,7 +91,7 @@ struct RadiusCountSink {
     cnt = 0;
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
-    if (min32(v) <= T) cnt += __popc(admit_mask32(v, T, col0, self));
+    cnt += __popc(admit_mask32(v, T, col0, self));
   }
   B2K_DEV void offer1(float x, int col) { cnt += (x <= T && col != self) ? 1 : 0; }
   B2K_DEV void tile_sync() {}
@@ -106,11 +112,8 @@ struct RadiusFillSink {
     out = a.rcols + a.roff[slot];
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
-    if (min32(v) <= T) {
-      // ascending columns: lowest set bit first
-      for (uint32_t m = admit_mask32(v, T, col0, self); m; m &= m - 1)
-        *out++ = col0 + __ffs(m) - 1;
-    }
+    // ascending columns: lowest set bit first
+    for (uint32_t m = admit_mask32(v, T, col0, self); m; m &= m - 1) *out++ = col0 + __ffs(m) - 1;
   }
   B2K_DEV void offer1(float x, int col) {
     if (x <= T && col != self) *out++ = col;
@@ -144,8 +147,8 @@ struct RadiusListSink {
     ++cnt;
   }
   B2K_DEV void offer32(const float (&v)[32], int col0, float*) {
-    if (min32(v) <= T) {
-      const uint32_t m = admit_mask32(v, T, col0, self);
+    const uint32_t m = admit_mask32(v, T, col0, self);
+    if (m) {
       // the entries that still fit, ascending (lowest set bit first); the
       // count goes on past the capacity
       int c = cnt;
