@@ -321,6 +321,19 @@ B2K_API int b2k_radius_result_class_votes(const b2k_radius_result *res, const in
                                           int32_t n_classes, int32_t weighted, double *d_votes,
                                           int64_t *d_counts, void *stream);
 
+/* Predicted class codes of a radius result with uniform weights, on the
+ * device: pred int64[m] receives each row's first maximum of its class counts
+ * (ties -> smallest code; 0 for an empty row) and counts int64[m] its
+ * neighbour count; the votes themselves are not written.  Equal to the argmax
+ * of the normalised votes: the counts are integers, and dividing them by the
+ * row's total keeps distinct counts distinct.  Synchronises `stream`.
+ * Replaces the host argmax of RadiusNeighborsClassifier.predict
+ * (src/mlxlearn/neighbors/_radius.py:110-136,180-205).  No separate reference entry
+ * point: the reference computes the probabilities and takes their argmax. */
+B2K_API int b2k_radius_result_class_predict(const b2k_radius_result *res,
+                                            const int32_t *d_codes, int32_t n_classes,
+                                            int64_t *d_pred, int64_t *d_counts, void *stream);
+
 /* Means of float64 targets[n_train] (device) over each radius row, weight 1 or
  * 1/d as above; NaN for empty rows.  means float64[m], counts int64[m]
  * (device).  Replaces src/mlxlearn/_kernels/radius_reduce.py:62-94

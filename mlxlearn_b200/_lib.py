@@ -123,6 +123,7 @@ SIGNATURES = {
     "b2k_radius_result_fetch": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "b2k_radius_result_release": (ctypes.c_int, [_vp]),
     "b2k_radius_result_class_votes": (ctypes.c_int, [_vp, _vp, _i32, _i32, _vp, _vp, _vp]),
+    "b2k_radius_result_class_predict": (ctypes.c_int, [_vp, _vp, _i32, _vp, _vp, _vp]),
     "b2k_radius_result_means": (ctypes.c_int, [_vp, _vp, _i32, _vp, _vp, _vp]),
     "b2k_batch_create": (ctypes.c_int, [ctypes.POINTER(Problem), _i32, _i32, _vp,
                                         ctypes.POINTER(_vp)]),

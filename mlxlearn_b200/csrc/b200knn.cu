@@ -1607,6 +1607,23 @@ int b2k_radius_result_class_votes(const b2k_radius_result* res, const int32_t* d
   return B2K_OK;
 }
 
+int b2k_radius_result_class_predict(const b2k_radius_result* res, const int32_t* d_codes,
+                                    int32_t n_classes, int64_t* d_pred, int64_t* d_counts,
+                                    void* stream) {
+  if (!res) return fail(B2K_EINVAL, "result must not be NULL");
+  if (n_classes <= 0) return fail(B2K_EINVAL, "n_classes must be positive");
+  if (res->m > 0 && (!d_codes || !d_pred || !d_counts))
+    return fail(B2K_EINVAL, "device pointers must not be NULL");
+  if (res->m == 0) return B2K_OK;
+  B2K_CUDA(cudaSetDevice(res->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  launch_radius_votes(res->indptr, res->indices, res->dist, res->m, d_codes, n_classes,
+                      /*weighted=*/0, /*votes=*/nullptr, d_counts, st, d_pred);
+  B2K_CUDA(cudaGetLastError());
+  B2K_CUDA(cudaStreamSynchronize(st));
+  return B2K_OK;
+}
+
 int b2k_radius_result_means(const b2k_radius_result* res, const double* d_targets,
                             int32_t weighted, double* d_means, int64_t* d_counts,
                             void* stream) {

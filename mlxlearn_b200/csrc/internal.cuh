@@ -329,9 +329,10 @@ void launch_votes(const int64_t* idx, const double* dist, int64_t m, int k, cons
                   int n_classes, int weighted, double* votes, int64_t* pred, int* status,
                   cudaStream_t st);
 
+// votes may be null when pred is given: pred[i] = the row's first maximum.
 void launch_radius_votes(const int64_t* indptr, const int64_t* indices, const double* dist,
                          int64_t m, const int* codes, int n_classes, int weighted, double* votes,
-                         int64_t* counts, cudaStream_t st);
+                         int64_t* counts, cudaStream_t st, int64_t* pred = nullptr);
 void launch_radius_means(const int64_t* indptr, const int64_t* indices, const double* dist,
                          int64_t m, const double* targets, int weighted, double* means,
                          int64_t* counts, cudaStream_t st);

@@ -60,11 +60,15 @@ __global__ void votes_kernel(const int64_t* __restrict__ idx, const double* __re
 // long row is no longer one thread's chain of dependent global updates.
 constexpr int kVoteWarps = 8;
 
+// votes may be null when pred is not: pred[i] is then the row's first
+// maximum over the classes (ties -> smallest code, 0 for an empty row), as
+// numpy's argmax.
 __global__ void __launch_bounds__(kVoteWarps * 32)
     radius_votes_kernel(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
                         const double* __restrict__ dist, int64_t m,
                         const int* __restrict__ codes, int n_classes, int weighted,
-                        double* __restrict__ votes, int64_t* __restrict__ counts) {
+                        double* __restrict__ votes, int64_t* __restrict__ counts,
+                        int64_t* __restrict__ pred) {
   const int lane = threadIdx.x & 31;
   const int64_t i = (int64_t)blockIdx.x * kVoteWarps + (threadIdx.x >> 5);
   if (i >= m) return;  // warp-uniform
@@ -75,6 +79,8 @@ __global__ void __launch_bounds__(kVoteWarps * 32)
       const int64_t e = e0 + lane;
       zero_row = __any_sync(0xffffffffu, e < b && dist[e] == 0.0);
     }
+  double best = -INFINITY;  // pred: the first maximum so far and its class
+  int best_class = 0;
   for (int c0 = 0; c0 < n_classes; c0 += 32) {
     const int mine = c0 + lane;
     double acc = 0.0;
@@ -93,9 +99,30 @@ __global__ void __launch_bounds__(kVoteWarps * 32)
         if (ct == mine) acc += wt;
       }
     }
-    if (mine < n_classes) votes[i * n_classes + mine] = acc;
+    if (votes && mine < n_classes) votes[i * n_classes + mine] = acc;
+    if (pred) {
+      // this pass's maximum, the smallest class among equal values; a later
+      // pass replaces the running one only when strictly larger
+      double v = mine < n_classes ? acc : -INFINITY;
+      int c = mine;
+      for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oc = __shfl_xor_sync(0xffffffffu, c, o);
+        if (ov > v || (ov == v && oc < c)) {
+          v = ov;
+          c = oc;
+        }
+      }
+      if (v > best) {
+        best = v;
+        best_class = c;
+      }
+    }
   }
-  if (lane == 0) counts[i] = b - a;
+  if (lane == 0) {
+    counts[i] = b - a;
+    if (pred) pred[i] = best_class;
+  }
 }
 
 // Weighted or plain mean of the row's targets, one warp per row: entries are
@@ -147,10 +174,10 @@ __global__ void __launch_bounds__(kVoteWarps * 32)
 
 void launch_radius_votes(const int64_t* indptr, const int64_t* indices, const double* dist,
                          int64_t m, const int* codes, int n_classes, int weighted, double* votes,
-                         int64_t* counts, cudaStream_t st) {
+                         int64_t* counts, cudaStream_t st, int64_t* pred) {
   if (m <= 0) return;
   radius_votes_kernel<<<(unsigned)((m + kVoteWarps - 1) / kVoteWarps), kVoteWarps * 32, 0, st>>>(
-      indptr, indices, dist, m, codes, n_classes, weighted, votes, counts);
+      indptr, indices, dist, m, codes, n_classes, weighted, votes, counts, pred);
 }
 
 void launch_radius_means(const int64_t* indptr, const int64_t* indices, const double* dist,

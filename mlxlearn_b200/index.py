@@ -342,6 +342,21 @@ class NeighborIndex:
             return pieces[0]
         return (np.concatenate([a for a, _ in pieces]), np.concatenate([c for _, c in pieces]))
 
+    def query_radius_predict(self, Q, radius, *, codes, n_classes, exclude_self=False,
+                             query_block_size=None):
+        """Per-query first maximum of the class counts within ``radius``
+        (uniform weights; ties -> smallest code, 0 for an empty row) and the
+        counts, as numpy int64 arrays: the argmax of the normalised votes,
+        computed on the device without downloading the votes."""
+        parts = self.query_radius_csr(Q, radius, need_distance=False, exclude_self=exclude_self,
+                                      query_block_size=query_block_size, raw=True)
+        pieces = [p.predict_codes(codes, n_classes) for p in parts]
+        for p in parts:
+            p.release()
+        if len(pieces) == 1:
+            return pieces[0]
+        return (np.concatenate([a for a, _ in pieces]), np.concatenate([c for _, c in pieces]))
+
     def query_radius(self, Q, radius, *, return_distance=True, exclude_self=False,
                      sort_results=False, query_block_size=None, train_block_size=None,
                      algorithm="auto"):

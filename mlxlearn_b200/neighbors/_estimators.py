@@ -198,37 +198,55 @@ class RadiusNeighborsClassifier(RadiusMixin, NeighborsMixin, ClassifierMixin, Ba
         self.outlier_label_ = _resolve_outlier_label(self.outlier_label, self.classes_, self._y)
         return self
 
-    def _proba(self, X):
+    def _codes_device(self):
+        """The training rows' class codes on the index's device (cached)."""
         import torch
 
-        if self.weights not in (None, "uniform", "distance"):
-            raise ValueError("weights not recognized: should be 'uniform' or 'distance', "
-                             f"got {self.weights!r}")
-        weighted = self.weights == "distance"
         codes = self.__dict__.get("_codes_dev")
         if codes is None:
             codes = torch.from_numpy(self._y.astype(np.int32)).to(
                 torch.device("cuda", self._index_.device))
             self.__dict__["_codes_dev"] = codes
-        Q, query_is_train = self._radius_query(X)
-        # votes reduced on the device from the device neighbourhoods
-        votes, counts = self._index_.query_radius_reduce(
-            Q, self.radius, codes=codes, n_classes=len(self.classes_), weighted=weighted,
-            exclude_self=query_is_train)
-        self._last_query_backend = "cuda"
+        return codes
+
+    def _check_weights(self):
+        if self.weights not in (None, "uniform", "distance"):
+            raise ValueError("weights not recognized: should be 'uniform' or 'distance', "
+                             f"got {self.weights!r}")
+        return self.weights == "distance"
+
+    def _outliers(self, counts, stacklevel):
+        """Rows without neighbours; raises without an outlier label, and
+        returns the label's column in ``classes_`` (or None, with the
+        reference's warning at the user's call) when there are some."""
         outliers = np.flatnonzero(counts == 0)
         if outliers.size > 0 and self.outlier_label_ is None:
             raise ValueError("No neighbors found for test samples "
                              f"{outliers!r}, you can try using larger radius, giving a label "
                              "for outliers, or considering removing them from your dataset.")
+        match = None
         if outliers.size > 0:
             label = self.outlier_label_[0]
-            match = np.flatnonzero(self.classes_ == label)
-            if match.size == 1:
-                votes[outliers, match[0]] = 1.0
+            found = np.flatnonzero(self.classes_ == label)
+            if found.size == 1:
+                match = int(found[0])
             else:
                 warnings.warn(f"Outlier label {label} is not in training classes. All class "
-                              "probabilities of outliers will be assigned with 0.", stacklevel=3)
+                              "probabilities of outliers will be assigned with 0.",
+                              stacklevel=stacklevel)
+        return outliers, match
+
+    def _proba(self, X):
+        weighted = self._check_weights()
+        Q, query_is_train = self._radius_query(X)
+        # votes reduced on the device from the device neighbourhoods
+        votes, counts = self._index_.query_radius_reduce(
+            Q, self.radius, codes=self._codes_device(), n_classes=len(self.classes_),
+            weighted=weighted, exclude_self=query_is_train)
+        self._last_query_backend = "cuda"
+        outliers, match = self._outliers(counts, stacklevel=4)  # user -> predict* -> _proba
+        if match is not None:
+            votes[outliers, match] = 1.0
         normalizer = votes.sum(axis=1)[:, None]
         normalizer[normalizer == 0.0] = 1.0
         votes /= normalizer
@@ -236,12 +254,28 @@ class RadiusNeighborsClassifier(RadiusMixin, NeighborsMixin, ClassifierMixin, Ba
 
     def predict(self, X):
         check_is_fitted(self, "_index_")
-        proba = self._proba(X)
-        labels = self.classes_.take(proba.argmax(axis=1))
-        empty = np.all(proba == 0.0, axis=1)
-        if np.any(empty):
+        if self._check_weights():
+            proba = self._proba(X)
+            labels = self.classes_.take(proba.argmax(axis=1))
+            empty = np.all(proba == 0.0, axis=1)
+            if np.any(empty):
+                labels = np.array(labels, copy=True)
+                labels[empty] = self.outlier_label_[0]
+            return labels
+        # uniform weights: the counts are integers, so the argmax of the
+        # normalised votes is the argmax of the counts, taken on the device;
+        # a row with neighbours is never all-zero, an outlier row takes the
+        # outlier label either way
+        Q, query_is_train = self._radius_query(X)
+        pred, counts = self._index_.query_radius_predict(
+            Q, self.radius, codes=self._codes_device(), n_classes=len(self.classes_),
+            exclude_self=query_is_train)
+        self._last_query_backend = "cuda"
+        outliers, _ = self._outliers(counts, stacklevel=3)  # user -> predict
+        labels = self.classes_.take(pred)
+        if outliers.size > 0:
             labels = np.array(labels, copy=True)
-            labels[empty] = self.outlier_label_[0]
+            labels[outliers] = self.outlier_label_[0]
         return labels
 
     def predict_proba(self, X):

@@ -179,6 +179,29 @@ class RadiusCSR:
         counts, summed on the device in ascending training-index order."""
         return self._reduce(codes, "votes", int(n_classes), weighted)
 
+    def predict_codes(self, codes, n_classes: int):
+        """Per-row first maximum of the class counts (ties -> smallest code,
+        0 for an empty row) and the neighbour counts, computed on the device
+        without downloading the votes; uniform weights only."""
+        import torch
+
+        if self._handle is None:
+            raise RuntimeError("device reductions need a batch whose device result is held "
+                               "(query_radius_csr(..., raw=True))")
+        dev = torch.device("cuda", self._device)
+        vals = (codes if isinstance(codes, torch.Tensor) and codes.is_cuda
+                else torch.from_numpy(np.ascontiguousarray(codes, dtype=np.int32)))
+        vals = vals.to(device=dev, dtype=torch.int32).contiguous()
+        pred = torch.empty(self._m, dtype=torch.int64, device=dev)
+        counts = torch.empty(self._m, dtype=torch.int64, device=dev)
+        if self._m:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            rc = _lib.load().b2k_radius_result_class_predict(
+                self._handle, vals.data_ptr(), int(n_classes), pred.data_ptr(),
+                counts.data_ptr(), stream)
+            _lib.check(rc, "radius prediction")
+        return pred.cpu().numpy(), counts.cpu().numpy()
+
     def mean(self, targets, weighted: bool):
         """Per-row (1/d-weighted) mean of float64 targets, NaN for empty rows,
         and neighbour counts."""

@@ -116,6 +116,43 @@ def test_radius_classifier_matches_reference():
 
 
 @gpu
+def test_radius_classifier_device_predict_equals_proba_argmax():
+    # uniform weights: predict takes each row's first maximum of its class
+    # counts on the device; it must equal the argmax of predict_proba (the
+    # reference's route) including ties (lattice points, many equal counts),
+    # outliers whose label is or is not a class, and 40 classes (two passes)
+    rng = np.random.default_rng(41)
+    X = rng.integers(-3, 4, size=(3000, 3)).astype(np.float32)
+    y = rng.integers(0, 40, size=3000)
+    Q = np.concatenate([rng.integers(-3, 4, size=(300, 3)).astype(np.float32),
+                        np.full((4, 3), 50.0, np.float32)])
+    for label, in_classes in ((7, True), (99, False)):
+        clf = RadiusNeighborsClassifier(radius=1.0, outlier_label=label).fit(X, y)
+        with warnings.catch_warnings(record=True) as w:
+            warnings.simplefilter("always")
+            pred = clf.predict(Q)
+            proba = clf.predict_proba(Q)
+        want = clf.classes_.take(proba.argmax(axis=1))
+        empty = np.all(proba == 0.0, axis=1)
+        want[empty] = label
+        np.testing.assert_array_equal(pred, want)
+        assert (pred[-4:] == label).all()
+        msgs = [str(x.message) for x in w if "not in training classes" in str(x.message)]
+        assert len(msgs) == (0 if in_classes else 2)  # predict and predict_proba
+        if not in_classes:
+            assert all(x.filename == __file__ for x in w
+                       if "not in training classes" in str(x.message))
+        # rows with tied top counts exist, so the tie rule is exercised
+        top = np.sort(proba[:-4], axis=1)
+        assert (top[:, -1] == top[:, -2]).any()
+    # string labels and self-queries (X=None) through the same route
+    names = np.array([f"c{v:02d}" for v in y])
+    clf = RadiusNeighborsClassifier(radius=1.0, outlier_label="most_frequent").fit(X, names)
+    proba = clf.predict_proba(None)
+    np.testing.assert_array_equal(clf.predict(None), clf.classes_.take(proba.argmax(axis=1)))
+
+
+@gpu
 def test_radius_regressor_nan_and_warning():
     X, y, Q = radius_data()
     reg = RadiusNeighborsRegressor(radius=6.25).fit(X, y.astype(np.float64))
