@@ -75,6 +75,33 @@ def test_sklearn_estimator_protocol():
 
 # ------------------------------------------------------------------ GPU side
 
+def test_radius_outlier_rules_on_the_host():
+    # the outlier rules shared by predict and predict_proba, without a search:
+    # no label raises the reference's error, a label among the classes gives
+    # its column, a label outside them warns at the caller and gives none
+    clf = RadiusNeighborsClassifier(radius=1.0)
+    clf.classes_ = np.array([3, 5, 9])
+    counts = np.array([2, 0, 1, 0])
+    clf.outlier_label_ = None
+    with pytest.raises(ValueError, match=r"No neighbors found for test samples array\(\[1, 3\]\)"):
+        clf._outliers(counts, stacklevel=2)
+    clf.outlier_label_ = [5]
+    outliers, match = clf._outliers(counts, stacklevel=2)
+    np.testing.assert_array_equal(outliers, [1, 3])
+    assert match == 1
+    clf.outlier_label_ = [4]
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        outliers, match = clf._outliers(counts, stacklevel=2)
+    assert match is None and len(w) == 1
+    assert "Outlier label 4 is not in training classes" in str(w[0].message)
+    assert w[0].filename == __file__
+    # no outliers: nothing raised or warned, whatever the label
+    clf.outlier_label_ = None
+    outliers, match = clf._outliers(np.array([1, 2]), stacklevel=2)
+    assert outliers.size == 0 and match is None
+
+
 @gpu
 def test_classifier_regressor_match_reference_predictions():
     X, y, Q = radius_data()
