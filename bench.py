@@ -649,8 +649,9 @@ def sec_pixels(args):
         "certified_bf16": {"value": len(Q) / (ms_bf16 / 1000), "unit": "queries/s",
                            "ms_per_step": ms_bf16, "screen_stats": st_bf16,
                            "form": "bf16 tcgen05 screen + certified re-rank on the same data"},
+        # downloaded per step: float64 votes [m, classes] and int64 predictions [m]
         "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": Q.nbytes,
-                "d2h_bytes_per_step": pred.nbytes,
+                "d2h_bytes_per_step": len(Q) * (len(clf.classes_) + 1) * 8,
                 "api": "KNeighborsClassifier.predict (host arrays; votes on the device)"},
     }
     threads = host_threads()
@@ -727,9 +728,11 @@ def sec_radius(args):
                      "frac": 2.0 * X.shape[0] * X.shape[1] * len(Q) / csr_s / 1e12 / tf_burst,
                      "peak_source": f"{peak_kind} burst bf16", "traffic": None,
                      "hbm_gbs_of_call": moved / csr_s / 1e9},
+        # downloaded per step: int64 class codes and int64 neighbour counts [m]
         "e2e": {"value": len(Q) / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": Q.nbytes,
-                "d2h_bytes_per_step": pred.nbytes,
-                "api": "RadiusNeighborsClassifier.predict (host arrays; votes on the device)"},
+                "d2h_bytes_per_step": len(Q) * 2 * 8,
+                "api": "RadiusNeighborsClassifier.predict (host arrays; class counts and "
+                       "their argmax on the device)"},
     }
     threads = host_threads()
     nb = reference_neighbors()
